@@ -1,0 +1,461 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 IFOS3D wavefield engine.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload visco256|elastic128]
+                    [--impl ours|reference]
+
+A step is one pass of the hot path over one batch of synthetic input:
+  visco256   (default) one viscoelastic (L=3) forward modelling run of a shot,
+             256^3 cells, NT=3000, 400 receivers — the plain viscoelastic
+             forward-modelling configuration; per GPU one shot (shots shard
+             across ranks, no data-path collective: weak scaling).
+  elastic128 one shot-gradient (forward + residual + adjoint + DFT gradient),
+             128^3, NT=2000, 2 frequencies.
+metric: cell-updates per second over all ranks (all NX*NY*NZ cells of every
+shot and time step, CPML frame included; forward and adjoint both count).
+
+Rank 0 prints one JSON line. Inputs are seeded synthetic models (no field data).
+The state of one 256^3 L=3 shot (about 2.1 GB of fields) is far larger than the
+126 MB L2, so every timed step streams from HBM without an explicit flush.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "ifos3d-dev_b200"))
+
+import numpy as np  # noqa: E402
+
+METRIC = "Gcell-updates/s and shot-gradients/s, batched vs per-shot, grad rel-err<=1e-4"
+UNIT = "Gcell-updates/s"
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def slab_memberships(p) -> float:
+    """Average number of CPML face slabs a cell lies in (x faces, z faces, bottom y
+    face, plus the top y face without a free surface)."""
+    n = p.nx * p.ny * p.nz
+    fw = p.fw
+    m = 2 * fw * p.ny * p.nz + 2 * fw * p.nx * p.ny + (1 if p.free_surf else 2) * fw * p.nx * p.nz
+    return m / n
+
+
+def alg_bytes_per_cell_step(p, nf: int, ntast: int) -> dict:
+    """Compulsory HBM bytes per cell-update: every live state word read and written
+    once, every model word read once, averaged moduli counted as recomputable.
+    Split between the two kernels of a step (velocity / stress)."""
+    L = p.nmech
+    slab = slab_memberships(p)
+    vel = 4 * (3 + 3) + 4 * 1 + 24 * slab            # v R+W, rho, 3 psi R+W per slab
+    stress = 4 * (6 + 6) + 4 * 2 + 24 * slab          # sigma R+W, pi, u, 3 psi R+W per slab
+    if L:
+        stress += 48 * L + 8                           # 6 r R+W per mechanism, taus, taup
+    stress += 48.0 * nf / max(ntast, 1)                # 6 DFT accumulators R+W per frequency
+    return dict(vel=vel, stress=stress, total=vel + stress)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, local_rank: int):
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+        ids = [x for x in vis.split(",") if x.strip()]
+        self.gpu = ids[local_rank] if local_rank < len(ids) else str(local_rank)
+        self.proc = None
+        self.tmp = None
+
+    def __enter__(self):
+        try:
+            self.tmp = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.tmp, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.tmp:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        with open(self.tmp.name) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9 and parts[1].replace(".", "").isdigit():
+                    rows.append(parts)
+        os.unlink(self.tmp.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[q] for r in rows for q in range(4) if r[5 + q].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]), "reasons": reasons,
+                "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit())}
+
+
+# ---------------------------------------------------------------------------
+# CPU side: the oracle (reported baseline and the reference arm)
+
+def _cpu_sample_worker(args):
+    """One process: the CPU implementation on a bounded sample grid."""
+    kind, nx, ny, nz, nmech, nt = args
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from pyoracle import Oracle, IfoParams
+    from ifosb import synth
+    c = synth.small_case(nx=nx, ny=ny, nz=nz, nt=nt, fw=10, nmech=nmech, ntr=16, finv=())
+    p = c["params"]
+    ip = IfoParams(nx=p.nx, ny=p.ny, nz=p.nz, dx=p.dx, dy=p.dy, dz=p.dz, dt=p.dt, nt=p.nt, time=p.time,
+                   fdcoeff=p.fdcoeff, free_surf=p.free_surf, fw=p.fw, nmech=p.nmech, ndt=1, ndtshift=0,
+                   vppml=c["vppml"], fpml=c["fpml"], alpha=0.0, beta=0.0, source_shape=4)
+    O = Oracle(kind)
+    vp, vs, rho = c["start"]
+    m = O.readmod(ip, vp, vs, rho, tau=c["tau"], fl=c["fl"])
+    cp = O.cpml_coeff(ip)
+    sp = c["shots"][0]
+    sig = O.wavelet(ip, sp)
+    t0 = time.perf_counter()
+    O.forward(ip, m, cp, sp, sig, c["recpos"])
+    return time.perf_counter() - t0, nx * ny * nz * nt
+
+
+def cpu_run(kind, nmech, procs, grid, nt):
+    """Run `procs` single-threaded oracle processes (spawned) on the sample; returns Gcell/s."""
+    import multiprocessing as mp
+    args = [(kind, grid[0], grid[1], grid[2], nmech, nt)] * procs
+    t0 = time.perf_counter()
+    if procs == 1:
+        res = [_cpu_sample_worker(args[0])]
+    else:
+        with mp.get_context("spawn").Pool(procs) as pool:
+            res = pool.map(_cpu_sample_worker, args)
+    wall = time.perf_counter() - t0
+    cells = sum(r[1] for r in res)
+    busy = max(r[0] for r in res)
+    return cells / busy / 1e9, cells / wall / 1e9, cells
+
+
+def cpu_kind(nmech):
+    """The reference itself (oracle/_ref) when it can run the workload, else the C restatement."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from pyoracle import have_ref
+    return ("ref", "reference") if (nmech <= 1 and have_ref()) else ("oracle", "port")
+
+
+# ---------------------------------------------------------------------------
+
+def setup_dist(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local, dist
+
+
+def reference_arm(args, world, rank, dist):
+    """Times the reference's CPU implementation on this host's cores (rank 0 only)."""
+    if rank != 0:
+        return
+    import multiprocessing as mp
+    wl = args.workload
+    nmech = 3 if wl == "visco256" else 0
+    code, kind = cpu_kind(nmech)
+    procs = max(1, min(mp.cpu_count(), args.cpu_procs or mp.cpu_count()))
+    grid, nt = (64, 64, 64), args.cpu_nt
+    for _ in range(args.warmup if args.cpu_warmup else 0):
+        cpu_run(code, nmech, procs, grid, max(2, nt // 4))
+    vals, walls = [], []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        agg, _, cells = cpu_run(code, nmech, procs, grid, nt)
+        walls.append(time.perf_counter() - t0)
+        vals.append(agg)
+    value = float(np.median(vals))
+    sample = (f"{procs} single-threaded processes, each a {grid[0]}x{grid[1]}x{grid[2]} grid x {nt} steps "
+              f"(FW=10 CPML, free surface, L={nmech}) of the same algorithm; Gcell-updates/s aggregated")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": round(value, 5), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * float(np.median(walls)), 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": workload_config(wl, world),
+        "cpu_baseline": {"value": round(value, 5), "unit": UNIT, "cores": procs, "kind": kind, "sample": sample},
+        "e2e": {"value": round(value, 5), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def workload_config(wl, world):
+    if wl == "visco256":
+        return {"workload": "visco256: viscoelastic L=3 (Q=50, 20-200 Hz) forward modelling, 256^3 cells, "
+                            "NT=3000, 8 layers, sin^3 fc=80 Hz, 400 receivers, 1 shot per GPU",
+                "grid": [256, 256, 256], "nt": 3000, "nmech": 3, "shots_per_gpu": 1, "receivers": 400,
+                "parallelism": f"shot-sharded x{world}", "l2_flush": "state 2.1 GB per shot > 126 MB L2"}
+    return {"workload": "elastic128: elastic FWI shot-gradient (forward+residual+adjoint+DFT gradient), 128^3, "
+                        "NT=2000, 2 frequencies, 25 receivers, 1 shot per GPU",
+            "grid": [128, 128, 128], "nt": 2000, "nmech": 0, "nf": 2, "shots_per_gpu": 1, "receivers": 25,
+            "parallelism": f"shot-sharded x{world}", "l2_flush": "state+DFT 0.37 GB per shot > 126 MB L2"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="visco256", choices=["visco256", "elastic128"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nt", type=int, default=None, help="override NT (testing only)")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extras", action="store_true")
+    ap.add_argument("--cpu-procs", type=int, default=0)
+    ap.add_argument("--cpu-nt", type=int, default=40)
+    ap.add_argument("--cpu-warmup", action="store_true")
+    args = ap.parse_args()
+    world, rank, local, dist = setup_dist(args)
+    if args.impl == "reference":
+        reference_arm(args, world, rank, dist)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    import torch
+    import ifosb
+    from ifosb import synth
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+
+    wl = args.workload
+    c = synth.case(wl, nt=args.nt)
+    p = c["params"]
+    # shot sharding: rank r models its own source position (a shifted copy of the case's shot)
+    sp = c["shots"][0].copy()
+    sp[0, 0] = min(p.nx - p.fw - 1, max(p.fw + 2, int(sp[0, 0]) + 8 * (rank - world // 2)))
+    c["shots"] = [sp]
+    m, cp, shots = synth.build_inputs(c)
+    nf = len(c["finv"])
+    eng = ifosb.Engine(p, max_shots=1, max_nf=nf)
+    eng.set_stream(stream.cuda_stream)
+    eng.set_cpml(cp)
+    eng.set_model(m["rho"], m["pi"], m["u"], m["taus"], m["taup"], m["eta"])
+    eng.set_receivers(c["recpos"])
+    eng.set_frequencies(c["finv"] if nf else None, c["ntast"])
+    cells_step = p.nx * p.ny * p.nz * p.nt * (2 if wl == "elastic128" else 1)
+
+    obs = None
+    if wl == "elastic128":
+        # observed data: the same shot in the true (anomaly) model
+        mt, _, _ = synth.build_inputs(c, "true")
+        eng.set_model(mt["rho"], mt["pi"], mt["u"], mt["taus"], mt["taup"], mt["eta"])
+        obs = eng.forward(shots)
+        eng.set_model(m["rho"], m["pi"], m["u"], m["taus"], m["taup"], m["eta"])
+
+    def step():
+        if wl == "elastic128":
+            eng.shot_gradient(shots, obs)
+        else:
+            eng.forward(shots, want_sections=False)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+        if dist:
+            dist.barrier()
+    clocks = clk.summary()
+    ms = ev0.elapsed_time(ev1)
+    if dist:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    # our kernels per step: 2 per time step (velocity, stress); a shot-gradient adds the
+    # adjoint loop, residual + misfit and the gradient kernel
+    launches = args.steps * (2 * p.nt if wl == "visco256" else 4 * p.nt + 3)
+    value = world * cells_step * args.steps / (ms / 1000.0) / 1e9
+
+    # ---- end to end through the public API: host model + wavelet in, traces out, every step
+    pin = lambda a: None if a is None else torch.from_numpy(np.ascontiguousarray(ifosb.ghost_wrap(a))).pin_memory()
+    hm = {k: pin(m[k]) for k in ("rho", "pi", "u", "taus", "taup")}
+    sig_pinned = torch.from_numpy(shots[0][1]).pin_memory()
+    h2d = sum(t.numel() * 4 for t in hm.values() if t is not None) + sig_pinned.numel() * 4 + sp.size * 4
+    d2h = 3 * eng.ntr * eng.ns * 4 * (1 if wl == "visco256" else 2)
+    ev2, ev3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    ev2.record(stream)
+    for _ in range(args.steps):
+        eng.set_model(*[None if hm[k] is None else hm[k].numpy() for k in ("rho", "pi", "u", "taus", "taup")],
+                      m["eta"], ghosted=True)
+        if wl == "elastic128":
+            eng.shot_gradient([(sp, sig_pinned.numpy())], obs)
+            eng.get_gradient()
+        else:
+            eng.forward([(sp, sig_pinned.numpy())], want_sections=True)
+    ev3.record(stream)
+    torch.cuda.synchronize(dev)
+    ms_e2e = ev2.elapsed_time(ev3)
+    if dist:
+        t = torch.tensor([ms_e2e], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    e2e = world * cells_step * args.steps / (ms_e2e / 1000.0) / 1e9
+    if wl == "elastic128":
+        d2h = 3 * eng.ntr * eng.ns * 4 + 3 * p.nx * p.ny * p.nz * 4
+
+    # ---- roofline: per-kernel CUDA events on the launching stream over one profiled step
+    eng.set_profiling(True)
+    eng.forward(shots, want_sections=False)
+    tv, ts, nsteps = eng.kernel_times()
+    eng.set_profiling(False)
+    b = alg_bytes_per_cell_step(p, nf if wl == "elastic128" else 0, c["ntast"])
+    ncell = p.nx * p.ny * p.nz
+    peak, peak_kind = load_peaks()
+    ach_step = b["total"] * ncell / ((tv + ts) / nsteps / 1000.0) / 1e9
+    ach_str = b["stress"] * ncell / (ts / nsteps / 1000.0) / 1e9
+    ach_vel = b["vel"] * ncell / (tv / nsteps / 1000.0) / 1e9
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tf):
+        try:
+            traffic = json.load(open(tf)).get(wl)
+        except Exception:
+            traffic = None
+    roofline = {"bound": "hbm", "kernel": "time step = k_velocity + k_stress<L> (one launch each)",
+                "achieved": round(ach_step, 1), "peak": peak, "unit": "GB/s", "frac": round(ach_step / peak, 4),
+                "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
+                "traffic": traffic, "alg_bytes_per_cell_step": round(b["total"], 2),
+                "per_kernel": {"k_stress": {"alg_bytes_per_cell": round(b["stress"], 2), "ms": round(ts / nsteps, 4),
+                                            "achieved_gbs": round(ach_str, 1), "frac": round(ach_str / peak, 4)},
+                               "k_velocity": {"alg_bytes_per_cell": round(b["vel"], 2), "ms": round(tv / nsteps, 4),
+                                              "achieved_gbs": round(ach_vel, 1), "frac": round(ach_vel / peak, 4)}}}
+
+    out = {
+        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 2), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": workload_config(wl, world), "clocks": clocks,
+        "e2e": {"value": round(e2e, 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": int(launches), "roofline": roofline,
+    }
+    if wl == "elastic128":
+        out["shot_gradients_per_s"] = round(world * args.steps / (ms / 1000.0), 4)
+
+    # ---- extras (rank 0, one GPU): batched vs one-shot-per-launch shot-gradients of elastic128
+    if rank == 0 and world == 1 and not args.no_extras:
+        eng.close()
+        out["shot_gradients"] = shot_gradient_comparison(torch, ifosb, synth, dev, stream, args.nt)
+    # ---- CPU baseline (rank 0, N=1): the oracle on a bounded sample of this workload
+    if rank == 0 and world == 1 and not args.no_cpu:
+        code, kind = cpu_kind(p.nmech)
+        grid, nt = (64, 64, 64), args.cpu_nt
+        v1, _, cells = cpu_run(code, p.nmech, 1, grid, nt)
+        out["cpu_baseline"] = {"value": round(v1, 5), "unit": UNIT, "cores": 1, "kind": kind,
+                               "sample": f"one core, {grid[0]}x{grid[1]}x{grid[2]} grid x {nt} steps of the "
+                                         f"same forward step (L={p.nmech}, FW=10 CPML, free surface)"}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def shot_gradient_comparison(torch, ifosb, synth, dev, stream, nt_override, nshots=4):
+    """elastic128 shot-gradients/s: the plain path (one shot per launch sequence,
+    kernel-by-kernel launches) against the batched path (all shots in one launch
+    per kernel, time loop replayed from a CUDA graph)."""
+    c = synth.case("elastic128", nt=nt_override)
+    p = c["params"]
+    base = c["shots"][0]
+    shots_sp = []
+    for s in range(nshots):
+        q = base.copy()
+        q[0, 0] = 40 + 16 * s
+        shots_sp.append(q)
+    c["shots"] = shots_sp
+    m, cp, shots = synth.build_inputs(c)
+    mt, _, _ = synth.build_inputs(c, "true")
+
+    def make(nb, mode):
+        e = ifosb.Engine(p, max_shots=nb, max_nf=len(c["finv"]))
+        e.set_stream(stream.cuda_stream)
+        e.set_launch_mode(mode)
+        e.set_cpml(cp)
+        e.set_receivers(c["recpos"])
+        e.set_frequencies(c["finv"], c["ntast"])
+        return e
+
+    eb = make(nshots, 0)
+    eb.set_model(mt["rho"], mt["pi"], mt["u"], mt["taus"], mt["taup"], mt["eta"])
+    obs = eb.forward(shots)
+    eb.set_model(m["rho"], m["pi"], m["u"], m["taus"], m["taup"], m["eta"])
+    eb.shot_gradient(shots, obs)  # warm-up (graph capture)
+    eb.zero_gradient()
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    eb.shot_gradient(shots, obs)
+    torch.cuda.synchronize(dev)
+    tb = time.perf_counter() - t0
+    gb = eb.get_gradient()
+    eb.close()
+    e1 = make(1, 1)
+    e1.set_model(m["rho"], m["pi"], m["u"], m["taus"], m["taup"], m["eta"])
+    e1.shot_gradient(shots[:1], obs[:1])  # warm-up
+    e1.zero_gradient()
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for s in range(nshots):
+        e1.shot_gradient(shots[s:s + 1], obs[s:s + 1])
+    torch.cuda.synchronize(dev)
+    t1 = time.perf_counter() - t0
+    g1 = e1.get_gradient()
+    e1.close()
+    return {"workload": f"elastic128, {nshots} shots, NT={p.nt}, nf=2", "batched_per_s": round(nshots / tb, 4),
+            "per_shot_per_s": round(nshots / t1, 4), "speedup": round(t1 / tb, 3),
+            "gcells_batched": round(2 * nshots * p.nx * p.ny * p.nz * p.nt / tb / 1e9, 3),
+            "gradients_bit_identical": bool(np.array_equal(gb, g1)), "timing": "host wall clock around synchronised calls"}
+
+
+if __name__ == "__main__":
+    main()

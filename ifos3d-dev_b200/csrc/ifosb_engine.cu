@@ -1,0 +1,823 @@
+// C-ABI implementation of the B200 wavefield engine (include/ifos_b200.h).
+//
+// One engine = one device-resident problem: the model (shared by all shots),
+// per-shot wavefield state, PML memory, DFT accumulators and traces for a
+// batch of up to max_shots shots, and the accumulated gradient. The time loops
+// run as two kernels per step (velocity; stress + source + DFT + surface +
+// receivers), captured once into a CUDA graph per batch shape and direction
+// and replayed on later calls.
+#include "../../include/ifos_b200.h"
+#include "ifosb_kernels.cuh"
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace ifosb;
+
+namespace {
+
+constexpr int DEFAULT_CY = 8;
+
+struct GraphCache {
+    cudaGraphExec_t exec = nullptr;
+    std::vector<unsigned char> key;
+};
+
+struct HostPt {
+    int s, j, i, k, kind, row;
+};
+
+}  // namespace
+
+struct ifosb_engine {
+    ifosb_params p{};
+    Geo g{};
+    Slabs sl{};
+    int max_shots = 0, max_nf = 0;
+    cudaStream_t stream = nullptr;
+    float b1 = 0.f, b2 = 0.f;
+    float eta[MAXMECH] = {0.f, 0.f, 0.f, 0.f};
+    // device memory
+    float *d_state = nullptr;  long long st_shot = 0;
+    float *d_psi = nullptr;    long long psi_shot = 0;
+    float *d_model = nullptr;  float *d_rho_w = nullptr;
+    float *d_dftf = nullptr, *d_dftb = nullptr; long long dft_shot = 0;
+    float *d_grad = nullptr;   double *d_grad64 = nullptr;
+    int *d_err = nullptr;
+    // receivers and traces
+    int ntr = 0, ns = 0;
+    std::vector<int> rec;
+    float *d_sec = nullptr, *d_diff = nullptr, *d_obs = nullptr;
+    double *d_part = nullptr, *d_misfit = nullptr;
+    float *d_l2 = nullptr;
+    // frequencies
+    int nf = 0, ntast = 1;
+    std::vector<float> finv;
+    double *d_trig_f = nullptr, *d_trig_b = nullptr;
+    // point lists (grow-only buffers)
+    int *d_voff = nullptr, *d_soff = nullptr; size_t cap_voff = 0, cap_soff = 0;
+    Pt *d_vpts = nullptr, *d_spts = nullptr;  size_t cap_vpts = 0, cap_spts = 0;
+    float *d_amp = nullptr;                   size_t cap_amp = 0;
+    // status
+    int nshots = 0;
+    bool have_model = false, have_cpml = false, fwd_ok = false, res_ok = false, adj_ok = false;
+    int launch_mode = 0;
+    long long launches = 0;
+    long long dev_bytes = 0;
+    GraphCache gfwd, gadj;
+    // kernel timing
+    int profile = 0;
+    double t_vel_ms = 0.0, t_str_ms = 0.0;
+    int t_steps = 0;
+    std::vector<cudaEvent_t> events;
+    cudaStream_t own_stream = nullptr;
+    std::string err;
+};
+
+// ---------------------------------------------------------------------------
+// helpers
+
+static int fail(ifosb_engine *e, int code, const std::string &msg) {
+    if (e) e->err = msg;
+    return code;
+}
+
+#define CU(call)                                                                                     \
+    do {                                                                                             \
+        cudaError_t _e = (call);                                                                     \
+        if (_e != cudaSuccess)                                                                       \
+            return fail(e, _e == cudaErrorMemoryAllocation ? IFOSB_ENOMEM : IFOSB_ECUDA,             \
+                        std::string(#call) + ": " + cudaGetErrorString(_e));                         \
+    } while (0)
+
+template <class T>
+static int dalloc(ifosb_engine *e, T **ptr, size_t count) {
+    if (count == 0) count = 1;
+    cudaError_t r = cudaMalloc((void **)ptr, count * sizeof(T));
+    if (r != cudaSuccess) {
+        *ptr = nullptr;
+        cudaGetLastError();
+        return fail(e, IFOSB_ENOMEM, "cudaMalloc of " + std::to_string(count * sizeof(T)) + " bytes failed");
+    }
+    e->dev_bytes += (long long)(count * sizeof(T));
+    return IFOSB_OK;
+}
+
+template <class T>
+static void dfree(ifosb_engine *e, T **ptr, size_t count) {
+    if (*ptr) {
+        cudaFree(*ptr);
+        e->dev_bytes -= (long long)(std::max<size_t>(count, 1) * sizeof(T));
+        *ptr = nullptr;
+    }
+}
+
+template <class T>
+static int dgrow(ifosb_engine *e, T **ptr, size_t *cap, size_t count) {
+    if (count <= *cap && *ptr) return IFOSB_OK;
+    dfree(e, ptr, *cap);
+    *cap = 0;
+    size_t want = std::max<size_t>(count, 16);
+    int rc = dalloc(e, ptr, want);
+    if (rc == IFOSB_OK) *cap = want;
+    return rc;
+}
+
+static void fd_coeffs(int fdcoeff, float *b1, float *b2) {
+    *b1 = 9.0 / 8.0; *b2 = -1.0 / 24.0;                  // Taylor (update_v_ssg.c:97)
+    if (fdcoeff == 2) { *b1 = 1.1382; *b2 = -0.046414; }  // Holberg (update_v_ssg.c:98-100)
+}
+
+static int nsamples(const ifosb_params *p) {
+    if (p->ndtshift > p->nt) return 0;
+    return (int)ceil((float)(p->nt - p->ndtshift) / (float)p->ndt);  // ifos3d.c:178-179
+}
+
+static void release_graph(GraphCache &gc) {
+    if (gc.exec) cudaGraphExecDestroy(gc.exec);
+    gc.exec = nullptr;
+    gc.key.clear();
+}
+
+static int check_launch(ifosb_engine *e, const char *what) {
+    cudaError_t le = cudaGetLastError();
+    if (le != cudaSuccess) return fail(e, IFOSB_ECUDA, std::string(what) + ": " + cudaGetErrorString(le));
+    return IFOSB_OK;
+}
+
+static int block_of(const Geo &g, int j, int i, int k) {
+    const int bx = (k - 1) / BX, by = (i - 1) / BY, yc = (j - 1) / g.cy;
+    return (yc * g.nti + by) * g.ntk + bx;
+}
+
+// Groups points per (shot, block), stable within a group (the reference's loop order).
+static int upload_points(ifosb_engine *e, int nshots, const std::vector<HostPt> &pts, int **d_off, size_t *cap_off,
+                         Pt **d_pts, size_t *cap_pts) {
+    const Geo &g = e->g;
+    const int nblk = g.ntk * g.nti * g.nyc;
+    std::vector<int> cnt((size_t)nshots * nblk, 0);
+    for (const HostPt &q : pts) cnt[(size_t)q.s * nblk + block_of(g, q.j, q.i, q.k)]++;
+    std::vector<int> off((size_t)nshots * (nblk + 1), 0), pos((size_t)nshots * nblk, 0);
+    int run = 0;
+    for (int s = 0; s < nshots; ++s) {
+        for (int b = 0; b < nblk; ++b) {
+            off[(size_t)s * (nblk + 1) + b] = run;
+            pos[(size_t)s * nblk + b] = run;
+            run += cnt[(size_t)s * nblk + b];
+        }
+        off[(size_t)s * (nblk + 1) + nblk] = run;
+    }
+    std::vector<Pt> out(pts.size());
+    for (const HostPt &q : pts) {
+        Pt t{};
+        t.j = q.j; t.i = q.i; t.k = q.k; t.kind = q.kind; t.row = q.row;
+        out[pos[(size_t)q.s * nblk + block_of(g, q.j, q.i, q.k)]++] = t;
+    }
+    int rc;
+    if ((rc = dgrow(e, d_off, cap_off, off.size())) || (rc = dgrow(e, d_pts, cap_pts, out.size()))) return rc;
+    CU(cudaMemcpyAsync(*d_off, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice, e->stream));
+    if (!out.empty()) CU(cudaMemcpyAsync(*d_pts, out.data(), out.size() * sizeof(Pt), cudaMemcpyHostToDevice, e->stream));
+    return IFOSB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// lifecycle
+
+extern "C" int ifosb_nsamples(const ifosb_params *p) { return p ? nsamples(p) : 0; }
+
+extern "C" int ifosb_create(const ifosb_params *p, int max_shots, int max_nf, ifosb_engine **out) {
+    if (!p || !out) return IFOSB_EARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return IFOSB_ENODEV;
+    }
+    if (p->fdorder != 4 || p->abs_type != 1 || p->nmech < 0 || p->nmech > MAXMECH || p->fw < 1 || p->fw > MAXFW ||
+        p->nx < 2 * p->fw + 1 || p->ny < 2 * p->fw + 1 || p->nz < 2 * p->fw + 1 || p->nt < 2 || p->ndt < 1 ||
+        p->ndtshift < 0 || max_shots < 1 || max_nf < 0 || max_nf > MAXNF || !(p->dt > 0.f) || !(p->dx > 0.f) ||
+        !(p->dy > 0.f) || !(p->dz > 0.f))
+        return IFOSB_EARG;
+    ifosb_engine *e = new ifosb_engine();
+    e->p = *p;
+    e->max_shots = max_shots;
+    e->max_nf = max_nf;
+    fd_coeffs(p->fdcoeff, &e->b1, &e->b2);
+    Geo &g = e->g;
+    g.nx = p->nx; g.ny = p->ny; g.nz = p->nz; g.fw = p->fw; g.free_surf = p->free_surf ? 1 : 0; g.nmech = p->nmech;
+    g.pz = ((p->nz + 10) + 7) / 8 * 8;
+    g.px = p->nx + 4;
+    g.plane = (long long)g.px * g.pz;
+    g.field = (long long)(p->ny + 5) * g.plane;
+    g.cy = DEFAULT_CY;
+    g.nyc = (p->ny + g.cy - 1) / g.cy;
+    g.ntk = (p->nz + BX - 1) / BX;
+    g.nti = (p->nx + BY - 1) / BY;
+    if ((long long)g.nyc * max_shots > 65535) { delete e; return IFOSB_EARG; }
+    e->sl.sx = (long long)p->ny * 2 * p->fw * p->nz;
+    e->sl.sy = (long long)2 * p->fw * p->nx * p->nz;
+    e->sl.sz = (long long)p->ny * p->nx * 2 * p->fw;
+    e->st_shot = (long long)(NEL + 6 * p->nmech) * g.field;
+    e->psi_shot = 6 * (e->sl.sx + e->sl.sy + e->sl.sz);
+    e->dft_shot = (long long)max_nf * 6 * g.field;
+    if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        delete e;
+        return IFOSB_ECUDA;
+    }
+    e->own_stream = e->stream;
+    const long long ncell = (long long)p->nx * p->ny * p->nz;
+    int rc;
+    if ((rc = dalloc(e, &e->d_state, (size_t)(e->st_shot * max_shots))) ||
+        (rc = dalloc(e, &e->d_psi, (size_t)(e->psi_shot * max_shots))) ||
+        (rc = dalloc(e, &e->d_model, (size_t)(NMODEL * g.field))) ||
+        (rc = dalloc(e, &e->d_rho_w, (size_t)g.field)) ||
+        (rc = dalloc(e, &e->d_grad, (size_t)(3 * ncell))) ||
+        (rc = dalloc(e, &e->d_grad64, (size_t)(3 * ncell))) ||
+        (rc = dalloc(e, &e->d_err, (size_t)max_shots))) {
+        ifosb_destroy(e);
+        return rc;
+    }
+    if (max_nf > 0) {
+        if ((rc = dalloc(e, &e->d_dftf, (size_t)(e->dft_shot * max_shots))) ||
+            (rc = dalloc(e, &e->d_dftb, (size_t)(e->dft_shot * max_shots)))) {
+            ifosb_destroy(e);
+            return rc;
+        }
+    }
+    // halos and row padding of every field stay zero for the engine's lifetime
+    cudaMemsetAsync(e->d_model, 0, sizeof(float) * NMODEL * g.field, e->stream);
+    cudaMemsetAsync(e->d_rho_w, 0, sizeof(float) * g.field, e->stream);
+    cudaMemsetAsync(e->d_grad, 0, sizeof(float) * 3 * ncell, e->stream);
+    cudaMemsetAsync(e->d_grad64, 0, sizeof(double) * 3 * ncell, e->stream);
+    if (cudaStreamSynchronize(e->stream) != cudaSuccess) {
+        cudaGetLastError();
+        ifosb_destroy(e);
+        return IFOSB_ECUDA;
+    }
+    *out = e;
+    return IFOSB_OK;
+}
+
+extern "C" void ifosb_destroy(ifosb_engine *e) {
+    if (!e) return;
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    release_graph(e->gfwd);
+    release_graph(e->gadj);
+    void *bufs[] = {e->d_state, e->d_psi, e->d_model, e->d_rho_w, e->d_dftf, e->d_dftb, e->d_grad, e->d_grad64,
+                    e->d_err, e->d_sec, e->d_diff, e->d_obs, e->d_part, e->d_misfit, e->d_l2, e->d_trig_f,
+                    e->d_trig_b, e->d_voff, e->d_soff, e->d_vpts, e->d_spts, e->d_amp};
+    for (void *b : bufs)
+        if (b) cudaFree(b);
+    for (cudaEvent_t ev : e->events) cudaEventDestroy(ev);
+    if (e->own_stream) cudaStreamDestroy(e->own_stream);
+    delete e;
+}
+
+extern "C" int ifosb_set_profiling(ifosb_engine *e, int profile) {
+    if (!e) return IFOSB_EARG;
+    e->profile = profile ? 1 : 0;
+    return IFOSB_OK;
+}
+
+extern "C" int ifosb_kernel_times(const ifosb_engine *e, double *vel_ms, double *str_ms, int *steps) {
+    if (!e) return IFOSB_EARG;
+    if (vel_ms) *vel_ms = e->t_vel_ms;
+    if (str_ms) *str_ms = e->t_str_ms;
+    if (steps) *steps = e->t_steps;
+    return IFOSB_OK;
+}
+
+extern "C" int ifosb_set_stream(ifosb_engine *e, void *stream) {
+    if (!e) return IFOSB_EARG;
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    e->stream = stream ? (cudaStream_t)stream : e->own_stream;
+    release_graph(e->gfwd);
+    release_graph(e->gadj);
+    return IFOSB_OK;
+}
+
+extern "C" const char *ifosb_last_error(const ifosb_engine *e) { return e ? e->err.c_str() : "no engine"; }
+extern "C" long long ifosb_device_bytes(const ifosb_engine *e) { return e ? e->dev_bytes : 0; }
+extern "C" long long ifosb_last_launch_count(const ifosb_engine *e) { return e ? e->launches : 0; }
+
+extern "C" int ifosb_set_launch_mode(ifosb_engine *e, int mode) {
+    if (!e || (mode != 0 && mode != 1)) return IFOSB_EARG;
+    e->launch_mode = mode;
+    return IFOSB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// static inputs
+
+extern "C" int ifosb_set_cpml(ifosb_engine *e, const float *coeff) {
+    if (!e || !coeff) return IFOSB_EARG;
+    std::vector<float> host((size_t)18 * 2 * MAXFW, 0.f);
+    const int n2 = 2 * e->p.fw;
+    for (int r = 0; r < 18; ++r)
+        for (int h = 0; h < n2; ++h) host[(size_t)r * 2 * MAXFW + h] = coeff[(size_t)r * n2 + h];
+    CU(cudaMemcpyToSymbol(c_cpml, host.data(), host.size() * sizeof(float)));
+    e->have_cpml = true;
+    return IFOSB_OK;
+}
+
+extern "C" int ifosb_set_model(ifosb_engine *e, const float *rho, const float *pi, const float *u, const float *taus,
+                               const float *taup, const float *eta) {
+    if (!e || !rho || !pi || !u) return IFOSB_EARG;
+    const ifosb_params &p = e->p;
+    if (p.nmech > 0 && (!taus || !taup || !eta)) return fail(e, IFOSB_EARG, "viscoelastic model needs taus, taup, eta");
+    const size_t ng = (size_t)(p.nx + 2) * (p.ny + 2) * (p.nz + 2);
+    for (size_t q = 0; q < ng; ++q)
+        if (!(rho[q] > 0.f) || !(u[q] > 0.f) || !(pi[q] > 0.f) || !std::isfinite(rho[q]) || !std::isfinite(u[q]) ||
+            !std::isfinite(pi[q]))
+            return fail(e, IFOSB_EARG, "model value not positive and finite at ghosted index " + std::to_string(q));
+    for (int l = 0; l < p.nmech; ++l)
+        if (!std::isfinite(eta[l])) return fail(e, IFOSB_EARG, "eta not finite");
+    float *tmp = nullptr;
+    int rc = dalloc(e, &tmp, ng * 5);
+    if (rc) return rc;
+    CU(cudaMemcpyAsync(tmp, rho, ng * sizeof(float), cudaMemcpyHostToDevice, e->stream));
+    CU(cudaMemcpyAsync(tmp + ng, pi, ng * sizeof(float), cudaMemcpyHostToDevice, e->stream));
+    CU(cudaMemcpyAsync(tmp + 2 * ng, u, ng * sizeof(float), cudaMemcpyHostToDevice, e->stream));
+    if (p.nmech > 0) {
+        CU(cudaMemcpyAsync(tmp + 3 * ng, taus, ng * sizeof(float), cudaMemcpyHostToDevice, e->stream));
+        CU(cudaMemcpyAsync(tmp + 4 * ng, taup, ng * sizeof(float), cudaMemcpyHostToDevice, e->stream));
+    }
+    AvArgs a{};
+    a.g = e->g;
+    a.rho = tmp; a.pi = tmp + ng; a.u = tmp + 2 * ng; a.taus = tmp + 3 * ng; a.taup = tmp + 4 * ng;
+    a.md = e->d_model;
+    a.rho_w = e->d_rho_w;
+    dim3 blk(32, 4), grd((p.nz + 31) / 32, (p.nx + 3) / 4, p.ny);
+    k_av_mat<<<grd, blk, 0, e->stream>>>(a);
+    cudaError_t le = cudaGetLastError();
+    cudaError_t se = cudaStreamSynchronize(e->stream);
+    dfree(e, &tmp, ng * 5);
+    if (le != cudaSuccess || se != cudaSuccess)
+        return fail(e, IFOSB_ECUDA, std::string("av_mat: ") + cudaGetErrorString(le != cudaSuccess ? le : se));
+    for (int l = 0; l < MAXMECH; ++l) e->eta[l] = l < p.nmech ? eta[l] : 0.f;
+    e->have_model = true;
+    e->fwd_ok = e->res_ok = e->adj_ok = false;
+    return IFOSB_OK;
+}
+
+extern "C" int ifosb_set_receivers(ifosb_engine *e, int ntr, const int *recpos) {
+    if (!e || ntr < 0 || (ntr > 0 && !recpos)) return IFOSB_EARG;
+    const ifosb_params &p = e->p;
+    for (int t = 0; t < ntr; ++t) {
+        const int i = recpos[3 * t], j = recpos[3 * t + 1], k = recpos[3 * t + 2];
+        if (i < 1 || i > p.nx || j < 1 || j > p.ny || k < 1 || k > p.nz)
+            return fail(e, IFOSB_EARG, "receiver " + std::to_string(t) + " outside the grid");
+    }
+    const int ns = nsamples(&p);
+    const size_t secn = (size_t)e->max_shots * 3 * std::max(ntr, 1) * std::max(ns, 1);
+    dfree(e, &e->d_sec, e->ntr ? (size_t)e->max_shots * 3 * e->ntr * e->ns : 0);
+    dfree(e, &e->d_diff, e->ntr ? (size_t)e->max_shots * 3 * e->ntr * e->ns : 0);
+    dfree(e, &e->d_obs, e->ntr ? (size_t)e->max_shots * 3 * e->ntr * e->ns : 0);
+    dfree(e, &e->d_part, e->ntr ? (size_t)e->max_shots * 3 * e->ntr : 0);
+    dfree(e, &e->d_misfit, (size_t)e->max_shots);
+    dfree(e, &e->d_l2, (size_t)e->max_shots);
+    e->ntr = 0;
+    int rc;
+    if ((rc = dalloc(e, &e->d_sec, secn)) || (rc = dalloc(e, &e->d_diff, secn)) || (rc = dalloc(e, &e->d_obs, secn)) ||
+        (rc = dalloc(e, &e->d_part, (size_t)e->max_shots * 3 * std::max(ntr, 1))) ||
+        (rc = dalloc(e, &e->d_misfit, (size_t)e->max_shots)) || (rc = dalloc(e, &e->d_l2, (size_t)e->max_shots)))
+        return rc;
+    CU(cudaMemsetAsync(e->d_sec, 0, secn * sizeof(float), e->stream));
+    e->ntr = ntr;
+    e->ns = ns;
+    e->rec.assign(recpos, recpos + 3 * ntr);
+    e->fwd_ok = e->res_ok = e->adj_ok = false;
+    release_graph(e->gfwd);
+    release_graph(e->gadj);
+    CU(cudaStreamSynchronize(e->stream));
+    return IFOSB_OK;
+}
+
+// Trig tables of discfourier (disc_fourier.c:36-45), in double as the reference.
+static void trig_table(const ifosb_params &p, int nf, const float *finv, int ntast, int back, std::vector<double> &out) {
+    out.assign((size_t)p.nt * nf * 2, 0.0);
+    for (int nt = 1; nt <= p.nt; ++nt) {
+        float t = 0.0;
+        if (back == 0) t = nt * p.dt;
+        if (back == 1) t = p.time - nt * p.dt;
+        for (int l = 0; l < nf; ++l) {
+            out[((size_t)(nt - 1) * nf + l) * 2 + 0] = cos(2.0 * t * finv[l] * M_PI) * p.dt * ntast;
+            out[((size_t)(nt - 1) * nf + l) * 2 + 1] = sin(2.0 * t * finv[l] * M_PI) * p.dt * ntast;
+        }
+    }
+}
+
+extern "C" int ifosb_set_frequencies(ifosb_engine *e, int nf, const float *finv, int ntast) {
+    if (!e || nf < 0 || nf > e->max_nf || (nf > 0 && (!finv || ntast < 1))) return IFOSB_EARG;
+    for (int l = 0; l < nf; ++l)
+        if (!(finv[l] > 0.f)) return fail(e, IFOSB_EARG, "frequency must be positive");
+    const ifosb_params &p = e->p;
+    dfree(e, &e->d_trig_f, (size_t)p.nt * e->nf * 2);
+    dfree(e, &e->d_trig_b, (size_t)p.nt * e->nf * 2);
+    e->nf = 0;
+    if (nf > 0) {
+        std::vector<double> tf, tb;
+        trig_table(p, nf, finv, ntast, 0, tf);
+        trig_table(p, nf, finv, ntast, 1, tb);
+        int rc;
+        if ((rc = dalloc(e, &e->d_trig_f, tf.size())) || (rc = dalloc(e, &e->d_trig_b, tb.size()))) return rc;
+        CU(cudaMemcpy(e->d_trig_f, tf.data(), tf.size() * sizeof(double), cudaMemcpyHostToDevice));
+        CU(cudaMemcpy(e->d_trig_b, tb.data(), tb.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    e->nf = nf;
+    e->ntast = nf > 0 ? ntast : 1;
+    e->finv.assign(finv, finv + nf);
+    e->fwd_ok = e->res_ok = e->adj_ok = false;
+    release_graph(e->gfwd);
+    release_graph(e->gadj);
+    return IFOSB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// the time loop
+
+static void fill_common(ifosb_engine *e, VelArgs &va, StrArgs &sa) {
+    const ifosb_params &p = e->p;
+    va = VelArgs{};
+    sa = StrArgs{};
+    va.g = sa.g = e->g;
+    va.sl = sa.sl = e->sl;
+    va.st = sa.st = e->d_state;
+    va.st_shot = sa.st_shot = e->st_shot;
+    va.md = sa.md = e->d_model;
+    va.psi = sa.psi = e->d_psi;
+    va.psi_shot = sa.psi_shot = e->psi_shot;
+    va.dxr = p.dt / p.dx; va.dyr = p.dt / p.dy; va.dzr = p.dt / p.dz;
+    va.b1 = sa.b1 = e->b1;
+    va.b2 = sa.b2 = e->b2;
+    {
+        // custom force direction factors (update_v_ssg.c:498-503); the reference is C,
+        // so cos/sin of its float angles run in double (C++ would pick the float overloads)
+        const float alpha_rad = p.alpha * 3.141592653589793 / 180, beta_rad = p.beta * 3.141592653589793 / 180;
+        const double ca = std::cos((double)alpha_rad), sa = std::sin((double)alpha_rad);
+        const double cb = std::cos((double)beta_rad), sb = std::sin((double)beta_rad);
+        va.cf5x = cb * ca;
+        va.cf5y = sa;
+        va.cf5z = sb * ca;
+    }
+    va.err_step = e->d_err;
+    va.probe_j = p.ny / 2; va.probe_i = p.nx / 2; va.probe_k = p.nz / 2;  // ifos3d.c:761
+    sa.dt = p.dt;
+    sa.dthalbe = p.dt / 2.0;
+    sa.rdx = p.dx; sa.rdy = p.dy; sa.rdz = p.dz;
+    for (int l = 0; l < MAXMECH; ++l) {
+        const float eta = e->eta[l];
+        sa.eta[l] = eta;
+        sa.mb[l] = 1.0 / (1.0 + (eta * 0.5));      // update_s_ssg.c:123
+        sa.mc[l] = 1.0 - (eta * 0.5);              // update_s_ssg.c:124
+        sa.msb[l] = eta / (1.0 + (eta * 0.5));     // surface_ssg.c:152
+    }
+    sa.sec = e->d_sec;
+    sa.sec_tr = e->ns;
+    sa.sec_comp = (long long)e->ntr * e->ns;
+    sa.sec_shot = 3 * sa.sec_comp;
+    sa.nf = e->nf;
+    sa.dft_shot = e->dft_shot;
+}
+
+template <int L>
+static void launch_stress(dim3 grd, dim3 blk, cudaStream_t st, const StrArgs &sa, int nt, int do_dft, int sample) {
+    k_stress<L><<<grd, blk, 0, st>>>(sa, nt, do_dft, sample);
+}
+
+static void launch_step_stress(int nmech, dim3 grd, dim3 blk, cudaStream_t st, const StrArgs &sa, int nt, int do_dft,
+                               int sample) {
+    switch (nmech) {
+    case 0: launch_stress<0>(grd, blk, st, sa, nt, do_dft, sample); break;
+    case 1: launch_stress<1>(grd, blk, st, sa, nt, do_dft, sample); break;
+    case 2: launch_stress<2>(grd, blk, st, sa, nt, do_dft, sample); break;
+    case 3: launch_stress<3>(grd, blk, st, sa, nt, do_dft, sample); break;
+    default: launch_stress<4>(grd, blk, st, sa, nt, do_dft, sample); break;
+    }
+}
+
+// Enqueue the NT steps (two kernels per step) on the engine stream.
+static void enqueue_loop(ifosb_engine *e, bool back, const VelArgs &va, const StrArgs &sa, int nshots) {
+    const ifosb_params &p = e->p;
+    dim3 blk(BX, BY), grd(e->g.ntk, e->g.nti, e->g.nyc * nshots);
+    int lsamp = p.ndtshift + 1, nlsamp = 0;
+    for (int nt = 1; nt <= p.nt; ++nt) {
+        if (back) k_velocity<true><<<grd, blk, 0, e->stream>>>(va, nt);
+        else k_velocity<false><<<grd, blk, 0, e->stream>>>(va, nt);
+        const int do_dft = (e->nf > 0 && nt % e->ntast == 0) ? 1 : 0;
+        int sample = -1;
+        if (!back && nt == lsamp) {
+            sample = nlsamp++;
+            lsamp += p.ndt;
+        }
+        launch_step_stress(p.nmech, grd, blk, e->stream, sa, nt, do_dft, sample);
+    }
+}
+
+// Kernel-by-kernel launches with an event pair around each kernel (kernel timing).
+static int run_loop_profiled(ifosb_engine *e, bool back, const VelArgs &va, const StrArgs &sa, int nshots) {
+    const ifosb_params &p = e->p;
+    const size_t need = (size_t)3 * p.nt;
+    while (e->events.size() < need) {
+        cudaEvent_t ev;
+        CU(cudaEventCreate(&ev));
+        e->events.push_back(ev);
+    }
+    dim3 blk(BX, BY), grd(e->g.ntk, e->g.nti, e->g.nyc * nshots);
+    int lsamp = p.ndtshift + 1, nlsamp = 0;
+    for (int nt = 1; nt <= p.nt; ++nt) {
+        cudaEvent_t *ev = &e->events[(size_t)3 * (nt - 1)];
+        CU(cudaEventRecord(ev[0], e->stream));
+        if (back) k_velocity<true><<<grd, blk, 0, e->stream>>>(va, nt);
+        else k_velocity<false><<<grd, blk, 0, e->stream>>>(va, nt);
+        CU(cudaEventRecord(ev[1], e->stream));
+        const int do_dft = (e->nf > 0 && nt % e->ntast == 0) ? 1 : 0;
+        int sample = -1;
+        if (!back && nt == lsamp) {
+            sample = nlsamp++;
+            lsamp += p.ndt;
+        }
+        launch_step_stress(p.nmech, grd, blk, e->stream, sa, nt, do_dft, sample);
+        CU(cudaEventRecord(ev[2], e->stream));
+    }
+    int rc = check_launch(e, "time loop");
+    if (rc) return rc;
+    CU(cudaStreamSynchronize(e->stream));
+    double tv = 0.0, ts = 0.0;
+    for (int nt = 1; nt <= p.nt; ++nt) {
+        cudaEvent_t *ev = &e->events[(size_t)3 * (nt - 1)];
+        float a = 0.f, b = 0.f;
+        CU(cudaEventElapsedTime(&a, ev[0], ev[1]));
+        CU(cudaEventElapsedTime(&b, ev[1], ev[2]));
+        tv += a;
+        ts += b;
+    }
+    e->t_vel_ms = tv;
+    e->t_str_ms = ts;
+    e->t_steps = p.nt;
+    return IFOSB_OK;
+}
+
+static int run_loop(ifosb_engine *e, bool back, const VelArgs &va, const StrArgs &sa, int nshots) {
+    GraphCache &gc = back ? e->gadj : e->gfwd;
+    e->launches = 2LL * e->p.nt;
+    if (e->profile) return run_loop_profiled(e, back, va, sa, nshots);
+    if (e->launch_mode == 1) {
+        enqueue_loop(e, back, va, sa, nshots);
+        return check_launch(e, "time loop");
+    }
+    std::vector<unsigned char> key(sizeof(VelArgs) + sizeof(StrArgs) + sizeof(int));
+    std::memcpy(key.data(), &va, sizeof(VelArgs));
+    std::memcpy(key.data() + sizeof(VelArgs), &sa, sizeof(StrArgs));
+    std::memcpy(key.data() + sizeof(VelArgs) + sizeof(StrArgs), &nshots, sizeof(int));
+    if (!gc.exec || gc.key != key) {
+        release_graph(gc);
+        cudaGraph_t graph = nullptr;
+        CU(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+        enqueue_loop(e, back, va, sa, nshots);
+        cudaError_t ce = cudaStreamEndCapture(e->stream, &graph);
+        if (ce != cudaSuccess) {
+            cudaGetLastError();
+            return fail(e, IFOSB_ECUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+        }
+        ce = cudaGraphInstantiate(&gc.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ce != cudaSuccess) {
+            gc.exec = nullptr;
+            cudaGetLastError();
+            return fail(e, IFOSB_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
+        }
+        gc.key = key;
+    }
+    CU(cudaGraphLaunch(gc.exec, e->stream));
+    return IFOSB_OK;
+}
+
+static int check_unstable(ifosb_engine *e, int nshots) {
+    std::vector<int> errs(nshots);
+    CU(cudaMemcpyAsync(errs.data(), e->d_err, sizeof(int) * nshots, cudaMemcpyDeviceToHost, e->stream));
+    CU(cudaStreamSynchronize(e->stream));
+    for (int s = 0; s < nshots; ++s)
+        if (errs[s] != INT_MAX)
+            return fail(e, IFOSB_EUNSTABLE,
+                        " Simulation is unstable ! (shot " + std::to_string(s) + ", step " + std::to_string(errs[s]) + ")");
+    return IFOSB_OK;
+}
+
+static int reset_state(ifosb_engine *e, int nshots, float *dft) {
+    CU(cudaMemsetAsync(e->d_state, 0, sizeof(float) * e->st_shot * nshots, e->stream));       // zero_wavefield
+    CU(cudaMemsetAsync(e->d_psi, 0, sizeof(float) * e->psi_shot * nshots, e->stream));
+    if (dft && e->nf > 0) CU(cudaMemsetAsync(dft, 0, sizeof(float) * e->dft_shot * nshots, e->stream));  // zero_invers
+    std::vector<int> init(nshots, INT_MAX);
+    CU(cudaMemcpyAsync(e->d_err, init.data(), sizeof(int) * nshots, cudaMemcpyHostToDevice, e->stream));
+    CU(cudaStreamSynchronize(e->stream));  // init lives on the host stack
+    return IFOSB_OK;
+}
+
+// psource.c:38-52, the explosive-source amplitude at step nt
+static float psource_amp(const ifosb_params &p, const float *s, int nt) {
+    float amp = 0.0;
+    if (nt == 1) amp = s[nt + 1 - 1] / (2.0 * p.dx * p.dy * p.dz);
+    if ((nt > 1) && (nt < p.nt)) amp = (s[nt + 1 - 1] - s[nt - 1 - 1]) / (2.0 * p.dx * p.dy * p.dz);
+    if (nt == p.nt) amp = -s[nt - 1 - 1] / (2.0 * p.dx * p.dy * p.dz);
+    return amp;
+}
+
+extern "C" int ifosb_forward(ifosb_engine *e, int nshots, const ifosb_shot *shots, float *sections) {
+    if (!e || !shots || nshots < 1 || nshots > e->max_shots) return IFOSB_EARG;
+    if (!e->have_model || !e->have_cpml) return fail(e, IFOSB_ESTATE, "set the model and the CPML profiles first");
+    const ifosb_params &p = e->p;
+    // point lists: forces (velocity kernel), explosive sources and receivers (stress kernel)
+    std::vector<HostPt> vp, sp;
+    std::vector<float> amp;
+    int row = 0;
+    for (int s = 0; s < nshots; ++s) {
+        const ifosb_shot &sh = shots[s];
+        if (sh.nsrc < 0 || (sh.nsrc > 0 && (!sh.srcpos || !sh.signals))) return IFOSB_EARG;
+        for (int l = 0; l < sh.nsrc; ++l) {
+            const float *sp7 = sh.srcpos + 7 * l;
+            const int i = (int)sp7[0], j = (int)sp7[1], k = (int)sp7[2], kind = (int)sp7[6];
+            if (i < 1 || i > p.nx || j < 1 || j > p.ny || k < 1 || k > p.nz)
+                return fail(e, IFOSB_EARG, "source outside the grid");
+            const float *sig = sh.signals + (size_t)l * p.nt;
+            if (kind == 1) {
+                for (int nt = 1; nt <= p.nt; ++nt) amp.push_back(psource_amp(p, sig, nt));
+                sp.push_back({s, j, i, k, 1, row++});
+            } else if (kind >= 2 && kind <= 5) {
+                // update_v_ssg.c:480: amp = DT*signals[l][nt]/(DX*DY*DZ)
+                for (int nt = 1; nt <= p.nt; ++nt) amp.push_back(p.dt * sig[nt - 1] / (p.dx * p.dy * p.dz));
+                vp.push_back({s, j, i, k, kind, row++});
+            }
+        }
+        for (int t = 0; t < e->ntr; ++t) sp.push_back({s, e->rec[3 * t + 1], e->rec[3 * t], e->rec[3 * t + 2], PT_RECEIVER, t});
+    }
+    int rc;
+    if ((rc = upload_points(e, nshots, vp, &e->d_voff, &e->cap_voff, &e->d_vpts, &e->cap_vpts)) ||
+        (rc = upload_points(e, nshots, sp, &e->d_soff, &e->cap_soff, &e->d_spts, &e->cap_spts)) ||
+        (rc = dgrow(e, &e->d_amp, &e->cap_amp, amp.size())))
+        return rc;
+    if (!amp.empty()) CU(cudaMemcpyAsync(e->d_amp, amp.data(), amp.size() * sizeof(float), cudaMemcpyHostToDevice, e->stream));
+    if ((rc = reset_state(e, nshots, e->d_dftf))) return rc;
+    VelArgs va;
+    StrArgs sa;
+    fill_common(e, va, sa);
+    va.pt_off = vp.empty() ? nullptr : e->d_voff;
+    va.pts = e->d_vpts;
+    va.val = e->d_amp;
+    va.val_row = p.nt;
+    va.val_comp = 0;
+    sa.pt_off = sp.empty() ? nullptr : e->d_soff;
+    sa.pts = e->d_spts;
+    sa.amp = e->d_amp;
+    sa.amp_row = p.nt;
+    sa.dft = e->d_dftf;
+    sa.trig = e->d_trig_f;
+    if ((rc = run_loop(e, false, va, sa, nshots))) return rc;
+    e->nshots = nshots;
+    e->fwd_ok = true;
+    e->res_ok = e->adj_ok = false;
+    if ((rc = check_unstable(e, nshots))) return rc;
+    if (sections && e->ntr > 0)
+        CU(cudaMemcpy(sections, e->d_sec, sizeof(float) * (size_t)nshots * 3 * e->ntr * e->ns, cudaMemcpyDeviceToHost));
+    return check_launch(e, "forward");
+}
+
+extern "C" int ifosb_residual(ifosb_engine *e, const float *obs, double *misfit_fp64, float *l2_ref) {
+    if (!e || !obs) return IFOSB_EARG;
+    if (!e->fwd_ok || e->ntr == 0) return fail(e, IFOSB_ESTATE, "residual needs a forward batch with receivers");
+    const int nshots = e->nshots, ntr = e->ntr, ns = e->ns;
+    const size_t n = (size_t)nshots * 3 * ntr * ns;
+    CU(cudaMemcpyAsync(e->d_obs, obs, n * sizeof(float), cudaMemcpyHostToDevice, e->stream));
+    const int nthr = nshots * 3 * ntr;
+    k_residual<<<(nthr + 127) / 128, 128, 0, e->stream>>>(e->d_sec, e->d_obs, e->d_diff, e->d_part, nshots, ntr, ns, e->p.dt);
+    k_misfit<<<nshots, 32, 0, e->stream>>>(e->d_part, e->d_misfit, 3 * ntr);
+    if (l2_ref) k_l2_ref<<<(nshots + 31) / 32, 32, 0, e->stream>>>(e->d_diff, e->d_l2, nshots, ntr, ns);
+    int rc = check_launch(e, "residual");
+    if (rc) return rc;
+    if (misfit_fp64) CU(cudaMemcpyAsync(misfit_fp64, e->d_misfit, sizeof(double) * nshots, cudaMemcpyDeviceToHost, e->stream));
+    if (l2_ref) CU(cudaMemcpyAsync(l2_ref, e->d_l2, sizeof(float) * nshots, cudaMemcpyDeviceToHost, e->stream));
+    CU(cudaStreamSynchronize(e->stream));
+    e->res_ok = true;
+    e->adj_ok = false;
+    return IFOSB_OK;
+}
+
+extern "C" int ifosb_adjoint(ifosb_engine *e, const float *diff) {
+    if (!e) return IFOSB_EARG;
+    const ifosb_params &p = e->p;
+    if (!e->fwd_ok) return fail(e, IFOSB_ESTATE, "adjoint needs a forward batch");
+    if (!diff && !e->res_ok) return fail(e, IFOSB_ESTATE, "adjoint needs ifosb_residual or a caller residual");
+    if (p.ndt != 1 || p.ndtshift != 0)
+        return fail(e, IFOSB_EARG, "the adjoint indexes the residual by time step: NDT=1, NDTSHIFT=0 (update_v_ssg.c:518)");
+    if (e->nf == 0) return fail(e, IFOSB_ESTATE, "adjoint needs DFT frequencies");
+    const int nshots = e->nshots, ntr = e->ntr, ns = e->ns;
+    if (diff) CU(cudaMemcpyAsync(e->d_diff, diff, sizeof(float) * (size_t)nshots * 3 * ntr * ns, cudaMemcpyHostToDevice, e->stream));
+    std::vector<HostPt> vp;
+    for (int s = 0; s < nshots; ++s)
+        for (int t = 0; t < ntr; ++t) vp.push_back({s, e->rec[3 * t + 1], e->rec[3 * t], e->rec[3 * t + 2], PT_ADJOINT, s * 3 * ntr + t});
+    int rc;
+    if ((rc = upload_points(e, nshots, vp, &e->d_voff, &e->cap_voff, &e->d_vpts, &e->cap_vpts))) return rc;
+    if ((rc = reset_state(e, nshots, e->d_dftb))) return rc;
+    VelArgs va;
+    StrArgs sa;
+    fill_common(e, va, sa);
+    va.pt_off = vp.empty() ? nullptr : e->d_voff;
+    va.pts = e->d_vpts;
+    va.val = e->d_diff;
+    va.val_row = ns;
+    va.val_comp = (long long)ntr * ns;
+    sa.pt_off = nullptr;
+    sa.pts = nullptr;
+    sa.dft = e->d_dftb;
+    sa.trig = e->d_trig_b;
+    if ((rc = run_loop(e, true, va, sa, nshots))) return rc;
+    if ((rc = check_unstable(e, nshots))) return rc;
+    e->adj_ok = true;
+    return check_launch(e, "adjoint");
+}
+
+extern "C" int ifosb_gradient(ifosb_engine *e) {
+    if (!e) return IFOSB_EARG;
+    if (!e->adj_ok) return fail(e, IFOSB_ESTATE, "gradient needs a forward and an adjoint batch");
+    const ifosb_params &p = e->p;
+    GradArgs a{};
+    a.g = e->g;
+    a.dftf = e->d_dftf;
+    a.dftb = e->d_dftb;
+    a.dft_shot = e->dft_shot;
+    a.nshots = e->nshots;
+    a.nf = e->nf;
+    a.md = e->d_model;
+    a.rho = e->d_rho_w;
+    for (int l = 0; l < e->nf; ++l) {
+        float fdummy = 0.0;
+        fdummy = 2.0 * 2.0 * e->finv[l] * e->finv[l] * M_PI * M_PI;  // gradient_F.c:70-72
+        fdummy = 1 / fdummy;
+        a.fdummy[l] = fdummy;
+    }
+    a.b1 = e->b1; a.b2 = e->b2;
+    a.rdx = p.dx; a.rdy = p.dy; a.rdz = p.dz;
+    a.grad = e->d_grad;
+    a.grad64 = e->d_grad64;
+    dim3 blk(BX, BY), grd(e->g.ntk, e->g.nti, e->g.nyc);
+    k_gradient<<<grd, blk, 0, e->stream>>>(a);
+    int rc = check_launch(e, "gradient");
+    if (rc) return rc;
+    CU(cudaStreamSynchronize(e->stream));
+    e->adj_ok = false;  // one gradient contribution per adjoint batch
+    return IFOSB_OK;
+}
+
+extern "C" int ifosb_zero_gradient(ifosb_engine *e) {
+    if (!e) return IFOSB_EARG;
+    const size_t n = (size_t)3 * e->p.nx * e->p.ny * e->p.nz;
+    CU(cudaMemsetAsync(e->d_grad, 0, n * sizeof(float), e->stream));
+    CU(cudaMemsetAsync(e->d_grad64, 0, n * sizeof(double), e->stream));
+    CU(cudaStreamSynchronize(e->stream));
+    return IFOSB_OK;
+}
+
+extern "C" int ifosb_get_gradient(ifosb_engine *e, float *grad, double *grad64) {
+    if (!e) return IFOSB_EARG;
+    const size_t n = (size_t)3 * e->p.nx * e->p.ny * e->p.nz;
+    if (grad) CU(cudaMemcpyAsync(grad, e->d_grad, n * sizeof(float), cudaMemcpyDeviceToHost, e->stream));
+    if (grad64) CU(cudaMemcpyAsync(grad64, e->d_grad64, n * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+    CU(cudaStreamSynchronize(e->stream));
+    return IFOSB_OK;
+}
+
+extern "C" int ifosb_shot_gradient(ifosb_engine *e, int nshots, const ifosb_shot *shots, const float *obs, double *misfit) {
+    int rc;
+    if ((rc = ifosb_forward(e, nshots, shots, nullptr))) return rc;
+    if ((rc = ifosb_residual(e, obs, misfit, nullptr))) return rc;
+    if ((rc = ifosb_adjoint(e, nullptr))) return rc;
+    return ifosb_gradient(e);
+}
+
+extern "C" int ifosb_get_field(ifosb_engine *e, int shot, int field, float *out) {
+    if (!e || !out || shot < 0 || shot >= std::max(e->nshots, 1)) return IFOSB_EARG;
+    const ifosb_params &p = e->p;
+    const Geo &g = e->g;
+    const float *src = nullptr;
+    if (field >= 0 && field < NEL) {
+        src = e->d_state + (long long)shot * e->st_shot + (long long)field * g.field;
+    } else if (field >= IFOSB_F_DFT_FWD && field < IFOSB_F_DFT_FWD + 6 * e->nf && e->d_dftf) {
+        const int q = field - IFOSB_F_DFT_FWD, comp = q / e->nf, l = q % e->nf;
+        src = e->d_dftf + (long long)shot * e->dft_shot + ((long long)l * 6 + comp) * g.field;
+    } else if (field >= IFOSB_F_DFT_BACK && field < IFOSB_F_DFT_BACK + 6 * e->nf && e->d_dftb) {
+        const int q = field - IFOSB_F_DFT_BACK, comp = q / e->nf, l = q % e->nf;
+        src = e->d_dftb + (long long)shot * e->dft_shot + ((long long)l * 6 + comp) * g.field;
+    } else {
+        return fail(e, IFOSB_EARG, "unknown field id");
+    }
+    // device rows start at k=-1 (offset 6); host rows are NZ+4 wide
+    CU(cudaMemcpy2D(out, sizeof(float) * (p.nz + 4), src + 6, sizeof(float) * g.pz, sizeof(float) * (p.nz + 4),
+                    (size_t)(p.ny + 5) * (p.nx + 4), cudaMemcpyDeviceToHost));
+    return IFOSB_OK;
+}

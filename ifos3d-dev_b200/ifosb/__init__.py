@@ -1,0 +1,313 @@
+"""Python host binding of the B200 IFOS3D wavefield engine.
+
+Thin ctypes layer over the C ABI in ``include/ifos_b200.h`` (library
+``ifos3d-dev_b200/lib/libifos_b200.so``). There is no CPU fallback: if the CUDA
+library is missing or no GPU is present, the calls raise.
+
+The names and argument meanings mirror the reference's driver
+(src/ifos3d.c): a forward batch, residual(), the back-propagation, gradient_F.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG_DIR, "lib", "libifos_b200.so")
+
+OK, EARG, ECUDA, ENOMEM, EUNSTABLE, ESTATE, ENODEV = 0, 1, 2, 3, 4, 5, 6
+_NAMES = {EARG: "EARG", ECUDA: "ECUDA", ENOMEM: "ENOMEM", EUNSTABLE: "EUNSTABLE", ESTATE: "ESTATE", ENODEV: "ENODEV"}
+
+F_VX, F_VY, F_VZ, F_SXX, F_SYY, F_SZZ, F_SXY, F_SYZ, F_SXZ = range(9)
+F_DFT_FWD, F_DFT_BACK = 100, 200
+
+
+class IfosbError(RuntimeError):
+    def __init__(self, code, msg=""):
+        super().__init__(f"ifosb error {_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+        ("dx", C.c_float), ("dy", C.c_float), ("dz", C.c_float),
+        ("dt", C.c_float), ("nt", C.c_int), ("time", C.c_float),
+        ("fdorder", C.c_int), ("fdcoeff", C.c_int), ("free_surf", C.c_int), ("abs_type", C.c_int),
+        ("fw", C.c_int), ("nmech", C.c_int), ("ndt", C.c_int), ("ndtshift", C.c_int),
+        ("alpha", C.c_float), ("beta", C.c_float),
+    ]
+
+
+class Shot(C.Structure):
+    _fields_ = [("nsrc", C.c_int), ("srcpos", C.c_void_p), ("signals", C.c_void_p)]
+
+
+def build_library(force: bool = False) -> str:
+    """Compile the CUDA library in-tree (nvcc, sm_100a). Returns the .so path."""
+    if force or not os.path.exists(LIB_PATH):
+        subprocess.run(["make", "-s", "-C", PKG_DIR], check=True)
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    """Load libifos_b200.so (raises if it is missing — no fallback path exists)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(f"{LIB_PATH} is missing: build it with `make -C {PKG_DIR}`")
+        L = C.CDLL(LIB_PATH)
+        vp = C.c_void_p
+        sig = {
+            "ifosb_create": (C.c_int, [C.POINTER(Params), C.c_int, C.c_int, C.POINTER(vp)]),
+            "ifosb_destroy": (None, [vp]),
+            "ifosb_last_error": (C.c_char_p, [vp]),
+            "ifosb_device_bytes": (C.c_longlong, [vp]),
+            "ifosb_set_cpml": (C.c_int, [vp, vp]),
+            "ifosb_set_model": (C.c_int, [vp, vp, vp, vp, vp, vp, vp]),
+            "ifosb_set_receivers": (C.c_int, [vp, C.c_int, vp]),
+            "ifosb_set_frequencies": (C.c_int, [vp, C.c_int, vp, C.c_int]),
+            "ifosb_forward": (C.c_int, [vp, C.c_int, C.POINTER(Shot), vp]),
+            "ifosb_residual": (C.c_int, [vp, vp, vp, vp]),
+            "ifosb_adjoint": (C.c_int, [vp, vp]),
+            "ifosb_gradient": (C.c_int, [vp]),
+            "ifosb_zero_gradient": (C.c_int, [vp]),
+            "ifosb_get_gradient": (C.c_int, [vp, vp, vp]),
+            "ifosb_shot_gradient": (C.c_int, [vp, C.c_int, C.POINTER(Shot), vp, vp]),
+            "ifosb_get_field": (C.c_int, [vp, C.c_int, C.c_int, vp]),
+            "ifosb_set_launch_mode": (C.c_int, [vp, C.c_int]),
+            "ifosb_last_launch_count": (C.c_longlong, [vp]),
+            "ifosb_cpml_coeff": (C.c_int, [C.POINTER(Params), C.c_float, C.c_float, vp]),
+            "ifosb_wavelet": (C.c_int, [C.POINTER(Params), C.c_int, C.c_int, vp, vp]),
+            "ifosb_nsamples": (C.c_int, [C.POINTER(Params)]),
+            "ifosb_moduli": (C.c_int, [C.POINTER(Params), C.c_longlong, vp, vp, vp, C.c_float, vp, vp, vp, vp, vp, vp]),
+            "ifosb_set_profiling": (C.c_int, [vp, C.c_int]),
+            "ifosb_kernel_times": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int)]),
+            "ifosb_set_stream": (C.c_int, [vp, vp]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def exported_symbols():
+    """Names of the C-ABI entry points this binding expects."""
+    return [
+        "ifosb_create", "ifosb_destroy", "ifosb_last_error", "ifosb_device_bytes", "ifosb_set_cpml",
+        "ifosb_set_model", "ifosb_set_receivers", "ifosb_set_frequencies", "ifosb_forward", "ifosb_residual",
+        "ifosb_adjoint", "ifosb_gradient", "ifosb_zero_gradient", "ifosb_get_gradient", "ifosb_shot_gradient",
+        "ifosb_get_field", "ifosb_set_launch_mode", "ifosb_last_launch_count", "ifosb_cpml_coeff",
+        "ifosb_wavelet", "ifosb_nsamples", "ifosb_moduli", "ifosb_set_profiling", "ifosb_kernel_times",
+        "ifosb_set_stream",
+    ]
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+def _f32(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float32)
+
+
+def make_params(nx, ny, nz, dh=1.0, dt=1e-4, nt=100, fdcoeff=2, free_surf=1, fw=10, nmech=0, ndt=1, ndtshift=0,
+                alpha=0.0, beta=0.0, dx=None, dy=None, dz=None) -> Params:
+    """Parameters as the reference derives them: TIME=(NT-1)*DT in float (ifos3d.c:176-177)."""
+    dtf = np.float32(dt)
+    return Params(nx=nx, ny=ny, nz=nz, dx=dx or dh, dy=dy or dh, dz=dz or dh, dt=dtf, nt=nt,
+                  time=np.float32(np.float32(nt - 1) * dtf), fdorder=4, fdcoeff=fdcoeff, free_surf=free_surf,
+                  abs_type=1, fw=fw, nmech=nmech, ndt=ndt, ndtshift=ndtshift, alpha=alpha, beta=beta)
+
+
+def nsamples(p: Params) -> int:
+    return lib().ifosb_nsamples(C.byref(p))
+
+
+def cpml_coeff(p: Params, vppml: float, fpml: float) -> np.ndarray:
+    out = np.zeros((18, 2 * p.fw), np.float32)
+    _check(None, lib().ifosb_cpml_coeff(C.byref(p), vppml, fpml, _p(out)))
+    return out
+
+
+def wavelet(p: Params, shape: int, srcpos) -> np.ndarray:
+    srcpos = _f32(np.atleast_2d(srcpos))
+    out = np.zeros((srcpos.shape[0], p.nt), np.float32)
+    _check(None, lib().ifosb_wavelet(C.byref(p), shape, srcpos.shape[0], _p(srcpos), _p(out)))
+    return out
+
+
+def moduli(p: Params, vp, vs, rho, tau=0.0, fl=None):
+    """readmod() arithmetic: returns dict(rho, pi, u, taus, taup, eta) (interior arrays)."""
+    vp, vs, rho = _f32(vp), _f32(vs), _f32(rho)
+    n = vp.size
+    pi, u = np.zeros_like(vp), np.zeros_like(vp)
+    L = p.nmech
+    taus = np.zeros_like(vp) if L else None
+    taup = np.zeros_like(vp) if L else None
+    eta = np.zeros(max(L, 1), np.float32)
+    fla = _f32(fl) if L else None
+    _check(None, lib().ifosb_moduli(C.byref(p), n, _p(vp), _p(vs), _p(rho), tau, _p(fla), _p(pi), _p(u),
+                                    _p(taus), _p(taup), _p(eta)))
+    return dict(rho=rho, pi=pi, u=u, taus=taus, taup=taup, eta=eta[:L] if L else None)
+
+
+def ghost_wrap(a) -> np.ndarray:
+    """The model with one ghost layer as matcopy() leaves it on one rank: a
+    periodic wrap (src/matcopy.c:31-327, receives from MPI_PROC_NULL are no-ops)."""
+    return np.ascontiguousarray(np.pad(np.asarray(a, np.float32), 1, mode="wrap"))
+
+
+def _check(eng, rc):
+    if rc != OK:
+        msg = lib().ifosb_last_error(eng).decode() if eng else ""
+        raise IfosbError(rc, msg)
+
+
+class Engine:
+    """One device-resident problem (model, CPML, receivers, frequencies) and a
+    batch of up to ``max_shots`` shots."""
+
+    def __init__(self, p: Params, max_shots: int = 1, max_nf: int = 0):
+        self.p = p
+        self.max_shots = max_shots
+        h = C.c_void_p()
+        rc = lib().ifosb_create(C.byref(p), max_shots, max_nf, C.byref(h))
+        if rc != OK:
+            raise IfosbError(rc, "ifosb_create")
+        self.h = h
+        self.ntr = 0
+        self.ns = nsamples(p)
+        self.nf = 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().ifosb_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _c(self, rc):
+        _check(self.h, rc)
+
+    @property
+    def device_bytes(self) -> int:
+        return lib().ifosb_device_bytes(self.h)
+
+    def set_cpml(self, coeff):
+        coeff = _f32(coeff)
+        self._c(lib().ifosb_set_cpml(self.h, _p(coeff)))
+
+    def set_model(self, rho, pi, u, taus=None, taup=None, eta=None, ghosted=False):
+        """Interior [NY][NX][NZ] arrays (wrapped here like matcopy on one rank) or,
+        with ghosted=True, the caller's own [NY+2][NX+2][NZ+2] arrays."""
+        w = (lambda a: _f32(a)) if ghosted else (lambda a: None if a is None else ghost_wrap(a))
+        arrs = [w(rho), w(pi), w(u), w(taus), w(taup), _f32(eta)]
+        self._keep = arrs
+        self._c(lib().ifosb_set_model(self.h, *[_p(a) for a in arrs]))
+
+    def set_receivers(self, recpos):
+        rec = np.ascontiguousarray(recpos, dtype=np.int32).reshape(-1, 3)
+        self._c(lib().ifosb_set_receivers(self.h, rec.shape[0], _p(rec)))
+        self.ntr = rec.shape[0]
+
+    def set_frequencies(self, finv, ntast=1):
+        f = _f32(finv) if finv is not None and len(finv) else None
+        nf = 0 if f is None else len(f)
+        self._c(lib().ifosb_set_frequencies(self.h, nf, _p(f), ntast))
+        self.nf = nf
+
+    def set_launch_mode(self, mode: int):
+        self._c(lib().ifosb_set_launch_mode(self.h, mode))
+
+    @property
+    def launch_count(self) -> int:
+        return lib().ifosb_last_launch_count(self.h)
+
+    def set_profiling(self, on: bool):
+        self._c(lib().ifosb_set_profiling(self.h, 1 if on else 0))
+
+    def kernel_times(self):
+        """(velocity ms, stress ms, steps) of the last profiled time loop."""
+        v, s, n = C.c_double(), C.c_double(), C.c_int()
+        self._c(lib().ifosb_kernel_times(self.h, C.byref(v), C.byref(s), C.byref(n)))
+        return v.value, s.value, n.value
+
+    def set_stream(self, stream_handle):
+        """Launch on the caller's cudaStream_t (an int handle, e.g. torch's stream.cuda_stream)."""
+        self._c(lib().ifosb_set_stream(self.h, C.c_void_p(stream_handle) if stream_handle else None))
+
+    @staticmethod
+    def _shots(shots):
+        keep, arr = [], (Shot * len(shots))()
+        for s, (srcpos, signals) in enumerate(shots):
+            sp = _f32(np.atleast_2d(srcpos))
+            sg = _f32(np.atleast_2d(signals))
+            keep += [sp, sg]
+            arr[s] = Shot(sp.shape[0], _p(sp), _p(sg))
+        return arr, keep
+
+    def forward(self, shots, want_sections=True):
+        """shots: list of (srcpos[nsrc][7], signals[nsrc][NT]). Returns [nshots][3][ntr][ns] or None."""
+        arr, keep = self._shots(shots)
+        out = np.zeros((len(shots), 3, self.ntr, self.ns), np.float32) if (want_sections and self.ntr) else None
+        self._c(lib().ifosb_forward(self.h, len(shots), arr, _p(out)))
+        return out
+
+    def residual(self, obs, want_l2_ref=False):
+        obs = _f32(obs)
+        nsh = obs.shape[0]
+        mis = np.zeros(nsh, np.float64)
+        l2 = np.zeros(nsh, np.float32) if want_l2_ref else None
+        self._c(lib().ifosb_residual(self.h, _p(obs), _p(mis), _p(l2)))
+        return (mis, l2) if want_l2_ref else mis
+
+    def adjoint(self, diff=None):
+        d = _f32(diff)
+        self._c(lib().ifosb_adjoint(self.h, _p(d)))
+
+    def gradient(self):
+        self._c(lib().ifosb_gradient(self.h))
+
+    def zero_gradient(self):
+        self._c(lib().ifosb_zero_gradient(self.h))
+
+    def get_gradient(self, fp64=False):
+        g = np.zeros((3, self.p.ny, self.p.nx, self.p.nz), np.float64 if fp64 else np.float32)
+        if fp64:
+            self._c(lib().ifosb_get_gradient(self.h, None, _p(g)))
+        else:
+            self._c(lib().ifosb_get_gradient(self.h, _p(g), None))
+        return g
+
+    def shot_gradient(self, shots, obs):
+        arr, keep = self._shots(shots)
+        obs = _f32(obs)
+        mis = np.zeros(len(shots), np.float64)
+        self._c(lib().ifosb_shot_gradient(self.h, len(shots), arr, _p(obs), _p(mis)))
+        return mis
+
+    def get_field(self, shot: int, field: int) -> np.ndarray:
+        out = np.zeros((self.p.ny + 5, self.p.nx + 4, self.p.nz + 4), np.float32)
+        self._c(lib().ifosb_get_field(self.h, shot, field, _p(out)))
+        return out
+
+    def get_state(self, shot: int = 0) -> np.ndarray:
+        return np.stack([self.get_field(shot, f) for f in range(9)])
+
+    def get_dft(self, shot: int = 0, back: bool = False) -> np.ndarray:
+        base = F_DFT_BACK if back else F_DFT_FWD
+        return np.stack([np.stack([self.get_field(shot, base + c * self.nf + l) for l in range(self.nf)])
+                         for c in range(6)])

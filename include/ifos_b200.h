@@ -1,0 +1,187 @@
+/*
+ * ifos_b200.h — C ABI of the B200 (sm_100a) wavefield engine for IFOS3D.
+ *
+ * The engine replaces the three time loops of the reference driver
+ * (src/ifos3d.c:754-814 forward, :909-960 back-propagation, :1070-1103
+ * step-length forwards) and the per-shot kernels they call, plus
+ * residual() and gradient_F(). The host program keeps its own JSON input,
+ * model/gradient/SU file handling and optimiser; it calls these entry points
+ * with the arrays it already owns. All device memory is owned by the library;
+ * host buffers belong to the caller. Every entry point is synchronous at
+ * return and returns an int status (IFOSB_OK == 0); a non-zero status is what
+ * the reference turns into err() (src/util.c:30-40).
+ *
+ * Index conventions are the reference's: y (index j) is depth, arrays are
+ * [j][i][k] with k (z) contiguous; grid indices are 1-based like the
+ * reference's loops (cells 1..NX, 1..NY, 1..NZ).
+ */
+#ifndef IFOS_B200_H
+#define IFOS_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+#define IFOSB_OK 0
+#define IFOSB_EARG 1          /* invalid argument or unsupported parameter        */
+#define IFOSB_ECUDA 2         /* CUDA runtime/launch error                        */
+#define IFOSB_ENOMEM 3        /* device allocation failed                         */
+#define IFOSB_EUNSTABLE 4     /* NaN probe fired (src/ifos3d.c:761, :916, :1075) */
+#define IFOSB_ESTATE 5        /* call order violated (e.g. adjoint before residual) */
+#define IFOSB_ENODEV 6        /* no CUDA device                                   */
+
+/* Parameters, taken from the reference's globals (src/globvar.h). One rank:
+ * NX, NY, NZ are the whole grid. */
+typedef struct ifosb_params {
+    int nx, ny, nz;         /* NX, NY, NZ                                          */
+    float dx, dy, dz;       /* DX, DY, DZ                                          */
+    float dt;               /* DT                                                  */
+    int nt;                 /* NT = ceil(TIME/DT)            (src/ifos3d.c:176)    */
+    float time;             /* TIME after TIME=(NT-1)*DT     (src/ifos3d.c:177)    */
+    int fdorder;            /* FDORDER; only 4 is implemented                     */
+    int fdcoeff;            /* FDCOEFF: 1 Taylor, 2 Holberg                       */
+    int free_surf;          /* FREE_SURF (free surface at j=1)                    */
+    int abs_type;           /* ABS_TYPE; only 1 (CPML) is implemented             */
+    int fw;                 /* FW, CPML width in cells                            */
+    int nmech;              /* L relaxation mechanisms; 0 = elastic               */
+    int ndt, ndtshift;      /* NDT, NDTSHIFT seismogram sampling                  */
+    float alpha, beta;      /* ALPHA, BETA (custom-force source type 5)           */
+} ifosb_params;
+
+/* One shot: the sources the reference keeps in srcpos_loc[1..7][l] and the
+ * wavelets in signals[l][1..NT] (src/ifos3d.c:712-732). */
+typedef struct ifosb_shot {
+    int nsrc;
+    const float *srcpos;   /* [nsrc][7]: x-index, y-index, z-index, tshift, fc, amp, stype */
+    const float *signals;  /* [nsrc][NT] */
+} ifosb_shot;
+
+typedef struct ifosb_engine ifosb_engine;
+
+/* Field ids for ifosb_get_field (diagnostics and parity tests). */
+#define IFOSB_F_VX 0
+#define IFOSB_F_VY 1
+#define IFOSB_F_VZ 2
+#define IFOSB_F_SXX 3
+#define IFOSB_F_SYY 4
+#define IFOSB_F_SZZ 5
+#define IFOSB_F_SXY 6
+#define IFOSB_F_SYZ 7
+#define IFOSB_F_SXZ 8
+#define IFOSB_F_DFT_FWD 100   /* + comp*nf + l, comp 0..5 = Re vx,vy,vz, Im vx,vy,vz */
+#define IFOSB_F_DFT_BACK 200  /* + comp*nf + l */
+
+/* ---- lifecycle ---------------------------------------------------------- */
+
+/* Creates an engine on the current CUDA device for up to max_shots shots per
+ * batch and up to max_nf DFT frequencies (0 = forward modelling only). */
+int ifosb_create(const ifosb_params *p, int max_shots, int max_nf, ifosb_engine **out);
+void ifosb_destroy(ifosb_engine *e);
+const char *ifosb_last_error(const ifosb_engine *e);
+/* Device bytes the engine holds (state, PML, DFT, model, gradient, traces). */
+long long ifosb_device_bytes(const ifosb_engine *e);
+
+/* ---- static inputs ------------------------------------------------------ */
+
+/* CPML profiles as CPML_coeff() returns them (src/CPML_coeff.c:87-324):
+ * coeff[18][2*FW], rows K_x,a_x,b_x,K_x_half,a_x_half,b_x_half, then _y, then _z;
+ * element h of a row is the reference's vector index h+1 (&K_x[1] etc.). */
+int ifosb_set_cpml(ifosb_engine *e, const float *coeff);
+
+/* Model after the host's matcopy (src/ifos3d.c:681): rho, pi (=lambda+2mu), u (=mu)
+ * and, when nmech>0, taus, taup as the reference allocates them,
+ * f3tensor(0,NY+1,0,NX+1,0,NZ+1) — pass &rho[0][0][0]. eta[nmech] as readmod()
+ * returns it (eta[l-1] = the reference's eta[l]). The staggered averages of
+ * av_mat() (src/av_mat.c:28-80) are formed on the device. */
+int ifosb_set_model(ifosb_engine *e, const float *rho, const float *pi, const float *u,
+                    const float *taus, const float *taup, const float *eta);
+
+/* Receivers (recpos_loc[1..3][itr], src/ifos3d.c:197-204): recpos[ntr][3] x, y, z index. */
+int ifosb_set_receivers(ifosb_engine *e, int ntr, const int *recpos);
+
+/* Monochromatic frequencies of the current stage (finv[0..nf-1], readinv.c) and the
+ * DFT sampling interval ntast (src/ifos3d.c:745-749). nf=0 = forward modelling (METHOD=0). */
+int ifosb_set_frequencies(ifosb_engine *e, int nf, const float *finv, int ntast);
+
+/* ---- the time loops ----------------------------------------------------- */
+
+/* Forward propagation of nshots shots in one batch (src/ifos3d.c:738-814 per shot):
+ * zeroes the wavefield, runs NT steps of update_v/_CPML, update_s(_elastic)/_CPML,
+ * psource, discfourier (if nf>0), surface, seismo. sections (optional, host):
+ * [nshots][3][ntr][ns] vx, vy, vz traces. DFT fields stay on the device. */
+int ifosb_forward(ifosb_engine *e, int nshots, const ifosb_shot *shots, float *sections);
+
+/* residual() for every shot of the last forward batch (src/ifos3d.c:837-858):
+ * obs [nshots][3][ntr][ns] observed traces (host). Forms the time-reversed
+ * displacement residual on the device. misfit_fp64 (optional, [nshots]) gets
+ * sum(residual^2) reduced in FP64; l2_ref (optional, [nshots]) gets the same
+ * sum in the reference's float accumulation order. */
+int ifosb_residual(ifosb_engine *e, const float *obs, double *misfit_fp64, float *l2_ref);
+
+/* Back-propagation (src/ifos3d.c:882-960): the residual of the last
+ * ifosb_residual (or, if diff != NULL, the caller's [nshots][3][ntr][ns] residual)
+ * is injected at the receivers, twice per step as the reference does with CPML,
+ * and the backward DFT is accumulated with t = TIME - nt*DT. */
+int ifosb_adjoint(ifosb_engine *e, const float *diff);
+
+/* gradient_F (src/gradient_F.c:30-171) of the last forward/adjoint batch,
+ * accumulated into the engine's gradient in shot order (the reference's shot
+ * loop): FP32 exactly as the reference, and a parallel FP64 accumulation. */
+int ifosb_gradient(ifosb_engine *e);
+
+/* Zero the accumulated gradients (zero_grad, src/zero_grad.c). */
+int ifosb_zero_gradient(ifosb_engine *e);
+
+/* Copy the accumulated gradient out: grad[3][NY][NX][NZ] (vp, vs, rho; the layout of
+ * grad1..3 interior) and/or the FP64 accumulation grad64[3][NY][NX][NZ]. */
+int ifosb_get_gradient(ifosb_engine *e, float *grad, double *grad64);
+
+/* forward + residual + adjoint + gradient for a batch: the per-shot body of
+ * src/ifos3d.c:712-975 for nshots shots at once. misfit (optional): [nshots] FP64. */
+int ifosb_shot_gradient(ifosb_engine *e, int nshots, const ifosb_shot *shots,
+                        const float *obs, double *misfit);
+
+/* Copy one field of one shot of the last batch in the reference's wavefield
+ * layout [NY+5][NX+4][NZ+4] (j=-2..NY+2, i=-1..NX+2, k=-1..NZ+2). */
+int ifosb_get_field(ifosb_engine *e, int shot, int field, float *out);
+
+/* Synchronous launch mode: 0 = the time loop is captured once into a CUDA graph
+ * and replayed (default); 1 = plain stream launches, one per kernel. */
+int ifosb_set_launch_mode(ifosb_engine *e, int mode);
+
+/* Kernels launched by the last forward/adjoint call (per-step kernels x steps). */
+long long ifosb_last_launch_count(const ifosb_engine *e);
+
+/* Kernel timing: with profile=1 the time loops launch kernel by kernel with a
+ * CUDA event pair around every launch on the engine's stream; after a forward
+ * or adjoint call ifosb_kernel_times returns the summed device milliseconds of
+ * the velocity and the stress kernels and the number of steps timed. */
+int ifosb_set_profiling(ifosb_engine *e, int profile);
+int ifosb_kernel_times(const ifosb_engine *e, double *vel_ms, double *str_ms, int *steps);
+
+/* Run the engine's work on the caller's CUDA stream (a cudaStream_t passed as
+ * void*; NULL = the engine's own stream). Calls stay synchronous at return. */
+int ifosb_set_stream(ifosb_engine *e, void *stream);
+
+/* ---- host utilities (restated reference host code) ---------------------- */
+
+/* CPML_coeff (src/CPML_coeff.c:87-324) with VPPML, FPML into coeff[18][2*FW]. */
+int ifosb_cpml_coeff(const ifosb_params *p, float vppml, float fpml, float *coeff);
+
+/* wavelet (src/wavelet.c:29-99) for source shapes 1, 2, 4, 5: signals[nsrc][NT]. */
+int ifosb_wavelet(const ifosb_params *p, int shape, int nsrc, const float *srcpos, float *signals);
+
+/* readmod (src/readmod.c:28-139) without the file reading: vp, vs, rho [n] ->
+ * rho stays, pi = vp^2 rho/(1+sumpi), u = vs^2 rho/(1+sumu) (relaxed moduli at
+ * ws = 2 pi FL[1]), taus = taup = TAU, eta[l] = DT/tau_sigma_l. fl[nmech] = FL[1..L]. */
+int ifosb_moduli(const ifosb_params *p, long long n, const float *vp, const float *vs, const float *rho, float tau,
+                 const float *fl, float *pi, float *u, float *taus, float *taup, float *eta);
+
+/* Number of samples per trace ns (src/ifos3d.c:178-179). */
+int ifosb_nsamples(const ifosb_params *p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
