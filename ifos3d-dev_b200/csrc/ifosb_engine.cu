@@ -8,6 +8,9 @@
 // and replayed on later calls.
 #include "../../include/ifos_b200.h"
 #include "ifosb_kernels.cuh"
+#include "ifosb_tma.cuh"
+
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <climits>
@@ -76,6 +79,12 @@ struct ifosb_engine {
     int t_steps = 0;
     std::vector<cudaEvent_t> events;
     cudaStream_t own_stream = nullptr;
+    // TMA staging (default) and its wait-timeout flag
+    int use_tma = 1;
+    int *d_tma_err = nullptr;
+    // uniform relaxation times: passed as scalars instead of five model fields
+    bool unif_tau = false;
+    float utaus = 0.f, utaup = 0.f, uts_avg = 0.f;
     std::string err;
 };
 
@@ -156,9 +165,8 @@ static int block_of(const Geo &g, int j, int i, int k) {
 }
 
 // Groups points per (shot, block), stable within a group (the reference's loop order).
-static int upload_points(ifosb_engine *e, int nshots, const std::vector<HostPt> &pts, int **d_off, size_t *cap_off,
-                         Pt **d_pts, size_t *cap_pts) {
-    const Geo &g = e->g;
+static int upload_points(ifosb_engine *e, const Geo &g, int nshots, const std::vector<HostPt> &pts, int **d_off,
+                         size_t *cap_off, Pt **d_pts, size_t *cap_pts) {
     const int nblk = g.ntk * g.nti * g.nyc;
     std::vector<int> cnt((size_t)nshots * nblk, 0);
     for (const HostPt &q : pts) cnt[(size_t)q.s * nblk + block_of(g, q.j, q.i, q.k)]++;
@@ -239,9 +247,13 @@ extern "C" int ifosb_create(const ifosb_params *p, int max_shots, int max_nf, if
         (rc = dalloc(e, &e->d_rho_w, (size_t)g.field)) ||
         (rc = dalloc(e, &e->d_grad, (size_t)(3 * ncell))) ||
         (rc = dalloc(e, &e->d_grad64, (size_t)(3 * ncell))) ||
-        (rc = dalloc(e, &e->d_err, (size_t)max_shots))) {
+        (rc = dalloc(e, &e->d_err, (size_t)max_shots)) || (rc = dalloc(e, &e->d_tma_err, 1))) {
         ifosb_destroy(e);
         return rc;
+    }
+    {
+        const char *v = getenv("IFOSB_TMA");
+        if (v && v[0] == '0') e->use_tma = 0;
     }
     if (max_nf > 0) {
         if ((rc = dalloc(e, &e->d_dftf, (size_t)(e->dft_shot * max_shots))) ||
@@ -271,7 +283,7 @@ extern "C" void ifosb_destroy(ifosb_engine *e) {
     release_graph(e->gadj);
     void *bufs[] = {e->d_state, e->d_psi, e->d_model, e->d_rho_w, e->d_dftf, e->d_dftb, e->d_grad, e->d_grad64,
                     e->d_err, e->d_sec, e->d_diff, e->d_obs, e->d_part, e->d_misfit, e->d_l2, e->d_trig_f,
-                    e->d_trig_b, e->d_voff, e->d_soff, e->d_vpts, e->d_spts, e->d_amp};
+                    e->d_trig_b, e->d_voff, e->d_soff, e->d_vpts, e->d_spts, e->d_amp, e->d_tma_err};
     for (void *b : bufs)
         if (b) cudaFree(b);
     for (cudaEvent_t ev : e->events) cudaEventDestroy(ev);
@@ -361,6 +373,20 @@ extern "C" int ifosb_set_model(ifosb_engine *e, const float *rho, const float *p
     if (le != cudaSuccess || se != cudaSuccess)
         return fail(e, IFOSB_ECUDA, std::string("av_mat: ") + cudaGetErrorString(le != cudaSuccess ? le : se));
     for (int l = 0; l < MAXMECH; ++l) e->eta[l] = l < p.nmech ? eta[l] : 0.f;
+    // readmod() gives every cell the same TAU (readmod.c:57-58, 119-120); then the
+    // staggered averages are one value too and the kernels take scalars
+    e->unif_tau = false;
+    if (p.nmech > 0) {
+        bool u = true;
+        for (size_t q = 1; q < ng && u; ++q) u = taus[q] == taus[0] && taup[q] == taup[0];
+        if (u) {
+            const float t = taus[0];
+            e->unif_tau = true;
+            e->utaus = t;
+            e->utaup = taup[0];
+            e->uts_avg = 0.25 * (t + t + t + t);  // av_mat.c:56-58 with four equal values
+        }
+    }
     e->have_model = true;
     e->fwd_ok = e->res_ok = e->adj_ok = false;
     return IFOSB_OK;
@@ -442,11 +468,45 @@ extern "C" int ifosb_set_frequencies(ifosb_engine *e, int nf, const float *finv,
 // ---------------------------------------------------------------------------
 // the time loop
 
-static void fill_common(ifosb_engine *e, VelArgs &va, StrArgs &sa) {
+static_assert(TZ == BX && TX == BY, "TMA tiles and plain blocks share one block geometry");
+
+// Everything one forward or adjoint call launches with.
+struct Loop {
+    Geo lg;  // launch geometry of this call (the y chunking depends on the batch size)
+    VelArgs va;
+    StrArgs sa;
+    VelTma vt;
+    StrTma stt;
+    int nshots = 0;
+    bool back = false;
+    bool tma = false;
+    bool p2 = false;  // power-of-two spacings (stress kernel multiplies by 1/DX etc.)
+    size_t vel_smem = 0, str_smem = 0;
+};
+
+// y planes per CTA: long chunks amortise the ring prologue; enough chunks keep
+// about four CTAs per SM in flight over the whole batch.
+static Geo launch_geo(const ifosb_engine *e, int nshots) {
+    Geo g = e->g;
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaGetLastError();
+    const long long per_set = (long long)g.ntk * g.nti * nshots;
+    const long long chunks = std::max<long long>(1, (4LL * sms + per_set - 1) / per_set);
+    int cy = (int)((g.ny + chunks - 1) / chunks);
+    cy = std::min(std::max(cy, DEFAULT_CY), 64);
+    g.cy = cy;
+    g.nyc = (g.ny + cy - 1) / cy;
+    return g;
+}
+
+static void fill_common(ifosb_engine *e, Loop &L) {
     const ifosb_params &p = e->p;
+    VelArgs &va = L.va;
+    StrArgs &sa = L.sa;
     va = VelArgs{};
     sa = StrArgs{};
-    va.g = sa.g = e->g;
+    va.g = sa.g = L.lg;
     va.sl = sa.sl = e->sl;
     va.st = sa.st = e->d_state;
     va.st_shot = sa.st_shot = e->st_shot;
@@ -460,10 +520,10 @@ static void fill_common(ifosb_engine *e, VelArgs &va, StrArgs &sa) {
         // custom force direction factors (update_v_ssg.c:498-503); the reference is C,
         // so cos/sin of its float angles run in double (C++ would pick the float overloads)
         const float alpha_rad = p.alpha * 3.141592653589793 / 180, beta_rad = p.beta * 3.141592653589793 / 180;
-        const double ca = std::cos((double)alpha_rad), sa = std::sin((double)alpha_rad);
+        const double ca = std::cos((double)alpha_rad), sa_ = std::sin((double)alpha_rad);
         const double cb = std::cos((double)beta_rad), sb = std::sin((double)beta_rad);
         va.cf5x = cb * ca;
-        va.cf5y = sa;
+        va.cf5y = sa_;
         va.cf5z = sb * ca;
     }
     va.err_step = e->d_err;
@@ -486,42 +546,164 @@ static void fill_common(ifosb_engine *e, VelArgs &va, StrArgs &sa) {
     sa.dft_shot = e->dft_shot;
 }
 
-template <int L>
-static void launch_stress(dim3 grd, dim3 blk, cudaStream_t st, const StrArgs &sa, int nt, int do_dft, int sample) {
-    k_stress<L><<<grd, blk, 0, st>>>(sa, nt, do_dft, sample);
+// cuTensorMapEncodeTiled from the driver, reached through the runtime (no libcuda link).
+static PFN_cuTensorMapEncodeTiled_v12000 tma_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)f;
+        else
+            cudaGetLastError();
+    }
+    return fn;
 }
 
-static void launch_step_stress(int nmech, dim3 grd, dim3 blk, cudaStream_t st, const StrArgs &sa, int nt, int do_dft,
-                               int sample) {
+static bool encode(CUtensorMap *m, void *base, int rank, const cuuint64_t *dims, const cuuint64_t *strides,
+                   const cuuint32_t *box) {
+    auto fn = tma_encoder();
+    if (!fn) return false;
+    const cuuint32_t es[5] = {1, 1, 1, 1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, (cuuint32_t)rank, base, dims, strides, box, es,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <int M>
+static void smem_attrs(size_t vel, size_t str) {
+    cudaFuncSetAttribute(k_velocity_tma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vel);
+    cudaFuncSetAttribute(k_velocity_tma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vel);
+    cudaFuncSetAttribute(k_stress_tma<M, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)str);
+    cudaFuncSetAttribute(k_stress_tma<M, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)str);
+}
+
+// An exact reciprocal exists for a power-of-two spacing: x/h == x*(1/h) bit for bit.
+static bool pow2(float h) {
+    int ex = 0;
+    return h > 0.f && std::isfinite(h) && std::frexp(h, &ex) == 0.5f;
+}
+
+// Tensor maps over the state [shot][slot][y][x][z], the model [slot][y][x][z] and the
+// DFT accumulators [shot][6 nf][y][x][z]; false if TMA staging cannot be used.
+static bool setup_tma(ifosb_engine *e, Loop &L, float *dft) {
+    const Geo &g = e->g;
+    const ifosb_params &p = e->p;
+    const int nslot = NEL + 6 * p.nmech;
+    const int nsr = 6 + 6 * p.nmech;
+    const int nm = (p.nmech == 0 || e->unif_tau) ? 5 : 10;
+    const int ndf = (dft && e->nf > 0) ? 6 * e->nf : 0;
+    const size_t vs = vel_tma_smem(), ss = str_tma_smem(nsr, nm, ndf);
+    if (vs > 227 * 1024 || ss > 227 * 1024) return false;
+    const cuuint64_t sdims[5] = {(cuuint64_t)g.pz, (cuuint64_t)g.px, (cuuint64_t)(p.ny + 5), (cuuint64_t)nslot,
+                                 (cuuint64_t)e->max_shots};
+    const cuuint64_t sstr[4] = {(cuuint64_t)g.pz * 4, (cuuint64_t)g.plane * 4, (cuuint64_t)g.field * 4,
+                                (cuuint64_t)e->st_shot * 4};
+    const cuuint64_t mdims[4] = {(cuuint64_t)g.pz, (cuuint64_t)g.px, (cuuint64_t)(p.ny + 5), (cuuint64_t)NMODEL};
+    const cuuint64_t mstr[3] = {(cuuint64_t)g.pz * 4, (cuuint64_t)g.plane * 4, (cuuint64_t)g.field * 4};
+    const cuuint32_t bhalo[5] = {RZ, RX, 1, 3, 1}, bpt[5] = {TZ, TX, 1, 3, 1};
+    const cuuint32_t bsr[5] = {TZ, TX, 1, (cuuint32_t)nsr, 1};
+    const cuuint32_t bmv[4] = {TZ, TX, 1, 3}, bms[4] = {TZ, TX, 1, (cuuint32_t)nm};
+    L.vt = VelTma{};
+    L.stt = StrTma{};
+    if (!encode(&L.vt.m_halo, e->d_state, 5, sdims, sstr, bhalo) || !encode(&L.vt.m_pt, e->d_state, 5, sdims, sstr, bpt) ||
+        !encode(&L.vt.m_mod, e->d_model, 4, mdims, mstr, bmv) || !encode(&L.stt.m_sr, e->d_state, 5, sdims, sstr, bsr) ||
+        !encode(&L.stt.m_mod, e->d_model, 4, mdims, mstr, bms))
+        return false;
+    L.stt.m_halo = L.vt.m_halo;
+    if (ndf) {
+        const cuuint64_t ddims[5] = {(cuuint64_t)g.pz, (cuuint64_t)g.px, (cuuint64_t)(p.ny + 5),
+                                     (cuuint64_t)(6 * e->max_nf), (cuuint64_t)e->max_shots};
+        const cuuint64_t dstr[4] = {(cuuint64_t)g.pz * 4, (cuuint64_t)g.plane * 4, (cuuint64_t)g.field * 4,
+                                    (cuuint64_t)e->dft_shot * 4};
+        const cuuint32_t bd[5] = {TZ, TX, 1, (cuuint32_t)ndf, 1};
+        if (!encode(&L.stt.m_dft, dft, 5, ddims, dstr, bd)) return false;
+    }
+    L.vt.a = L.va;
+    L.stt.a = L.sa;
+    L.vt.tma_err = L.stt.tma_err = e->d_tma_err;
+    L.stt.nsr = nsr;
+    L.stt.nm = nm;
+    L.stt.ndf = ndf;
+    L.stt.utaus = e->utaus;
+    L.stt.utaup = e->utaup;
+    L.stt.uts_avg = e->uts_avg;
+    L.p2 = pow2(p.dx) && pow2(p.dy) && pow2(p.dz);
+    L.stt.idx = 1.0f / p.dx;
+    L.stt.idy = 1.0f / p.dy;
+    L.stt.idz = 1.0f / p.dz;
+    L.vel_smem = vs;
+    L.str_smem = ss;
+    switch (p.nmech) {
+    case 0: smem_attrs<0>(vs, ss); break;
+    case 1: smem_attrs<1>(vs, ss); break;
+    case 2: smem_attrs<2>(vs, ss); break;
+    case 3: smem_attrs<3>(vs, ss); break;
+    default: smem_attrs<4>(vs, ss); break;
+    }
+    return cudaGetLastError() == cudaSuccess;
+}
+
+template <int M>
+static void launch_str_m(const Loop &L, dim3 grd, cudaStream_t st, int nt, int do_dft, int sample) {
+    if (L.tma) {
+        const dim3 blk(TZ, TX + 1);
+        if (L.p2) k_stress_tma<M, true><<<grd, blk, L.str_smem, st>>>(L.stt, nt, do_dft, sample);
+        else k_stress_tma<M, false><<<grd, blk, L.str_smem, st>>>(L.stt, nt, do_dft, sample);
+    } else {
+        k_stress<M><<<grd, dim3(BX, BY), 0, st>>>(L.sa, nt, do_dft, sample);
+    }
+}
+
+static void launch_str(int nmech, const Loop &L, dim3 grd, cudaStream_t st, int nt, int do_dft, int sample) {
     switch (nmech) {
-    case 0: launch_stress<0>(grd, blk, st, sa, nt, do_dft, sample); break;
-    case 1: launch_stress<1>(grd, blk, st, sa, nt, do_dft, sample); break;
-    case 2: launch_stress<2>(grd, blk, st, sa, nt, do_dft, sample); break;
-    case 3: launch_stress<3>(grd, blk, st, sa, nt, do_dft, sample); break;
-    default: launch_stress<4>(grd, blk, st, sa, nt, do_dft, sample); break;
+    case 0: launch_str_m<0>(L, grd, st, nt, do_dft, sample); break;
+    case 1: launch_str_m<1>(L, grd, st, nt, do_dft, sample); break;
+    case 2: launch_str_m<2>(L, grd, st, nt, do_dft, sample); break;
+    case 3: launch_str_m<3>(L, grd, st, nt, do_dft, sample); break;
+    default: launch_str_m<4>(L, grd, st, nt, do_dft, sample); break;
+    }
+}
+
+static void launch_vel(const Loop &L, dim3 grd, cudaStream_t st, int nt) {
+    if (L.tma) {
+        const dim3 blk(TZ, TX + 1);
+        if (L.back) k_velocity_tma<true><<<grd, blk, L.vel_smem, st>>>(L.vt, nt);
+        else k_velocity_tma<false><<<grd, blk, L.vel_smem, st>>>(L.vt, nt);
+    } else {
+        const dim3 blk(BX, BY);
+        if (L.back) k_velocity<true><<<grd, blk, 0, st>>>(L.va, nt);
+        else k_velocity<false><<<grd, blk, 0, st>>>(L.va, nt);
+    }
+}
+
+// Per-step launch parameters: DFT on steps nt % ntast == 0 (ifos3d.c:788), seismogram
+// sample index when nt == lsamp (ifos3d.c:799-804, forward only).
+static void step_flags(const ifosb_engine *e, bool back, int nt, int &lsamp, int &nlsamp, int &do_dft, int &sample) {
+    do_dft = (e->nf > 0 && nt % e->ntast == 0) ? 1 : 0;
+    sample = -1;
+    if (!back && nt == lsamp) {
+        sample = nlsamp++;
+        lsamp += e->p.ndt;
     }
 }
 
 // Enqueue the NT steps (two kernels per step) on the engine stream.
-static void enqueue_loop(ifosb_engine *e, bool back, const VelArgs &va, const StrArgs &sa, int nshots) {
+static void enqueue_loop(ifosb_engine *e, const Loop &L) {
     const ifosb_params &p = e->p;
-    dim3 blk(BX, BY), grd(e->g.ntk, e->g.nti, e->g.nyc * nshots);
+    dim3 grd(L.lg.ntk, L.lg.nti, L.lg.nyc * L.nshots);
     int lsamp = p.ndtshift + 1, nlsamp = 0;
     for (int nt = 1; nt <= p.nt; ++nt) {
-        if (back) k_velocity<true><<<grd, blk, 0, e->stream>>>(va, nt);
-        else k_velocity<false><<<grd, blk, 0, e->stream>>>(va, nt);
-        const int do_dft = (e->nf > 0 && nt % e->ntast == 0) ? 1 : 0;
-        int sample = -1;
-        if (!back && nt == lsamp) {
-            sample = nlsamp++;
-            lsamp += p.ndt;
-        }
-        launch_step_stress(p.nmech, grd, blk, e->stream, sa, nt, do_dft, sample);
+        launch_vel(L, grd, e->stream, nt);
+        int do_dft, sample;
+        step_flags(e, L.back, nt, lsamp, nlsamp, do_dft, sample);
+        launch_str(p.nmech, L, grd, e->stream, nt, do_dft, sample);
     }
 }
 
 // Kernel-by-kernel launches with an event pair around each kernel (kernel timing).
-static int run_loop_profiled(ifosb_engine *e, bool back, const VelArgs &va, const StrArgs &sa, int nshots) {
+static int run_loop_profiled(ifosb_engine *e, const Loop &L) {
     const ifosb_params &p = e->p;
     const size_t need = (size_t)3 * p.nt;
     while (e->events.size() < need) {
@@ -529,21 +711,16 @@ static int run_loop_profiled(ifosb_engine *e, bool back, const VelArgs &va, cons
         CU(cudaEventCreate(&ev));
         e->events.push_back(ev);
     }
-    dim3 blk(BX, BY), grd(e->g.ntk, e->g.nti, e->g.nyc * nshots);
+    dim3 grd(L.lg.ntk, L.lg.nti, L.lg.nyc * L.nshots);
     int lsamp = p.ndtshift + 1, nlsamp = 0;
     for (int nt = 1; nt <= p.nt; ++nt) {
         cudaEvent_t *ev = &e->events[(size_t)3 * (nt - 1)];
         CU(cudaEventRecord(ev[0], e->stream));
-        if (back) k_velocity<true><<<grd, blk, 0, e->stream>>>(va, nt);
-        else k_velocity<false><<<grd, blk, 0, e->stream>>>(va, nt);
+        launch_vel(L, grd, e->stream, nt);
         CU(cudaEventRecord(ev[1], e->stream));
-        const int do_dft = (e->nf > 0 && nt % e->ntast == 0) ? 1 : 0;
-        int sample = -1;
-        if (!back && nt == lsamp) {
-            sample = nlsamp++;
-            lsamp += p.ndt;
-        }
-        launch_step_stress(p.nmech, grd, blk, e->stream, sa, nt, do_dft, sample);
+        int do_dft, sample;
+        step_flags(e, L.back, nt, lsamp, nlsamp, do_dft, sample);
+        launch_str(p.nmech, L, grd, e->stream, nt, do_dft, sample);
         CU(cudaEventRecord(ev[2], e->stream));
     }
     int rc = check_launch(e, "time loop");
@@ -564,23 +741,21 @@ static int run_loop_profiled(ifosb_engine *e, bool back, const VelArgs &va, cons
     return IFOSB_OK;
 }
 
-static int run_loop(ifosb_engine *e, bool back, const VelArgs &va, const StrArgs &sa, int nshots) {
-    GraphCache &gc = back ? e->gadj : e->gfwd;
+static int run_loop(ifosb_engine *e, const Loop &L) {
+    GraphCache &gc = L.back ? e->gadj : e->gfwd;
     e->launches = 2LL * e->p.nt;
-    if (e->profile) return run_loop_profiled(e, back, va, sa, nshots);
+    if (e->profile) return run_loop_profiled(e, L);
     if (e->launch_mode == 1) {
-        enqueue_loop(e, back, va, sa, nshots);
+        enqueue_loop(e, L);
         return check_launch(e, "time loop");
     }
-    std::vector<unsigned char> key(sizeof(VelArgs) + sizeof(StrArgs) + sizeof(int));
-    std::memcpy(key.data(), &va, sizeof(VelArgs));
-    std::memcpy(key.data() + sizeof(VelArgs), &sa, sizeof(StrArgs));
-    std::memcpy(key.data() + sizeof(VelArgs) + sizeof(StrArgs), &nshots, sizeof(int));
+    std::vector<unsigned char> key(sizeof(Loop));
+    std::memcpy(key.data(), &L, sizeof(Loop));
     if (!gc.exec || gc.key != key) {
         release_graph(gc);
         cudaGraph_t graph = nullptr;
         CU(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
-        enqueue_loop(e, back, va, sa, nshots);
+        enqueue_loop(e, L);
         cudaError_t ce = cudaStreamEndCapture(e->stream, &graph);
         if (ce != cudaSuccess) {
             cudaGetLastError();
@@ -601,8 +776,11 @@ static int run_loop(ifosb_engine *e, bool back, const VelArgs &va, const StrArgs
 
 static int check_unstable(ifosb_engine *e, int nshots) {
     std::vector<int> errs(nshots);
+    int terr = 0;
     CU(cudaMemcpyAsync(errs.data(), e->d_err, sizeof(int) * nshots, cudaMemcpyDeviceToHost, e->stream));
+    CU(cudaMemcpyAsync(&terr, e->d_tma_err, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
     CU(cudaStreamSynchronize(e->stream));
+    if (terr) return fail(e, IFOSB_ECUDA, "a TMA stage did not arrive within 1 s (mbarrier wait timed out)");
     for (int s = 0; s < nshots; ++s)
         if (errs[s] != INT_MAX)
             return fail(e, IFOSB_EUNSTABLE,
@@ -616,6 +794,7 @@ static int reset_state(ifosb_engine *e, int nshots, float *dft) {
     if (dft && e->nf > 0) CU(cudaMemsetAsync(dft, 0, sizeof(float) * e->dft_shot * nshots, e->stream));  // zero_invers
     std::vector<int> init(nshots, INT_MAX);
     CU(cudaMemcpyAsync(e->d_err, init.data(), sizeof(int) * nshots, cudaMemcpyHostToDevice, e->stream));
+    CU(cudaMemsetAsync(e->d_tma_err, 0, sizeof(int), e->stream));
     CU(cudaStreamSynchronize(e->stream));  // init lives on the host stack
     return IFOSB_OK;
 }
@@ -657,16 +836,20 @@ extern "C" int ifosb_forward(ifosb_engine *e, int nshots, const ifosb_shot *shot
         }
         for (int t = 0; t < e->ntr; ++t) sp.push_back({s, e->rec[3 * t + 1], e->rec[3 * t], e->rec[3 * t + 2], PT_RECEIVER, t});
     }
+    Loop L;
+    L.nshots = nshots;
+    L.back = false;
+    L.lg = launch_geo(e, nshots);
     int rc;
-    if ((rc = upload_points(e, nshots, vp, &e->d_voff, &e->cap_voff, &e->d_vpts, &e->cap_vpts)) ||
-        (rc = upload_points(e, nshots, sp, &e->d_soff, &e->cap_soff, &e->d_spts, &e->cap_spts)) ||
+    if ((rc = upload_points(e, L.lg, nshots, vp, &e->d_voff, &e->cap_voff, &e->d_vpts, &e->cap_vpts)) ||
+        (rc = upload_points(e, L.lg, nshots, sp, &e->d_soff, &e->cap_soff, &e->d_spts, &e->cap_spts)) ||
         (rc = dgrow(e, &e->d_amp, &e->cap_amp, amp.size())))
         return rc;
     if (!amp.empty()) CU(cudaMemcpyAsync(e->d_amp, amp.data(), amp.size() * sizeof(float), cudaMemcpyHostToDevice, e->stream));
     if ((rc = reset_state(e, nshots, e->d_dftf))) return rc;
-    VelArgs va;
-    StrArgs sa;
-    fill_common(e, va, sa);
+    fill_common(e, L);
+    VelArgs &va = L.va;
+    StrArgs &sa = L.sa;
     va.pt_off = vp.empty() ? nullptr : e->d_voff;
     va.pts = e->d_vpts;
     va.val = e->d_amp;
@@ -678,7 +861,8 @@ extern "C" int ifosb_forward(ifosb_engine *e, int nshots, const ifosb_shot *shot
     sa.amp_row = p.nt;
     sa.dft = e->d_dftf;
     sa.trig = e->d_trig_f;
-    if ((rc = run_loop(e, false, va, sa, nshots))) return rc;
+    L.tma = e->use_tma && setup_tma(e, L, e->d_dftf);
+    if ((rc = run_loop(e, L))) return rc;
     e->nshots = nshots;
     e->fwd_ok = true;
     e->res_ok = e->adj_ok = false;
@@ -721,12 +905,16 @@ extern "C" int ifosb_adjoint(ifosb_engine *e, const float *diff) {
     std::vector<HostPt> vp;
     for (int s = 0; s < nshots; ++s)
         for (int t = 0; t < ntr; ++t) vp.push_back({s, e->rec[3 * t + 1], e->rec[3 * t], e->rec[3 * t + 2], PT_ADJOINT, s * 3 * ntr + t});
+    Loop L;
+    L.nshots = nshots;
+    L.back = true;
+    L.lg = launch_geo(e, nshots);
     int rc;
-    if ((rc = upload_points(e, nshots, vp, &e->d_voff, &e->cap_voff, &e->d_vpts, &e->cap_vpts))) return rc;
+    if ((rc = upload_points(e, L.lg, nshots, vp, &e->d_voff, &e->cap_voff, &e->d_vpts, &e->cap_vpts))) return rc;
     if ((rc = reset_state(e, nshots, e->d_dftb))) return rc;
-    VelArgs va;
-    StrArgs sa;
-    fill_common(e, va, sa);
+    fill_common(e, L);
+    VelArgs &va = L.va;
+    StrArgs &sa = L.sa;
     va.pt_off = vp.empty() ? nullptr : e->d_voff;
     va.pts = e->d_vpts;
     va.val = e->d_diff;
@@ -736,7 +924,8 @@ extern "C" int ifosb_adjoint(ifosb_engine *e, const float *diff) {
     sa.pts = nullptr;
     sa.dft = e->d_dftb;
     sa.trig = e->d_trig_b;
-    if ((rc = run_loop(e, true, va, sa, nshots))) return rc;
+    L.tma = e->use_tma && setup_tma(e, L, e->d_dftb);
+    if ((rc = run_loop(e, L))) return rc;
     if ((rc = check_unstable(e, nshots))) return rc;
     e->adj_ok = true;
     return check_launch(e, "adjoint");
@@ -805,8 +994,10 @@ extern "C" int ifosb_get_field(ifosb_engine *e, int shot, int field, float *out)
     const ifosb_params &p = e->p;
     const Geo &g = e->g;
     const float *src = nullptr;
+    // IFOSB_F_* ids follow the reference's vx, vy, vz, sxx, syy, szz, sxy, syz, sxz
+    static const int slot_of[NEL] = {VX, VY, VZ, SXX, SYY, SZZ, SXY, SYZ, SXZ};
     if (field >= 0 && field < NEL) {
-        src = e->d_state + (long long)shot * e->st_shot + (long long)field * g.field;
+        src = e->d_state + (long long)shot * e->st_shot + (long long)slot_of[field] * g.field;
     } else if (field >= IFOSB_F_DFT_FWD && field < IFOSB_F_DFT_FWD + 6 * e->nf && e->d_dftf) {
         const int q = field - IFOSB_F_DFT_FWD, comp = q / e->nf, l = q % e->nf;
         src = e->d_dftf + (long long)shot * e->dft_shot + ((long long)l * 6 + comp) * g.field;

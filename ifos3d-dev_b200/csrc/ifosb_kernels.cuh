@@ -22,11 +22,14 @@ constexpr int MAXNF = 16;
 constexpr int BX = 32;  // threads along z (contiguous)
 constexpr int BY = 8;   // threads along x
 
-// state field slots of a shot
-enum { VX = 0, VY, VZ, SXX, SYY, SZZ, SXY, SYZ, SXZ, NEL };
+// state field slots of a shot. The stresses with a y derivative in the velocity
+// update (syy, sxy, syz) come first, then the in-plane ones (sxx, szz, sxz), then
+// the memory variables, so each group is one contiguous TMA box.
+enum { VX = 0, VY, VZ, SYY, SXY, SYZ, SXX, SZZ, SXZ, NEL };
 // memory variables: slot NEL + 6*l + q, q: 0 rxx, 1 ryy, 2 rzz, 3 rxy, 4 ryz, 5 rxz
-// model slots (one copy shared by every shot)
-enum { MD_RIP = 0, MD_RJP, MD_RKP, MD_PI, MD_U, MD_UIPJP, MD_UJPKP, MD_UIPKP, MD_TAUS, MD_TAUP, MD_TSIPJP, MD_TSJPKP, MD_TSIPKP, NMODEL };
+// model slots (one copy shared by every shot): the stress update's coefficients
+// first (5, or 10 with non-uniform relaxation times), then the velocity update's.
+enum { MD_PI = 0, MD_U, MD_UIPJP, MD_UJPKP, MD_UIPKP, MD_TAUS, MD_TAUP, MD_TSIPJP, MD_TSJPKP, MD_TSIPKP, MD_RIP, MD_RJP, MD_RKP, NMODEL };
 // CPML coefficient rows
 enum { K_X = 0, A_X, B_X, KH_X, AH_X, BH_X, K_Y, A_Y, B_Y, KH_Y, AH_Y, BH_Y, K_Z, A_Z, B_Z, KH_Z, AH_Z, BH_Z };
 

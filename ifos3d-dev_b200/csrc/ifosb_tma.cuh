@@ -1,0 +1,602 @@
+// TMA-staged time-step kernels (sm_100a).
+//
+// A CTA owns an x-z tile (TZ=32 cells along z, TX=8 along x) of one shot and
+// streams along y through a chunk of planes. Per plane, the Tensor Memory
+// Accelerator brings into shared memory
+//   * the stencil planes with their x/z halos into a ring of RING planes
+//     (velocity kernel: syy, sxy, syz; stress kernel: vx, vy, vz), and
+//   * the point-wise fields of the plane into one of two stage buffers (velocity
+//     kernel: v and rip/rjp/rkp plus the in-plane stencil fields sxx, szz, sxz;
+//     stress kernel: sigma and every memory variable in one 5-D box, the model
+//     coefficients, and the DFT accumulators on DFT steps),
+// each completing on a "full" mbarrier with the byte count of its boxes. One
+// producer warp issues every TMA load; the TX consumer warps compute one row of
+// the tile each and hand a ring plane or a stage back through an "empty"
+// mbarrier once they have read it, so warps never wait on each other through
+// CTA-wide barriers. Results go straight from registers to HBM with coalesced
+// stores (consumers never write shared memory). No cluster multicast is used.
+//
+// Every mbarrier wait is bounded in time (1 s of %globaltimer): on expiry the
+// warp sets the error flag and returns; the other warps' waits then expire in
+// turn, and CTAs that start after the flag is set return at once.
+//
+// The per-cell arithmetic is the expression sequence of the plain kernels in
+// ifosb_kernels.cuh (and of the reference), so the results are bit-identical.
+// With power-of-two grid spacings the divisions by DX, DY, DZ become
+// multiplications by the exact reciprocal, which gives the same bits.
+#pragma once
+#include <cuda.h>
+
+#include "ifosb_kernels.cuh"
+
+namespace ifosb {
+
+constexpr int TZ = 32;    // tile extent along z (== BX)
+constexpr int TX = 8;     // tile extent along x (== BY), one consumer warp per row
+constexpr int RING = 6;   // stencil planes held: j-2..j+2 and the one being loaded
+constexpr int HZ = 4;     // z halo (keeps TMA z-coordinates 16-byte aligned)
+constexpr int HX = 2;     // x halo
+constexpr int RZ = TZ + 2 * HZ;              // ring row length
+constexpr int RX = TX + 2 * HX;              // ring rows
+constexpr int RPLANE = RX * RZ;              // floats per field per ring plane
+constexpr int PT = TX * TZ;                  // floats per point-wise field tile
+constexpr int NTHR = 32 * (TX + 1);          // TX consumer warps + 1 producer warp
+constexpr int NBAR = 2 * RING + 4;           // full/empty per ring slot, full/empty per stage
+
+__device__ __forceinline__ uint32_t su32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *b, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(su32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *b, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(su32(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *b) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(su32(b)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t *b, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(su32(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ uint64_t gtimer() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Bounded wait: gives up after 1 s of wall time (a TMA box lands in microseconds).
+__device__ __forceinline__ bool mbar_wait(uint64_t *b, uint32_t parity) {
+    if (mbar_try(b, parity)) return true;
+    const uint64_t t0 = gtimer();
+    while (!mbar_try(b, parity))
+        if (gtimer() - t0 > 1000000000ull) return false;
+    return true;
+}
+__device__ __forceinline__ void tma_load5(void *dst, const CUtensorMap *m, int c0, int c1, int c2, int c3, int c4,
+                                          uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(su32(dst)),
+        "l"(m), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(su32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void tma_load4(void *dst, const CUtensorMap *m, int c0, int c1, int c2, int c3, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(su32(dst)),
+        "l"(m), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(su32(bar))
+        : "memory");
+}
+
+// Tensor-map coordinates of a cell: z index k+7, row i+1, plane j+2.
+__device__ __forceinline__ int zc(int k) { return k + 7; }
+__device__ __forceinline__ int xc(int i) { return i + 1; }
+__device__ __forceinline__ int yc_(int j) { return j + 2; }
+
+struct VelTma {
+    CUtensorMap m_halo;  // state, box {RZ, RX, 1, 3, 1}
+    CUtensorMap m_pt;    // state, box {TZ, TX, 1, 3, 1}
+    CUtensorMap m_mod;   // model, box {TZ, TX, 1, 3}
+    VelArgs a;
+    int *tma_err;
+};
+
+struct StrTma {
+    CUtensorMap m_halo;  // state, box {RZ, RX, 1, 3, 1}
+    CUtensorMap m_sr;    // state, box {TZ, TX, 1, nsr, 1}
+    CUtensorMap m_mod;   // model, box {TZ, TX, 1, nm}
+    CUtensorMap m_dft;   // DFT accumulators, box {TZ, TX, 1, ndf, 1}
+    StrArgs a;
+    int nsr, nm, ndf;
+    float utaus, utaup, uts_avg;  // uniform taus, taup and their staggered averages (nm == 5)
+    float idx, idy, idz;          // exact 1/DX, 1/DY, 1/DZ (power-of-two spacings)
+    int *tma_err;
+};
+
+__host__ __device__ constexpr size_t vel_tma_smem() {
+    return sizeof(float) * ((size_t)RING * 3 * RPLANE + 2 * ((size_t)3 * RPLANE + 6 * PT)) + 8 * NBAR;
+}
+__host__ __device__ inline size_t str_tma_smem(int nsr, int nm, int ndf) {
+    return sizeof(float) * ((size_t)RING * 3 * RPLANE + 2 * (size_t)(nsr + nm + ndf) * PT) + 8 * NBAR;
+}
+
+// CTA start: returns false (for every thread) if an earlier CTA reported a timeout.
+__device__ __forceinline__ bool pipeline_start(uint64_t *bar, const int *err) {
+    __shared__ int s_go;
+    if (threadIdx.x == 0 && threadIdx.y == TX) {
+        s_go = *(volatile const int *)err == 0;
+        if (s_go) {
+            for (int q = 0; q < RING; ++q) {
+                mbar_init(&bar[q], 1);             // full ring slot
+                mbar_init(&bar[RING + q], TX);     // empty ring slot
+            }
+            for (int b = 0; b < 2; ++b) {
+                mbar_init(&bar[2 * RING + b], 1);  // full stage
+                mbar_init(&bar[2 * RING + 2 + b], TX);  // empty stage
+            }
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+    }
+    __syncthreads();
+    return s_go != 0;
+}
+
+// Consumer side of one plane: wait for the stencil planes and the stage.
+__device__ __forceinline__ bool consumer_wait(uint64_t *bar, int it, int j, int j0, int rfirst) {
+    bool ok = true;
+    if (it == 0) {
+        for (int P = j0 - 2; P <= j0 + 2; ++P) ok &= mbar_wait(&bar[(P - rfirst) % RING], ((P - rfirst) / RING) & 1);
+    } else {
+        const int r = j + 2 - rfirst;
+        ok &= mbar_wait(&bar[r % RING], (r / RING) & 1);
+    }
+    ok &= mbar_wait(&bar[2 * RING + (it & 1)], (it >> 1) & 1);
+    return ok;
+}
+
+// Consumer hands back the ring plane j-2 and the stage of iteration `it`.
+__device__ __forceinline__ void consumer_release(uint64_t *bar, int it) {
+    __syncwarp();
+    if (threadIdx.x == 0) {
+        mbar_arrive(&bar[RING + it % RING]);
+        mbar_arrive(&bar[2 * RING + 2 + (it & 1)]);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Velocity update. Stage layout: [sxx|szz|sxz halo planes][vx vy vz][rip rjp rkp].
+template <bool BACK>
+__global__ void __launch_bounds__(NTHR, 3) k_velocity_tma(const __grid_constant__ VelTma T, int nt) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const VelArgs &a = T.a;
+    const Geo &g = a.g;
+    const int tz = threadIdx.x, tx = threadIdx.y;
+    const int k0 = blockIdx.x * TZ + 1, i0 = blockIdx.y * TX + 1;
+    const int ycn = blockIdx.z % g.nyc, s = blockIdx.z / g.nyc;
+    const int j0 = ycn * g.cy + 1, j1 = min(j0 + g.cy - 1, g.ny);
+    const int n = j1 - j0 + 1;
+    float *ring = reinterpret_cast<float *>(smem);
+    constexpr int SP = 3 * RPLANE + 6 * PT;
+    float *stg = ring + RING * 3 * RPLANE;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(stg + 2 * SP);
+    const int rfirst = j0 - 2, rlast = j1 + 2;
+    if (!pipeline_start(bar, T.tma_err)) return;
+
+    if (tx == TX) {  // ---------------- producer warp
+        if (tz != 0) return;
+        auto ring_load = [&](int P) {
+            const int sl = (P - rfirst) % RING;
+            mbar_expect_tx(&bar[sl], 3 * RPLANE * 4);
+            tma_load5(ring + sl * 3 * RPLANE, &T.m_halo, zc(k0) - HZ, xc(i0) - HX, yc_(P), SYY, s, &bar[sl]);
+        };
+        auto stage_load = [&](int it) {
+            const int j = j0 + it, b = it & 1;
+            float *d = stg + b * SP;
+            uint64_t *fb = &bar[2 * RING + b];
+            mbar_expect_tx(fb, SP * 4);
+            tma_load5(d, &T.m_halo, zc(k0) - HZ, xc(i0) - HX, yc_(j), SXX, s, fb);
+            tma_load5(d + 3 * RPLANE, &T.m_pt, zc(k0), xc(i0), yc_(j), VX, s, fb);
+            tma_load4(d + 3 * RPLANE + 3 * PT, &T.m_mod, zc(k0), xc(i0), yc_(j), MD_RIP, fb);
+        };
+        for (int P = rfirst; P <= min(rfirst + RING - 1, rlast); ++P) ring_load(P);
+        for (int it = 0; it < 2 && it < n; ++it) stage_load(it);
+        for (int it = 0; it < n; ++it) {
+            if (rfirst + it + RING <= rlast) {
+                if (!mbar_wait(&bar[RING + it % RING], (it / RING) & 1)) { atomicExch(T.tma_err, 1); return; }
+                ring_load(rfirst + it + RING);
+            }
+            if (it + 2 < n) {
+                if (!mbar_wait(&bar[2 * RING + 2 + (it & 1)], (it >> 1) & 1)) { atomicExch(T.tma_err, 1); return; }
+                stage_load(it + 2);
+            }
+        }
+        return;
+    }
+
+    // ---------------- consumer warps: row tx of the tile
+    const int k = k0 + tz, i = i0 + tx;
+    const bool active = k <= g.nz && i <= g.nx;
+    int p0, p1;
+    block_points(a.pt_off, g, s, ycn, p0, p1);
+    float *st = a.st + (long long)s * a.st_shot;
+    float *ps = a.psi + (long long)s * a.psi_shot;
+    const long long F = g.field;
+    const float b1 = a.b1, b2 = a.b2, dx = a.dxr, dy = a.dyr, dz = a.dzr;
+    const int hx = face_x(g, i), hz = face_z(g, k);
+    const int cz = tz + HZ, cx = tx + HX;
+    const bool probe_here = a.probe_i == i && a.probe_k == k;
+    int sl = 2;  // ring slot of plane j (plane j0 has ring index 2)
+    for (int it = 0, j = j0; j <= j1; ++it, ++j) {
+        if (!consumer_wait(bar, it, j, j0, rfirst)) { if (tz == 0) atomicExch(T.tma_err, 1); return; }
+        if (active) {
+            const float *stage = stg + (it & 1) * SP;
+            const int sm2 = sl >= 2 ? sl - 2 : sl + RING - 2, sm1 = sl >= 1 ? sl - 1 : sl + RING - 1;
+            const int sp1 = sl + 1 < RING ? sl + 1 : sl + 1 - RING, sp2 = sl + 2 < RING ? sl + 2 : sl + 2 - RING;
+            const float *R0 = ring + sl * 3 * RPLANE + cx * RZ + cz;
+            const float *Rm2 = ring + sm2 * 3 * RPLANE + cx * RZ + cz, *Rm1 = ring + sm1 * 3 * RPLANE + cx * RZ + cz;
+            const float *Rp1 = ring + sp1 * 3 * RPLANE + cx * RZ + cz, *Rp2 = ring + sp2 * 3 * RPLANE + cx * RZ + cz;
+            const float *Ip = stage + cx * RZ + cz;
+            // ring fields: 0 syy, 1 sxy, 2 syz; stage in-plane fields: 0 sxx, 1 szz, 2 sxz
+#define RF(Rp, f, x, z) Rp[(f) * RPLANE + (x) * RZ + (z)]
+#define IP(f, x, z) Ip[(f) * RPLANE + (x) * RZ + (z)]
+            float sxx_x = dx * (b1 * (IP(0, 1, 0) - IP(0, 0, 0)) + b2 * (IP(0, 2, 0) - IP(0, -1, 0)));
+            float sxy_y = dy * (b1 * (RF(R0, 1, 0, 0) - RF(Rm1, 1, 0, 0)) + b2 * (RF(Rp1, 1, 0, 0) - RF(Rm2, 1, 0, 0)));
+            float sxz_z = dz * (b1 * (IP(2, 0, 0) - IP(2, 0, -1)) + b2 * (IP(2, 0, 1) - IP(2, 0, -2)));
+            float syy_y = dy * (b1 * (RF(Rp1, 0, 0, 0) - RF(R0, 0, 0, 0)) + b2 * (RF(Rp2, 0, 0, 0) - RF(Rm1, 0, 0, 0)));
+            float sxy_x = dx * (b1 * (RF(R0, 1, 0, 0) - RF(R0, 1, -1, 0)) + b2 * (RF(R0, 1, 1, 0) - RF(R0, 1, -2, 0)));
+            float syz_z = dz * (b1 * (RF(R0, 2, 0, 0) - RF(R0, 2, 0, -1)) + b2 * (RF(R0, 2, 0, 1) - RF(R0, 2, 0, -2)));
+            float szz_z = dz * (b1 * (IP(1, 0, 1) - IP(1, 0, 0)) + b2 * (IP(1, 0, 2) - IP(1, 0, -1)));
+            float sxz_x = dx * (b1 * (IP(2, 0, 0) - IP(2, -1, 0)) + b2 * (IP(2, 1, 0) - IP(2, -2, 0)));
+            float syz_y = dy * (b1 * (RF(R0, 2, 0, 0) - RF(Rm1, 2, 0, 0)) + b2 * (RF(Rp1, 2, 0, 0) - RF(Rm2, 2, 0, 0)));
+#undef RF
+#undef IP
+            const int hy = face_y(g, j);
+            const bool frame = hx || hy || hz;
+            if (hx) {
+                float *p = ps + sxi(g, j, hx, k);
+                const long long o = a.sl.sx;
+                float v0 = CP(BH_X, hx) * p[0] + CP(AH_X, hx) * sxx_x; p[0] = v0; sxx_x = sxx_x / CP(KH_X, hx) + v0;
+                float v1 = CP(B_X, hx) * p[o] + CP(A_X, hx) * sxy_x; p[o] = v1; sxy_x = sxy_x / CP(K_X, hx) + v1;
+                float v2 = CP(B_X, hx) * p[2 * o] + CP(A_X, hx) * sxz_x; p[2 * o] = v2; sxz_x = sxz_x / CP(K_X, hx) + v2;
+            }
+            if (hy) {
+                float *p = ps + 3 * a.sl.sx + syi(g, hy, i, k);
+                const long long o = a.sl.sy;
+                float v0 = CP(B_Y, hy) * p[0] + CP(A_Y, hy) * sxy_y; p[0] = v0; sxy_y = sxy_y / CP(K_Y, hy) + v0;
+                float v1 = CP(BH_Y, hy) * p[o] + CP(AH_Y, hy) * syy_y; p[o] = v1; syy_y = syy_y / CP(KH_Y, hy) + v1;
+                float v2 = CP(B_Y, hy) * p[2 * o] + CP(A_Y, hy) * syz_y; p[2 * o] = v2; syz_y = syz_y / CP(K_Y, hy) + v2;
+            }
+            if (hz) {
+                float *p = ps + 3 * a.sl.sx + 3 * a.sl.sy + szi(g, j, i, hz);
+                const long long o = a.sl.sz;
+                float v0 = CP(B_Z, hz) * p[0] + CP(A_Z, hz) * sxz_z; p[0] = v0; sxz_z = sxz_z / CP(K_Z, hz) + v0;
+                float v1 = CP(B_Z, hz) * p[o] + CP(A_Z, hz) * syz_z; p[o] = v1; syz_z = syz_z / CP(K_Z, hz) + v1;
+                float v2 = CP(BH_Z, hz) * p[2 * o] + CP(AH_Z, hz) * szz_z; p[2 * o] = v2; szz_z = szz_z / CP(KH_Z, hz) + v2;
+            }
+            const float *pv = stage + 3 * RPLANE + tx * TZ + tz;
+            const long long c = widx(g, j, i, k);
+            float *V = st + c;
+            if (p1 > p0) {
+                // cells of this block hold point forces: the order of update_v / update_v_CPML
+                V[VX * F] = pv[0]; V[VY * F] = pv[PT]; V[VZ * F] = pv[2 * PT];
+                if (frame) vel_points<BACK>(a, st, p0, p1, j, i, k, nt, c);
+                V[VX * F] = V[VX * F] + (sxx_x + sxy_y + sxz_z) / pv[3 * PT];
+                V[VY * F] = V[VY * F] + (syy_y + sxy_x + syz_z) / pv[4 * PT];
+                V[VZ * F] = V[VZ * F] + (szz_z + sxz_x + syz_y) / pv[5 * PT];
+                const int passes = frame ? (BACK ? 1 : 0) : (BACK ? 2 : 1);
+                for (int pass = 0; pass < passes; ++pass) vel_points<BACK>(a, st, p0, p1, j, i, k, nt, c);
+            } else {
+                V[VX * F] = pv[0] + (sxx_x + sxy_y + sxz_z) / pv[3 * PT];
+                V[VY * F] = pv[PT] + (syy_y + sxy_x + syz_z) / pv[4 * PT];
+                V[VZ * F] = pv[2 * PT] + (szz_z + sxz_x + syz_y) / pv[5 * PT];
+            }
+            if (probe_here && j == a.probe_j && isnan(V[VY * F])) atomicMin(a.err_step + s, nt);
+        }
+        consumer_release(bar, it);
+        sl = sl + 1 < RING ? sl + 1 : 0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Stress update (+ source, DFT, free surface, receivers).
+// Stage layout: [sigma(6) r(6L)][model(nm)][dft(6 nf) on DFT steps].
+template <bool P2>
+__device__ __forceinline__ float ddiv(float a, float d, float inv) {
+    if constexpr (P2) return a * inv;
+    else return a / d;
+}
+
+template <int L, bool P2>
+__global__ void __launch_bounds__(NTHR, 2) k_stress_tma(const __grid_constant__ StrTma T, int nt, int do_dft, int sample) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const StrArgs &a = T.a;
+    const Geo &g = a.g;
+    const int tz = threadIdx.x, tx = threadIdx.y;
+    const int k0 = blockIdx.x * TZ + 1, i0 = blockIdx.y * TX + 1;
+    const int ycn = blockIdx.z % g.nyc, s = blockIdx.z / g.nyc;
+    const int j0 = ycn * g.cy + 1, j1 = min(j0 + g.cy - 1, g.ny);
+    const int n = j1 - j0 + 1;
+    const int nsr = T.nsr, nm = T.nm, ndf = do_dft ? T.ndf : 0;
+    const int SP = (nsr + nm + T.ndf) * PT;
+    float *ring = reinterpret_cast<float *>(smem);
+    float *stg = ring + RING * 3 * RPLANE;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(stg + 2 * SP);
+    const int rfirst = j0 - 2, rlast = j1 + 2;
+    if (!pipeline_start(bar, T.tma_err)) return;
+
+    if (tx == TX) {  // ---------------- producer warp
+        if (tz != 0) return;
+        const uint32_t stage_bytes = (uint32_t)(nsr + nm + ndf) * PT * 4;
+        auto ring_load = [&](int P) {
+            const int sl = (P - rfirst) % RING;
+            mbar_expect_tx(&bar[sl], 3 * RPLANE * 4);
+            tma_load5(ring + sl * 3 * RPLANE, &T.m_halo, zc(k0) - HZ, xc(i0) - HX, yc_(P), VX, s, &bar[sl]);
+        };
+        auto stage_load = [&](int it) {
+            const int j = j0 + it, b = it & 1;
+            float *d = stg + b * SP;
+            uint64_t *fb = &bar[2 * RING + b];
+            mbar_expect_tx(fb, stage_bytes);
+            tma_load5(d, &T.m_sr, zc(k0), xc(i0), yc_(j), SYY, s, fb);
+            tma_load4(d + nsr * PT, &T.m_mod, zc(k0), xc(i0), yc_(j), 0, fb);
+            if (ndf) tma_load5(d + (nsr + nm) * PT, &T.m_dft, zc(k0), xc(i0), yc_(j), 0, s, fb);
+        };
+        for (int P = rfirst; P <= min(rfirst + RING - 1, rlast); ++P) ring_load(P);
+        for (int it = 0; it < 2 && it < n; ++it) stage_load(it);
+        for (int it = 0; it < n; ++it) {
+            if (rfirst + it + RING <= rlast) {
+                if (!mbar_wait(&bar[RING + it % RING], (it / RING) & 1)) { atomicExch(T.tma_err, 1); return; }
+                ring_load(rfirst + it + RING);
+            }
+            if (it + 2 < n) {
+                if (!mbar_wait(&bar[2 * RING + 2 + (it & 1)], (it >> 1) & 1)) { atomicExch(T.tma_err, 1); return; }
+                stage_load(it + 2);
+            }
+        }
+        return;
+    }
+
+    // ---------------- consumer warps: row tx of the tile
+    const int k = k0 + tz, i = i0 + tx;
+    const bool active = k <= g.nz && i <= g.nx;
+    int p0, p1;
+    block_points(a.pt_off, g, s, ycn, p0, p1);
+    float *st = a.st + (long long)s * a.st_shot;
+    float *ps = a.psi + (long long)s * a.psi_shot + 3 * (a.sl.sx + a.sl.sy + a.sl.sz);
+    const long long F = g.field, dJ = g.plane;
+    const float b1 = a.b1, b2 = a.b2, DX = a.rdx, DY = a.rdy, DZ = a.rdz, DT = a.dt;
+    const float iX = T.idx, iY = T.idy, iZ = T.idz;
+    const int hx = face_x(g, i), hz = face_z(g, k);
+    const bool zfront = k <= g.fw;
+    const int cz = tz + HZ, cx = tx + HX;
+    int sl = 2;
+    for (int it = 0, j = j0; j <= j1; ++it, ++j) {
+        if (!consumer_wait(bar, it, j, j0, rfirst)) { if (tz == 0) atomicExch(T.tma_err, 1); return; }
+        if (active) {
+            const float *stage = stg + (it & 1) * SP;
+            const int sm2 = sl >= 2 ? sl - 2 : sl + RING - 2, sm1 = sl >= 1 ? sl - 1 : sl + RING - 1;
+            const int sp1 = sl + 1 < RING ? sl + 1 : sl + 1 - RING, sp2 = sl + 2 < RING ? sl + 2 : sl + 2 - RING;
+            const float *R0 = ring + sl * 3 * RPLANE + cx * RZ + cz;
+            const float *Rm2 = ring + sm2 * 3 * RPLANE + cx * RZ + cz, *Rm1 = ring + sm1 * 3 * RPLANE + cx * RZ + cz;
+            const float *Rp1 = ring + sp1 * 3 * RPLANE + cx * RZ + cz, *Rp2 = ring + sp2 * 3 * RPLANE + cx * RZ + cz;
+#define RF(Rp, f, x, z) Rp[(f) * RPLANE + (x) * RZ + (z)]
+            const float vx0 = RF(R0, 0, 0, 0), vy0 = RF(R0, 1, 0, 0), vz0 = RF(R0, 2, 0, 0);
+            float vxx = ddiv<P2>(b1 * (vx0 - RF(R0, 0, -1, 0)) + b2 * (RF(R0, 0, 1, 0) - RF(R0, 0, -2, 0)), DX, iX);
+            float vxy = ddiv<P2>(b1 * (RF(Rp1, 0, 0, 0) - vx0) + b2 * (RF(Rp2, 0, 0, 0) - RF(Rm1, 0, 0, 0)), DY, iY);
+            float vxz = ddiv<P2>(b1 * (RF(R0, 0, 0, 1) - vx0) + b2 * (RF(R0, 0, 0, 2) - RF(R0, 0, 0, -1)), DZ, iZ);
+            float vyx = ddiv<P2>(b1 * (RF(R0, 1, 1, 0) - vy0) + b2 * (RF(R0, 1, 2, 0) - RF(R0, 1, -1, 0)), DX, iX);
+            float vyy = ddiv<P2>(b1 * (vy0 - RF(Rm1, 1, 0, 0)) + b2 * (RF(Rp1, 1, 0, 0) - RF(Rm2, 1, 0, 0)), DY, iY);
+            float vyz = ddiv<P2>(b1 * (RF(R0, 1, 0, 1) - vy0) + b2 * (RF(R0, 1, 0, 2) - RF(R0, 1, 0, -1)), DZ, iZ);
+            float vzx = ddiv<P2>(b1 * (RF(R0, 2, 1, 0) - vz0) + b2 * (RF(R0, 2, 2, 0) - RF(R0, 2, -1, 0)), DX, iX);
+            float vzy = ddiv<P2>(b1 * (RF(Rp1, 2, 0, 0) - vz0) + b2 * (RF(Rp2, 2, 0, 0) - RF(Rm1, 2, 0, 0)), DY, iY);
+            float vzz = ddiv<P2>(b1 * (vz0 - RF(R0, 2, 0, -1)) + b2 * (RF(R0, 2, 0, 1) - RF(R0, 2, 0, -2)), DZ, iZ);
+#undef RF
+            const float svxx = vxx, svyy = vyy, svzz = vzz;  // the free surface uses the plain derivatives
+            const int hy = face_y(g, j);
+            if (hx) {
+                float *p = ps + sxi(g, j, hx, k);
+                const long long o = a.sl.sx;
+                float v0 = CP(B_X, hx) * p[0] + CP(A_X, hx) * vxx; p[0] = v0; vxx = vxx / CP(K_X, hx) + v0;
+                float v1 = CP(BH_X, hx) * p[o] + CP(AH_X, hx) * vyx; p[o] = v1; vyx = vyx / CP(KH_X, hx) + v1;
+                float v2 = CP(BH_X, hx) * p[2 * o] + CP(AH_X, hx) * vzx; p[2 * o] = v2; vzx = vzx / CP(KH_X, hx) + v2;
+            }
+            if (hy) {
+                float *p = ps + 3 * a.sl.sx + syi(g, hy, i, k);
+                const long long o = a.sl.sy;
+                float v0 = CP(BH_Y, hy) * p[0] + CP(AH_Y, hy) * vxy; p[0] = v0; vxy = vxy / CP(KH_Y, hy) + v0;
+                float v1 = CP(B_Y, hy) * p[o] + CP(A_Y, hy) * vyy; p[o] = v1; vyy = vyy / CP(K_Y, hy) + v1;
+                float v2 = CP(BH_Y, hy) * p[2 * o] + CP(AH_Y, hy) * vzy; p[2 * o] = v2; vzy = vzy / CP(KH_Y, hy) + v2;
+            }
+            if (hz) {
+                // the reference divides by K_y on the front z face (update_s_ssg_CPML_elastic.c:104-108)
+                float *p = ps + 3 * a.sl.sx + 3 * a.sl.sy + szi(g, j, i, hz);
+                const long long o = a.sl.sz;
+                const float kh = zfront ? CP(KH_Y, hz) : CP(KH_Z, hz);
+                const float kf = zfront ? CP(K_Y, hz) : CP(K_Z, hz);
+                float v0 = CP(BH_Z, hz) * p[0] + CP(AH_Z, hz) * vxz; p[0] = v0; vxz = vxz / kh + v0;
+                float v1 = CP(BH_Z, hz) * p[o] + CP(AH_Z, hz) * vyz; p[o] = v1; vyz = vyz / kh + v1;
+                float v2 = CP(B_Z, hz) * p[2 * o] + CP(A_Z, hz) * vzz; p[2 * o] = v2; vzz = vzz / kf + v2;
+            }
+            const float *S = stage + tx * TZ + tz;      // sigma + memory variables (old values)
+            const float *Mo = S + nsr * PT;             // model
+            const float pim = Mo[MD_PI * PT], um = Mo[MD_U * PT];
+            const float uipjp = Mo[MD_UIPJP * PT], ujpkp = Mo[MD_UJPKP * PT], uipkp = Mo[MD_UIPKP * PT];
+            const float vxyyx = vxy + vyx, vyzzy = vyz + vzy, vxzzx = vxz + vzx;
+            const float vxxyyzz = vxx + vyy + vzz, vyyzz = vyy + vzz, vxxzz = vxx + vzz, vxxyy = vxx + vyy;
+            // stage order of sigma: syy, sxy, syz, sxx, szz, sxz (state slots 3..8)
+            float syy = S[0], sxy = S[PT], syz = S[2 * PT], sxx = S[3 * PT], szz = S[4 * PT], sxz = S[5 * PT];
+            const long long c = widx(g, j, i, k);
+            float *O = st + c;
+            const bool surf = g.free_surf && j == 1;
+            float taus = 0.f, taup = 0.f, sr[6];
+            if constexpr (L == 0) {
+                const float fipjp = uipjp * DT, fjpkp = ujpkp * DT, fipkp = uipkp * DT;
+                const float gg = pim, f = (float)(2.0 * (double)um);
+                sxy += (fipjp * vxyyx);
+                syz += (fjpkp * vyzzy);
+                sxz += (fipkp * vxzzx);
+                sxx += DT * ((gg * vxxyyzz) - (f * vyyzz));
+                syy += DT * ((gg * vxxyyzz) - (f * vxxzz));
+                szz += DT * ((gg * vxxyyzz) - (f * vxxyy));
+            } else {
+                float tausipjp, tausjpkp, tausipkp;
+                if (nm == 5) {
+                    taus = T.utaus; taup = T.utaup;
+                    tausipjp = tausjpkp = tausipkp = T.uts_avg;
+                } else {
+                    taus = Mo[MD_TAUS * PT]; taup = Mo[MD_TAUP * PT];
+                    tausipjp = Mo[MD_TSIPJP * PT]; tausjpkp = Mo[MD_TSJPKP * PT]; tausipkp = Mo[MD_TSIPKP * PT];
+                }
+                const float Lf = (float)L, dthalbe = a.dthalbe;
+                const float *R = S + 6 * PT;  // r[l][q] at (6 l + q) PT
+#pragma unroll
+                for (int q = 0; q < 6; ++q) {
+                    sr[q] = R[q * PT];
+#pragma unroll
+                    for (int l = 1; l < L; ++l) sr[q] += R[(6 * l + q) * PT];
+                }
+                const float fipjp = (float)((double)(uipjp * DT) * (1.0 + (double)(Lf * tausipjp)));
+                const float fjpkp = (float)((double)(ujpkp * DT) * (1.0 + (double)(Lf * tausjpkp)));
+                const float fipkp = (float)((double)(uipkp * DT) * (1.0 + (double)(Lf * tausipkp)));
+                const float gg = (float)((double)pim * (1.0 + (double)(Lf * taup)));
+                const float f = (float)((2.0 * (double)um) * (1.0 + (double)(Lf * taus)));
+                sxy += (fipjp * vxyyx) + (dthalbe * sr[3]);
+                syz += (fjpkp * vyzzy) + (dthalbe * sr[4]);
+                sxz += (fipkp * vxzzx) + (dthalbe * sr[5]);
+                sxx += DT * ((gg * vxxyyzz) - (f * vyyzz)) + (dthalbe * sr[0]);
+                syy += DT * ((gg * vxxyyzz) - (f * vxxzz)) + (dthalbe * sr[1]);
+                szz += DT * ((gg * vxxyyzz) - (f * vxxyy)) + (dthalbe * sr[2]);
+                // memory variables, one mechanism at a time from the stage's old values
+#pragma unroll
+                for (int l = 0; l < L; ++l) {
+                    const float eta = a.eta[l], bb = a.mb[l], cc = a.mc[l];
+                    const float dipjp = uipjp * eta * tausipjp, djpkp = ujpkp * eta * tausjpkp, dipkp = uipkp * eta * tausipkp;
+                    const float d = (float)(((2.0 * (double)um) * (double)eta) * (double)taus);
+                    const float e = pim * eta * taup;
+                    const float *Rl = R + 6 * l * PT;
+                    const float nxy = bb * (Rl[3 * PT] * cc - (dipjp * vxyyx));
+                    const float nyz = bb * (Rl[4 * PT] * cc - (djpkp * vyzzy));
+                    const float nxz = bb * (Rl[5 * PT] * cc - (dipkp * vxzzx));
+                    const float nxx = bb * (Rl[0] * cc - (e * vxxyyzz) + (d * vyyzz));
+                    const float nyy = bb * (Rl[PT] * cc - (e * vxxyyzz) + (d * vxxzz));
+                    const float nzz = bb * (Rl[2 * PT] * cc - (e * vxxyyzz) + (d * vxxyy));
+                    if (l == 0) {
+                        sr[0] = nxx; sr[1] = nyy; sr[2] = nzz; sr[3] = nxy; sr[4] = nyz; sr[5] = nxz;
+                    } else {
+                        sr[0] += nxx; sr[1] += nyy; sr[2] += nzz; sr[3] += nxy; sr[4] += nyz; sr[5] += nxz;
+                    }
+                    if (!surf) {
+                        float *Ol = O + (NEL + 6 * l) * F;
+                        Ol[0] = nxx; Ol[F] = nyy; Ol[2 * F] = nzz; Ol[3 * F] = nxy; Ol[4 * F] = nyz; Ol[5 * F] = nxz;
+                    }
+                }
+                sxy += (dthalbe * sr[3]);
+                syz += (dthalbe * sr[4]);
+                sxz += (dthalbe * sr[5]);
+                sxx += (dthalbe * sr[0]);
+                syy += (dthalbe * sr[1]);
+                szz += (dthalbe * sr[2]);
+            }
+            if (p1 > p0) {
+                for (int q = p0; q < p1; ++q) {
+                    const Pt pt = a.pts[q];
+                    if (pt.kind == PT_EXPLOSIVE && pt.j == j && pt.i == i && pt.k == k) {
+                        const float amp = a.amp[(long long)pt.row * a.amp_row + (nt - 1)];
+                        sxx += amp; syy += amp; szz += amp;
+                    }
+                }
+            }
+            if (ndf) {
+                const float *Fs = S + (nsr + nm) * PT;
+                float *Fd = a.dft + (long long)s * a.dft_shot + c;
+                const double *tr = a.trig + (long long)(nt - 1) * a.nf * 2;
+                for (int l = 0; l < a.nf; ++l) {
+                    const double t1 = tr[2 * l], t2 = tr[2 * l + 1];
+                    const float *Fl = Fs + l * 6 * PT;
+                    float *Gl = Fd + (long long)l * 6 * F;
+                    Gl[0 * F] = (float)((double)Fl[0 * PT] + (double)vx0 * t1);
+                    Gl[1 * F] = (float)((double)Fl[1 * PT] + (double)vy0 * t1);
+                    Gl[2 * F] = (float)((double)Fl[2 * PT] + (double)vz0 * t1);
+                    Gl[3 * F] = (float)((double)Fl[3 * PT] + (double)vx0 * t2);
+                    Gl[4 * F] = (float)((double)Fl[4 * PT] + (double)vy0 * t2);
+                    Gl[5 * F] = (float)((double)Fl[5 * PT] + (double)vz0 * t2);
+                }
+            }
+            if (surf) {
+                // surface_ssg_elastic.c:69-111 / surface_ssg.c:117-160
+                syy = 0.0f;
+                if constexpr (L == 0) {
+                    const float f = (float)((double)um * 2.0), gg = pim;
+                    const float h = -(DT * (gg - f) * (gg - f) * (svxx + svzz) / gg) - (DT * (gg - f) * svyy);
+                    sxx += h;
+                    szz += h;
+                } else {
+                    const float Lf = (float)L, dthalbe = a.dthalbe;
+                    const float f = (float)(((double)um * 2.0) * (1.0 + (double)(Lf * taus)));
+                    const float gg = (float)((double)pim * (1.0 + (double)(Lf * taup)));
+                    const float h = -(DT * (gg - f) * (gg - f) * (svxx + svzz) / gg) - (DT * (gg - f) * svyy);
+                    sxx += h - (dthalbe * sr[0]);
+                    szz += h - (dthalbe * sr[2]);
+                    const float d = (float)((2.0 * (double)um) * (double)taus);
+                    const float e = pim * taup;
+                    // the memory variables of the surface row: recompute each mechanism's
+                    // update (same bits), apply the surface term, then store
+                    const float *R = S + 6 * PT;
+                    const float tausipjp = nm == 5 ? T.uts_avg : Mo[MD_TSIPJP * PT];
+                    const float tausjpkp = nm == 5 ? T.uts_avg : Mo[MD_TSJPKP * PT];
+                    const float tausipkp = nm == 5 ? T.uts_avg : Mo[MD_TSIPKP * PT];
+                    float srx = 0.f, srz = 0.f;
+#pragma unroll
+                    for (int l = 0; l < L; ++l) {
+                        const float eta = a.eta[l], bb = a.mb[l], cc = a.mc[l];
+                        const float dipjp = uipjp * eta * tausipjp, djpkp = ujpkp * eta * tausjpkp, dipkp = uipkp * eta * tausipkp;
+                        const float dd = (float)(((2.0 * (double)um) * (double)eta) * (double)taus);
+                        const float ee = pim * eta * taup;
+                        const float *Rl = R + 6 * l * PT;
+                        const float nxy = bb * (Rl[3 * PT] * cc - (dipjp * vxyyx));
+                        const float nyz = bb * (Rl[4 * PT] * cc - (djpkp * vyzzy));
+                        const float nxz = bb * (Rl[5 * PT] * cc - (dipkp * vxzzx));
+                        float nxx = bb * (Rl[0] * cc - (ee * vxxyyzz) + (dd * vyyzz));
+                        float nzz = bb * (Rl[2 * PT] * cc - (ee * vxxyyzz) + (dd * vxxyy));
+                        const float hh = (float)((double)a.msb[l] *
+                                                 ((((double)(d - e) * ((double)(f / gg) - 1.0)) * (double)(svxx + svzz)) -
+                                                  (double)((d - e) * svyy)));
+                        nxx += hh;
+                        nzz += hh;
+                        if (l == 0) { srx = nxx; srz = nzz; } else { srx += nxx; srz += nzz; }
+                        float *Ol = O + (NEL + 6 * l) * F;
+                        Ol[0] = nxx; Ol[F] = 0.0f; Ol[2 * F] = nzz; Ol[3 * F] = nxy; Ol[4 * F] = nyz; Ol[5 * F] = nxz;
+                    }
+                    sxx += (dthalbe * srx);
+                    szz += (dthalbe * srz);
+                }
+            }
+            O[SYY * F] = syy; O[SXY * F] = sxy; O[SYZ * F] = syz;
+            O[SXX * F] = sxx; O[SZZ * F] = szz; O[SXZ * F] = sxz;
+            if (g.free_surf && j <= 3) {
+                if (j == 1) { O[SXY * F - dJ] = -sxy; O[SYZ * F - dJ] = -syz; }
+                if (j == 2) { O[SYY * F - 2 * dJ] = -syy; O[SXY * F - 3 * dJ] = -sxy; O[SYZ * F - 3 * dJ] = -syz; }
+                if (j == 3) { O[SYY * F - 4 * dJ] = -syy; }
+            }
+            if (sample >= 0 && p1 > p0) {
+                for (int q = p0; q < p1; ++q) {
+                    const Pt pt = a.pts[q];
+                    if (pt.kind == PT_RECEIVER && pt.j == j && pt.i == i && pt.k == k) {
+                        float *o = a.sec + (long long)s * a.sec_shot + (long long)pt.row * a.sec_tr + sample;
+                        o[0] = vx0;
+                        o[a.sec_comp] = vy0;
+                        o[2 * a.sec_comp] = vz0;
+                    }
+                }
+            }
+        }
+        consumer_release(bar, it);
+        sl = sl + 1 < RING ? sl + 1 : 0;
+    }
+}
+
+}  // namespace ifosb

@@ -118,6 +118,21 @@ def test_plain_launch_mode_matches(oracle, request):
     check_case(c, pick_oracle(1, oracle, request), launch_mode=1)
 
 
+@pytest.mark.parametrize("nmech", [0, 3])
+def test_untiled_kernels_match(nmech, oracle, request, monkeypatch):
+    """The kernels without TMA staging (IFOSB_TMA=0) give the same bits."""
+    monkeypatch.setenv("IFOSB_TMA", "0")
+    c = synth.small_case(nt=50, nmech=nmech, seed=13, nshots=2)
+    check_case(c, pick_oracle(nmech, oracle, request))
+
+
+def test_tile_edges_and_long_chunks(oracle, request):
+    """Grid sizes that are not multiples of the 32x8 tile, several shots, and a y
+    extent long enough for multi-plane chunks with ring reuse."""
+    c = synth.small_case(nx=37, ny=70, nz=45, nt=30, fw=6, nshots=3, seed=17)
+    check_case(c, pick_oracle(0, oracle, request))
+
+
 @pytest.mark.parametrize("stype", [2, 3, 4, 5])
 def test_body_force_sources(stype, oracle, request):
     """Single forces (update_v_ssg.c:474-510), including the reference's rjp/rkp
