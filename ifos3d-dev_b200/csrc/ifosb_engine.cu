@@ -82,6 +82,7 @@ struct ifosb_engine {
     // TMA staging (default) and its wait-timeout flag
     int use_tma = 1;
     int *d_tma_err = nullptr;
+    float *d_cpg = nullptr;  // CPML rows in global memory (lane-divergent reads)
     // uniform relaxation times: passed as scalars instead of five model fields
     bool unif_tau = false;
     float utaus = 0.f, utaup = 0.f, uts_avg = 0.f;
@@ -283,7 +284,7 @@ extern "C" void ifosb_destroy(ifosb_engine *e) {
     release_graph(e->gadj);
     void *bufs[] = {e->d_state, e->d_psi, e->d_model, e->d_rho_w, e->d_dftf, e->d_dftb, e->d_grad, e->d_grad64,
                     e->d_err, e->d_sec, e->d_diff, e->d_obs, e->d_part, e->d_misfit, e->d_l2, e->d_trig_f,
-                    e->d_trig_b, e->d_voff, e->d_soff, e->d_vpts, e->d_spts, e->d_amp, e->d_tma_err};
+                    e->d_trig_b, e->d_voff, e->d_soff, e->d_vpts, e->d_spts, e->d_amp, e->d_tma_err, e->d_cpg};
     for (void *b : bufs)
         if (b) cudaFree(b);
     for (cudaEvent_t ev : e->events) cudaEventDestroy(ev);
@@ -334,6 +335,11 @@ extern "C" int ifosb_set_cpml(ifosb_engine *e, const float *coeff) {
     for (int r = 0; r < 18; ++r)
         for (int h = 0; h < n2; ++h) host[(size_t)r * 2 * MAXFW + h] = coeff[(size_t)r * n2 + h];
     CU(cudaMemcpyToSymbol(c_cpml, host.data(), host.size() * sizeof(float)));
+    if (!e->d_cpg) {
+        int rc = dalloc(e, &e->d_cpg, host.size());
+        if (rc) return rc;
+    }
+    CU(cudaMemcpy(e->d_cpg, host.data(), host.size() * sizeof(float), cudaMemcpyHostToDevice));
     e->have_cpml = true;
     return IFOSB_OK;
 }
@@ -527,6 +533,7 @@ static void fill_common(ifosb_engine *e, Loop &L) {
         va.cf5z = sb * ca;
     }
     va.err_step = e->d_err;
+    va.cpg = sa.cpg = e->d_cpg;
     va.probe_j = p.ny / 2; va.probe_i = p.nx / 2; va.probe_k = p.nz / 2;  // ifos3d.c:761
     sa.dt = p.dt;
     sa.dthalbe = p.dt / 2.0;

@@ -59,6 +59,9 @@ enum { PT_EXPLOSIVE = 1, PT_ADJOINT = 6, PT_RECEIVER = 7 };
 __constant__ float c_cpml[18][2 * MAXFW];
 
 __device__ __forceinline__ float CP(int row, int h) { return c_cpml[row][h - 1]; }
+// z-face slab indices differ between the lanes of a warp; the constant cache would
+// serialise them, L1 serves them in one pass
+__device__ __forceinline__ float CPG(const float *cpg, int row, int h) { return __ldg(cpg + row * 2 * MAXFW + h - 1); }
 
 // CPML frame membership (CPML_ini_elastic.c:26-71): 1-based slab index or 0.
 __device__ __forceinline__ int face_x(const Geo &g, int i) {
@@ -102,6 +105,7 @@ struct VelArgs {
     float dxr, dyr, dzr;  // DT/DX, DT/DY, DT/DZ
     float b1, b2;
     double cf5x, cf5y, cf5z;  // type-5 force direction factors (update_v_ssg.c:498-503)
+    const float *cpg;         // global copy of the CPML rows, for lane-divergent (z-face) reads
     int *err_step;        // [nshots] first step whose probe cell went NaN
     int probe_j, probe_i, probe_k;
 };
@@ -127,6 +131,7 @@ struct StrArgs {
     float dt, dthalbe, rdx, rdy, rdz;
     float b1, b2;
     float eta[MAXMECH], mb[MAXMECH], mc[MAXMECH], msb[MAXMECH];
+    const float *cpg;     // global copy of the CPML rows, for lane-divergent (z-face) reads
 };
 
 __device__ __forceinline__ void block_points(const int *pt_off, const Geo &g, int s, int yc, int &p0, int &p1) {

@@ -92,6 +92,24 @@ __device__ __forceinline__ void tma_load4(void *dst, const CUtensorMap *m, int c
         : "memory");
 }
 
+// L2 prefetch of a box (no shared memory, no completion): warms L2 for a later load.
+__device__ __forceinline__ void tma_prefetch5(const CUtensorMap *m, int c0, int c1, int c2, int c3, int c4) {
+    asm volatile("cp.async.bulk.prefetch.tensor.5d.L2.global.tile [%0, {%1, %2, %3, %4, %5}];" ::"l"(m), "r"(c0), "r"(c1),
+                 "r"(c2), "r"(c3), "r"(c4)
+                 : "memory");
+}
+__device__ __forceinline__ void tma_prefetch4(const CUtensorMap *m, int c0, int c1, int c2, int c3) {
+    asm volatile("cp.async.bulk.prefetch.tensor.4d.L2.global.tile [%0, {%1, %2, %3, %4}];" ::"l"(m), "r"(c0), "r"(c1), "r"(c2),
+                 "r"(c3)
+                 : "memory");
+}
+
+// Planes are prefetched into L2 this many iterations before their shared-memory load.
+#ifndef IFOSB_L2_AHEAD
+#define IFOSB_L2_AHEAD 3
+#endif
+constexpr int L2AHEAD = IFOSB_L2_AHEAD;
+
 // Tensor-map coordinates of a cell: z index k+7, row i+1, plane j+2.
 __device__ __forceinline__ int zc(int k) { return k + 7; }
 __device__ __forceinline__ int xc(int i) { return i + 1; }
@@ -158,12 +176,34 @@ __device__ __forceinline__ bool consumer_wait(uint64_t *bar, int it, int j, int 
     return ok;
 }
 
-// Consumer hands back the ring plane j-2 and the stage of iteration `it`.
-__device__ __forceinline__ void consumer_release(uint64_t *bar, int it) {
+// PML memory values of one cell (x, y, z slabs: three each), read one plane ahead
+// so that the global-memory latency overlaps the previous plane's work.
+struct PsiPre {
+    float x[3], y[3], z[3];
+};
+__device__ __forceinline__ void psi_load(PsiPre &q, const float *ps, const Slabs &sl, const Geo &g, int j, int i, int k,
+                                         int hx, int hz) {
+    if (hx) {
+        const float *p = ps + sxi(g, j, hx, k);
+        q.x[0] = p[0]; q.x[1] = p[sl.sx]; q.x[2] = p[2 * sl.sx];
+    }
+    const int hy = face_y(g, j);
+    if (hy) {
+        const float *p = ps + 3 * sl.sx + syi(g, hy, i, k);
+        q.y[0] = p[0]; q.y[1] = p[sl.sy]; q.y[2] = p[2 * sl.sy];
+    }
+    if (hz) {
+        const float *p = ps + 3 * sl.sx + 3 * sl.sy + szi(g, j, i, hz);
+        q.z[0] = p[0]; q.z[1] = p[sl.sz]; q.z[2] = p[2 * sl.sz];
+    }
+}
+
+// Consumer hands back the ring plane j-2 and/or the stage of iteration `it`.
+__device__ __forceinline__ void consumer_release(uint64_t *bar, int it, bool ring_slot, bool stage) {
     __syncwarp();
     if (threadIdx.x == 0) {
-        mbar_arrive(&bar[RING + it % RING]);
-        mbar_arrive(&bar[2 * RING + 2 + (it & 1)]);
+        if (ring_slot) mbar_arrive(&bar[RING + it % RING]);
+        if (stage) mbar_arrive(&bar[2 * RING + 2 + (it & 1)]);
     }
 }
 
@@ -202,16 +242,29 @@ __global__ void __launch_bounds__(NTHR, 3) k_velocity_tma(const __grid_constant_
             tma_load5(d + 3 * RPLANE, &T.m_pt, zc(k0), xc(i0), yc_(j), VX, s, fb);
             tma_load4(d + 3 * RPLANE + 3 * PT, &T.m_mod, zc(k0), xc(i0), yc_(j), MD_RIP, fb);
         };
+        auto stage_prefetch = [&](int it) {
+            const int j = j0 + it;
+            tma_prefetch5(&T.m_halo, zc(k0) - HZ, xc(i0) - HX, yc_(j), SXX, s);
+            tma_prefetch5(&T.m_pt, zc(k0), xc(i0), yc_(j), VX, s);
+            tma_prefetch4(&T.m_mod, zc(k0), xc(i0), yc_(j), MD_RIP);
+        };
+        auto ring_prefetch = [&](int P) { tma_prefetch5(&T.m_halo, zc(k0) - HZ, xc(i0) - HX, yc_(P), SYY, s); };
         for (int P = rfirst; P <= min(rfirst + RING - 1, rlast); ++P) ring_load(P);
         for (int it = 0; it < 2 && it < n; ++it) stage_load(it);
+        for (int q = 0; q < L2AHEAD; ++q) {
+            if (2 + q < n) stage_prefetch(2 + q);
+            if (rfirst + RING + q <= rlast) ring_prefetch(rfirst + RING + q);
+        }
         for (int it = 0; it < n; ++it) {
             if (rfirst + it + RING <= rlast) {
                 if (!mbar_wait(&bar[RING + it % RING], (it / RING) & 1)) { atomicExch(T.tma_err, 1); return; }
                 ring_load(rfirst + it + RING);
+                if (rfirst + it + RING + L2AHEAD <= rlast) ring_prefetch(rfirst + it + RING + L2AHEAD);
             }
             if (it + 2 < n) {
                 if (!mbar_wait(&bar[2 * RING + 2 + (it & 1)], (it >> 1) & 1)) { atomicExch(T.tma_err, 1); return; }
                 stage_load(it + 2);
+                if (it + 2 + L2AHEAD < n) stage_prefetch(it + 2 + L2AHEAD);
             }
         }
         return;
@@ -230,73 +283,87 @@ __global__ void __launch_bounds__(NTHR, 3) k_velocity_tma(const __grid_constant_
     const int cz = tz + HZ, cx = tx + HX;
     const bool probe_here = a.probe_i == i && a.probe_k == k;
     int sl = 2;  // ring slot of plane j (plane j0 has ring index 2)
+    PsiPre q{};
+    if (active && (hx || hz || face_y(g, j0))) psi_load(q, ps, a.sl, g, j0, i, k, hx, hz);
     for (int it = 0, j = j0; j <= j1; ++it, ++j) {
         if (!consumer_wait(bar, it, j, j0, rfirst)) { if (tz == 0) atomicExch(T.tma_err, 1); return; }
+        // everything this row needs from the stage, so the stage can go back at once
+        float sxx_x = 0.f, sxz_z = 0.f, szz_z = 0.f, sxz_x = 0.f;
+        float vxo = 0.f, vyo = 0.f, vzo = 0.f, rip = 1.f, rjp = 1.f, rkp = 1.f;
         if (active) {
             const float *stage = stg + (it & 1) * SP;
+            const float *Ip = stage + cx * RZ + cz;
+            // stage in-plane fields: 0 sxx, 1 szz, 2 sxz
+#define IP(f, x, z) Ip[(f) * RPLANE + (x) * RZ + (z)]
+            sxx_x = dx * (b1 * (IP(0, 1, 0) - IP(0, 0, 0)) + b2 * (IP(0, 2, 0) - IP(0, -1, 0)));
+            sxz_z = dz * (b1 * (IP(2, 0, 0) - IP(2, 0, -1)) + b2 * (IP(2, 0, 1) - IP(2, 0, -2)));
+            szz_z = dz * (b1 * (IP(1, 0, 1) - IP(1, 0, 0)) + b2 * (IP(1, 0, 2) - IP(1, 0, -1)));
+            sxz_x = dx * (b1 * (IP(2, 0, 0) - IP(2, -1, 0)) + b2 * (IP(2, 1, 0) - IP(2, -2, 0)));
+#undef IP
+            const float *pv = stage + 3 * RPLANE + tx * TZ + tz;
+            vxo = pv[0]; vyo = pv[PT]; vzo = pv[2 * PT];
+            rip = pv[3 * PT]; rjp = pv[4 * PT]; rkp = pv[5 * PT];
+        }
+        consumer_release(bar, it, false, true);
+        if (active) {
             const int sm2 = sl >= 2 ? sl - 2 : sl + RING - 2, sm1 = sl >= 1 ? sl - 1 : sl + RING - 1;
             const int sp1 = sl + 1 < RING ? sl + 1 : sl + 1 - RING, sp2 = sl + 2 < RING ? sl + 2 : sl + 2 - RING;
             const float *R0 = ring + sl * 3 * RPLANE + cx * RZ + cz;
             const float *Rm2 = ring + sm2 * 3 * RPLANE + cx * RZ + cz, *Rm1 = ring + sm1 * 3 * RPLANE + cx * RZ + cz;
             const float *Rp1 = ring + sp1 * 3 * RPLANE + cx * RZ + cz, *Rp2 = ring + sp2 * 3 * RPLANE + cx * RZ + cz;
-            const float *Ip = stage + cx * RZ + cz;
-            // ring fields: 0 syy, 1 sxy, 2 syz; stage in-plane fields: 0 sxx, 1 szz, 2 sxz
+            // ring fields: 0 syy, 1 sxy, 2 syz
 #define RF(Rp, f, x, z) Rp[(f) * RPLANE + (x) * RZ + (z)]
-#define IP(f, x, z) Ip[(f) * RPLANE + (x) * RZ + (z)]
-            float sxx_x = dx * (b1 * (IP(0, 1, 0) - IP(0, 0, 0)) + b2 * (IP(0, 2, 0) - IP(0, -1, 0)));
             float sxy_y = dy * (b1 * (RF(R0, 1, 0, 0) - RF(Rm1, 1, 0, 0)) + b2 * (RF(Rp1, 1, 0, 0) - RF(Rm2, 1, 0, 0)));
-            float sxz_z = dz * (b1 * (IP(2, 0, 0) - IP(2, 0, -1)) + b2 * (IP(2, 0, 1) - IP(2, 0, -2)));
             float syy_y = dy * (b1 * (RF(Rp1, 0, 0, 0) - RF(R0, 0, 0, 0)) + b2 * (RF(Rp2, 0, 0, 0) - RF(Rm1, 0, 0, 0)));
             float sxy_x = dx * (b1 * (RF(R0, 1, 0, 0) - RF(R0, 1, -1, 0)) + b2 * (RF(R0, 1, 1, 0) - RF(R0, 1, -2, 0)));
             float syz_z = dz * (b1 * (RF(R0, 2, 0, 0) - RF(R0, 2, 0, -1)) + b2 * (RF(R0, 2, 0, 1) - RF(R0, 2, 0, -2)));
-            float szz_z = dz * (b1 * (IP(1, 0, 1) - IP(1, 0, 0)) + b2 * (IP(1, 0, 2) - IP(1, 0, -1)));
-            float sxz_x = dx * (b1 * (IP(2, 0, 0) - IP(2, -1, 0)) + b2 * (IP(2, 1, 0) - IP(2, -2, 0)));
             float syz_y = dy * (b1 * (RF(R0, 2, 0, 0) - RF(Rm1, 2, 0, 0)) + b2 * (RF(Rp1, 2, 0, 0) - RF(Rm2, 2, 0, 0)));
 #undef RF
-#undef IP
             const int hy = face_y(g, j);
             const bool frame = hx || hy || hz;
             if (hx) {
                 float *p = ps + sxi(g, j, hx, k);
                 const long long o = a.sl.sx;
-                float v0 = CP(BH_X, hx) * p[0] + CP(AH_X, hx) * sxx_x; p[0] = v0; sxx_x = sxx_x / CP(KH_X, hx) + v0;
-                float v1 = CP(B_X, hx) * p[o] + CP(A_X, hx) * sxy_x; p[o] = v1; sxy_x = sxy_x / CP(K_X, hx) + v1;
-                float v2 = CP(B_X, hx) * p[2 * o] + CP(A_X, hx) * sxz_x; p[2 * o] = v2; sxz_x = sxz_x / CP(K_X, hx) + v2;
+                float v0 = CP(BH_X, hx) * q.x[0] + CP(AH_X, hx) * sxx_x; p[0] = v0; sxx_x = sxx_x / CP(KH_X, hx) + v0;
+                float v1 = CP(B_X, hx) * q.x[1] + CP(A_X, hx) * sxy_x; p[o] = v1; sxy_x = sxy_x / CP(K_X, hx) + v1;
+                float v2 = CP(B_X, hx) * q.x[2] + CP(A_X, hx) * sxz_x; p[2 * o] = v2; sxz_x = sxz_x / CP(K_X, hx) + v2;
             }
             if (hy) {
                 float *p = ps + 3 * a.sl.sx + syi(g, hy, i, k);
                 const long long o = a.sl.sy;
-                float v0 = CP(B_Y, hy) * p[0] + CP(A_Y, hy) * sxy_y; p[0] = v0; sxy_y = sxy_y / CP(K_Y, hy) + v0;
-                float v1 = CP(BH_Y, hy) * p[o] + CP(AH_Y, hy) * syy_y; p[o] = v1; syy_y = syy_y / CP(KH_Y, hy) + v1;
-                float v2 = CP(B_Y, hy) * p[2 * o] + CP(A_Y, hy) * syz_y; p[2 * o] = v2; syz_y = syz_y / CP(K_Y, hy) + v2;
+                float v0 = CP(B_Y, hy) * q.y[0] + CP(A_Y, hy) * sxy_y; p[0] = v0; sxy_y = sxy_y / CP(K_Y, hy) + v0;
+                float v1 = CP(BH_Y, hy) * q.y[1] + CP(AH_Y, hy) * syy_y; p[o] = v1; syy_y = syy_y / CP(KH_Y, hy) + v1;
+                float v2 = CP(B_Y, hy) * q.y[2] + CP(A_Y, hy) * syz_y; p[2 * o] = v2; syz_y = syz_y / CP(K_Y, hy) + v2;
             }
             if (hz) {
                 float *p = ps + 3 * a.sl.sx + 3 * a.sl.sy + szi(g, j, i, hz);
                 const long long o = a.sl.sz;
-                float v0 = CP(B_Z, hz) * p[0] + CP(A_Z, hz) * sxz_z; p[0] = v0; sxz_z = sxz_z / CP(K_Z, hz) + v0;
-                float v1 = CP(B_Z, hz) * p[o] + CP(A_Z, hz) * syz_z; p[o] = v1; syz_z = syz_z / CP(K_Z, hz) + v1;
-                float v2 = CP(BH_Z, hz) * p[2 * o] + CP(AH_Z, hz) * szz_z; p[2 * o] = v2; szz_z = szz_z / CP(KH_Z, hz) + v2;
+                const float *cg = a.cpg;
+                float v0 = CPG(cg, B_Z, hz) * q.z[0] + CPG(cg, A_Z, hz) * sxz_z; p[0] = v0; sxz_z = sxz_z / CPG(cg, K_Z, hz) + v0;
+                float v1 = CPG(cg, B_Z, hz) * q.z[1] + CPG(cg, A_Z, hz) * syz_z; p[o] = v1; syz_z = syz_z / CPG(cg, K_Z, hz) + v1;
+                float v2 = CPG(cg, BH_Z, hz) * q.z[2] + CPG(cg, AH_Z, hz) * szz_z; p[2 * o] = v2; szz_z = szz_z / CPG(cg, KH_Z, hz) + v2;
             }
-            const float *pv = stage + 3 * RPLANE + tx * TZ + tz;
+            // the next plane's PML memory, a plane ahead of its use
+            if (j < j1 && (hx || hz || face_y(g, j + 1))) psi_load(q, ps, a.sl, g, j + 1, i, k, hx, hz);
             const long long c = widx(g, j, i, k);
             float *V = st + c;
             if (p1 > p0) {
                 // cells of this block hold point forces: the order of update_v / update_v_CPML
-                V[VX * F] = pv[0]; V[VY * F] = pv[PT]; V[VZ * F] = pv[2 * PT];
+                V[VX * F] = vxo; V[VY * F] = vyo; V[VZ * F] = vzo;
                 if (frame) vel_points<BACK>(a, st, p0, p1, j, i, k, nt, c);
-                V[VX * F] = V[VX * F] + (sxx_x + sxy_y + sxz_z) / pv[3 * PT];
-                V[VY * F] = V[VY * F] + (syy_y + sxy_x + syz_z) / pv[4 * PT];
-                V[VZ * F] = V[VZ * F] + (szz_z + sxz_x + syz_y) / pv[5 * PT];
+                V[VX * F] = V[VX * F] + (sxx_x + sxy_y + sxz_z) / rip;
+                V[VY * F] = V[VY * F] + (syy_y + sxy_x + syz_z) / rjp;
+                V[VZ * F] = V[VZ * F] + (szz_z + sxz_x + syz_y) / rkp;
                 const int passes = frame ? (BACK ? 1 : 0) : (BACK ? 2 : 1);
                 for (int pass = 0; pass < passes; ++pass) vel_points<BACK>(a, st, p0, p1, j, i, k, nt, c);
             } else {
-                V[VX * F] = pv[0] + (sxx_x + sxy_y + sxz_z) / pv[3 * PT];
-                V[VY * F] = pv[PT] + (syy_y + sxy_x + syz_z) / pv[4 * PT];
-                V[VZ * F] = pv[2 * PT] + (szz_z + sxz_x + syz_y) / pv[5 * PT];
+                V[VX * F] = vxo + (sxx_x + sxy_y + sxz_z) / rip;
+                V[VY * F] = vyo + (syy_y + sxy_x + syz_z) / rjp;
+                V[VZ * F] = vzo + (szz_z + sxz_x + syz_y) / rkp;
             }
             if (probe_here && j == a.probe_j && isnan(V[VY * F])) atomicMin(a.err_step + s, nt);
         }
-        consumer_release(bar, it);
+        consumer_release(bar, it, true, false);
         sl = sl + 1 < RING ? sl + 1 : 0;
     }
 }
@@ -311,7 +378,7 @@ __device__ __forceinline__ float ddiv(float a, float d, float inv) {
 }
 
 template <int L, bool P2>
-__global__ void __launch_bounds__(NTHR, 2) k_stress_tma(const __grid_constant__ StrTma T, int nt, int do_dft, int sample) {
+__global__ void __maxnreg__(112) k_stress_tma(const __grid_constant__ StrTma T, int nt, int do_dft, int sample) {
     extern __shared__ __align__(128) unsigned char smem[];
     const StrArgs &a = T.a;
     const Geo &g = a.g;
@@ -345,16 +412,29 @@ __global__ void __launch_bounds__(NTHR, 2) k_stress_tma(const __grid_constant__ 
             tma_load4(d + nsr * PT, &T.m_mod, zc(k0), xc(i0), yc_(j), 0, fb);
             if (ndf) tma_load5(d + (nsr + nm) * PT, &T.m_dft, zc(k0), xc(i0), yc_(j), 0, s, fb);
         };
+        auto stage_prefetch = [&](int it) {
+            const int j = j0 + it;
+            tma_prefetch5(&T.m_sr, zc(k0), xc(i0), yc_(j), SYY, s);
+            tma_prefetch4(&T.m_mod, zc(k0), xc(i0), yc_(j), 0);
+            if (ndf) tma_prefetch5(&T.m_dft, zc(k0), xc(i0), yc_(j), 0, s);
+        };
+        auto ring_prefetch = [&](int P) { tma_prefetch5(&T.m_halo, zc(k0) - HZ, xc(i0) - HX, yc_(P), VX, s); };
         for (int P = rfirst; P <= min(rfirst + RING - 1, rlast); ++P) ring_load(P);
         for (int it = 0; it < 2 && it < n; ++it) stage_load(it);
+        for (int q = 0; q < L2AHEAD; ++q) {
+            if (2 + q < n) stage_prefetch(2 + q);
+            if (rfirst + RING + q <= rlast) ring_prefetch(rfirst + RING + q);
+        }
         for (int it = 0; it < n; ++it) {
             if (rfirst + it + RING <= rlast) {
                 if (!mbar_wait(&bar[RING + it % RING], (it / RING) & 1)) { atomicExch(T.tma_err, 1); return; }
                 ring_load(rfirst + it + RING);
+                if (rfirst + it + RING + L2AHEAD <= rlast) ring_prefetch(rfirst + it + RING + L2AHEAD);
             }
             if (it + 2 < n) {
                 if (!mbar_wait(&bar[2 * RING + 2 + (it & 1)], (it >> 1) & 1)) { atomicExch(T.tma_err, 1); return; }
                 stage_load(it + 2);
+                if (it + 2 + L2AHEAD < n) stage_prefetch(it + 2 + L2AHEAD);
             }
         }
         return;
@@ -374,6 +454,8 @@ __global__ void __launch_bounds__(NTHR, 2) k_stress_tma(const __grid_constant__ 
     const bool zfront = k <= g.fw;
     const int cz = tz + HZ, cx = tx + HX;
     int sl = 2;
+    PsiPre q{};
+    if (active && (hx || hz || face_y(g, j0))) psi_load(q, ps, a.sl, g, j0, i, k, hx, hz);
     for (int it = 0, j = j0; j <= j1; ++it, ++j) {
         if (!consumer_wait(bar, it, j, j0, rfirst)) { if (tz == 0) atomicExch(T.tma_err, 1); return; }
         if (active) {
@@ -400,27 +482,30 @@ __global__ void __launch_bounds__(NTHR, 2) k_stress_tma(const __grid_constant__ 
             if (hx) {
                 float *p = ps + sxi(g, j, hx, k);
                 const long long o = a.sl.sx;
-                float v0 = CP(B_X, hx) * p[0] + CP(A_X, hx) * vxx; p[0] = v0; vxx = vxx / CP(K_X, hx) + v0;
-                float v1 = CP(BH_X, hx) * p[o] + CP(AH_X, hx) * vyx; p[o] = v1; vyx = vyx / CP(KH_X, hx) + v1;
-                float v2 = CP(BH_X, hx) * p[2 * o] + CP(AH_X, hx) * vzx; p[2 * o] = v2; vzx = vzx / CP(KH_X, hx) + v2;
+                float v0 = CP(B_X, hx) * q.x[0] + CP(A_X, hx) * vxx; p[0] = v0; vxx = vxx / CP(K_X, hx) + v0;
+                float v1 = CP(BH_X, hx) * q.x[1] + CP(AH_X, hx) * vyx; p[o] = v1; vyx = vyx / CP(KH_X, hx) + v1;
+                float v2 = CP(BH_X, hx) * q.x[2] + CP(AH_X, hx) * vzx; p[2 * o] = v2; vzx = vzx / CP(KH_X, hx) + v2;
             }
             if (hy) {
                 float *p = ps + 3 * a.sl.sx + syi(g, hy, i, k);
                 const long long o = a.sl.sy;
-                float v0 = CP(BH_Y, hy) * p[0] + CP(AH_Y, hy) * vxy; p[0] = v0; vxy = vxy / CP(KH_Y, hy) + v0;
-                float v1 = CP(B_Y, hy) * p[o] + CP(A_Y, hy) * vyy; p[o] = v1; vyy = vyy / CP(K_Y, hy) + v1;
-                float v2 = CP(BH_Y, hy) * p[2 * o] + CP(AH_Y, hy) * vzy; p[2 * o] = v2; vzy = vzy / CP(KH_Y, hy) + v2;
+                float v0 = CP(BH_Y, hy) * q.y[0] + CP(AH_Y, hy) * vxy; p[0] = v0; vxy = vxy / CP(KH_Y, hy) + v0;
+                float v1 = CP(B_Y, hy) * q.y[1] + CP(A_Y, hy) * vyy; p[o] = v1; vyy = vyy / CP(K_Y, hy) + v1;
+                float v2 = CP(BH_Y, hy) * q.y[2] + CP(AH_Y, hy) * vzy; p[2 * o] = v2; vzy = vzy / CP(KH_Y, hy) + v2;
             }
             if (hz) {
                 // the reference divides by K_y on the front z face (update_s_ssg_CPML_elastic.c:104-108)
                 float *p = ps + 3 * a.sl.sx + 3 * a.sl.sy + szi(g, j, i, hz);
                 const long long o = a.sl.sz;
-                const float kh = zfront ? CP(KH_Y, hz) : CP(KH_Z, hz);
-                const float kf = zfront ? CP(K_Y, hz) : CP(K_Z, hz);
-                float v0 = CP(BH_Z, hz) * p[0] + CP(AH_Z, hz) * vxz; p[0] = v0; vxz = vxz / kh + v0;
-                float v1 = CP(BH_Z, hz) * p[o] + CP(AH_Z, hz) * vyz; p[o] = v1; vyz = vyz / kh + v1;
-                float v2 = CP(B_Z, hz) * p[2 * o] + CP(A_Z, hz) * vzz; p[2 * o] = v2; vzz = vzz / kf + v2;
+                const float *cg = a.cpg;
+                const float kh = zfront ? CPG(cg, KH_Y, hz) : CPG(cg, KH_Z, hz);
+                const float kf = zfront ? CPG(cg, K_Y, hz) : CPG(cg, K_Z, hz);
+                float v0 = CPG(cg, BH_Z, hz) * q.z[0] + CPG(cg, AH_Z, hz) * vxz; p[0] = v0; vxz = vxz / kh + v0;
+                float v1 = CPG(cg, BH_Z, hz) * q.z[1] + CPG(cg, AH_Z, hz) * vyz; p[o] = v1; vyz = vyz / kh + v1;
+                float v2 = CPG(cg, B_Z, hz) * q.z[2] + CPG(cg, A_Z, hz) * vzz; p[2 * o] = v2; vzz = vzz / kf + v2;
             }
+            // the next plane's PML memory, a plane ahead of its use
+            if (j < j1 && (hx || hz || face_y(g, j + 1))) psi_load(q, ps, a.sl, g, j + 1, i, k, hx, hz);
             const float *S = stage + tx * TZ + tz;      // sigma + memory variables (old values)
             const float *Mo = S + nsr * PT;             // model
             const float pim = Mo[MD_PI * PT], um = Mo[MD_U * PT];
@@ -594,7 +679,7 @@ __global__ void __launch_bounds__(NTHR, 2) k_stress_tma(const __grid_constant__ 
                 }
             }
         }
-        consumer_release(bar, it);
+        consumer_release(bar, it, true, true);
         sl = sl + 1 < RING ? sl + 1 : 0;
     }
 }
