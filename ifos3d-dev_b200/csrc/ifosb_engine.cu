@@ -17,6 +17,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1018,4 +1019,49 @@ extern "C" int ifosb_get_field(ifosb_engine *e, int shot, int field, float *out)
     CU(cudaMemcpy2D(out, sizeof(float) * (p.nz + 4), src + 6, sizeof(float) * g.pz, sizeof(float) * (p.nz + 4),
                     (size_t)(p.ny + 5) * (p.nx + 4), cudaMemcpyDeviceToHost));
     return IFOSB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// ifosb_residual_noalloc: the residual and FP64 misfit of ifosb_residual on the
+// caller's device buffers and stream, with the per-trace partial sums in a
+// fixed file-scope device array instead of engine memory. It runs the same two
+// kernels (k_residual, k_misfit) as ifosb_residual, so the results are the same
+// bits. Every scratch word that k_misfit reads is written by k_residual earlier
+// in the same call, so nothing has to be cleared between calls.
+static __device__ __align__(256) double g_noalloc_part[IFOSB_NOALLOC_MAX_TRACES];
+
+namespace {
+constexpr int NOALLOC_MAX_DEVICES = 64;
+std::mutex g_noalloc_mu;
+double *g_noalloc_addr[NOALLOC_MAX_DEVICES];  // address of g_noalloc_part on each device
+}  // namespace
+
+extern "C" int ifosb_residual_noalloc(int nshots, int ntr, int ns, float dt, const float *d_syn, const float *d_obs,
+                                      float *d_diff, double *d_misfit, void *stream) {
+    if (nshots < 1 || ntr < 1 || ns < 1 || !d_syn || !d_obs || !d_diff || !d_misfit) return IFOSB_EARG;
+    if ((long long)nshots * 3 * ntr > IFOSB_NOALLOC_MAX_TRACES) return IFOSB_ETOOBIG;
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return IFOSB_ENODEV;
+    }
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return IFOSB_EARG;
+    double *part;
+    {
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        if (!g_noalloc_addr[dev]) {
+            void *addr = nullptr;
+            if (cudaGetSymbolAddress(&addr, g_noalloc_part) != cudaSuccess || !addr) {
+                cudaGetLastError();
+                return IFOSB_ECUDA;
+            }
+            g_noalloc_addr[dev] = static_cast<double *>(addr);
+        }
+        part = g_noalloc_addr[dev];
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int nthr = nshots * 3 * ntr;
+    k_residual<<<(nthr + 127) / 128, 128, 0, s>>>(d_syn, d_obs, d_diff, part, nshots, ntr, ns, dt);
+    k_misfit<<<nshots, 32, 0, s>>>(part, d_misfit, 3 * ntr);
+    return cudaGetLastError() == cudaSuccess ? IFOSB_OK : IFOSB_ECUDA;
 }

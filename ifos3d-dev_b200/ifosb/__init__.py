@@ -18,8 +18,10 @@ import numpy as np
 PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LIB_PATH = os.path.join(PKG_DIR, "lib", "libifos_b200.so")
 
-OK, EARG, ECUDA, ENOMEM, EUNSTABLE, ESTATE, ENODEV = 0, 1, 2, 3, 4, 5, 6
-_NAMES = {EARG: "EARG", ECUDA: "ECUDA", ENOMEM: "ENOMEM", EUNSTABLE: "EUNSTABLE", ESTATE: "ESTATE", ENODEV: "ENODEV"}
+OK, EARG, ECUDA, ENOMEM, EUNSTABLE, ESTATE, ENODEV, ETOOBIG = 0, 1, 2, 3, 4, 5, 6, 7
+_NAMES = {EARG: "EARG", ECUDA: "ECUDA", ENOMEM: "ENOMEM", EUNSTABLE: "EUNSTABLE", ESTATE: "ESTATE", ENODEV: "ENODEV",
+          ETOOBIG: "ETOOBIG"}
+NOALLOC_MAX_TRACES = 65536
 
 F_VX, F_VY, F_VZ, F_SXX, F_SYY, F_SZZ, F_SXY, F_SYZ, F_SXZ = range(9)
 F_DFT_FWD, F_DFT_BACK = 100, 200
@@ -90,6 +92,7 @@ def lib():
             "ifosb_set_profiling": (C.c_int, [vp, C.c_int]),
             "ifosb_kernel_times": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int)]),
             "ifosb_set_stream": (C.c_int, [vp, vp]),
+            "ifosb_residual_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_float, vp, vp, vp, vp, vp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -107,7 +110,7 @@ def exported_symbols():
         "ifosb_adjoint", "ifosb_gradient", "ifosb_zero_gradient", "ifosb_get_gradient", "ifosb_shot_gradient",
         "ifosb_get_field", "ifosb_set_launch_mode", "ifosb_last_launch_count", "ifosb_cpml_coeff",
         "ifosb_wavelet", "ifosb_nsamples", "ifosb_moduli", "ifosb_set_profiling", "ifosb_kernel_times",
-        "ifosb_set_stream",
+        "ifosb_set_stream", "ifosb_residual_noalloc",
     ]
 
 
@@ -130,6 +133,14 @@ def make_params(nx, ny, nz, dh=1.0, dt=1e-4, nt=100, fdcoeff=2, free_surf=1, fw=
 
 def nsamples(p: Params) -> int:
     return lib().ifosb_nsamples(C.byref(p))
+
+
+def residual_noalloc(nshots: int, ntr: int, ns: int, dt: float, d_syn: int, d_obs: int, d_diff: int,
+                     d_misfit: int, stream: int = 0) -> int:
+    """ifosb_residual_noalloc on device addresses (ints); enqueued on `stream`
+    (a cudaStream_t as int), not waited for. Returns the status code."""
+    return lib().ifosb_residual_noalloc(nshots, ntr, ns, dt, C.c_void_p(d_syn), C.c_void_p(d_obs),
+                                        C.c_void_p(d_diff), C.c_void_p(d_misfit), C.c_void_p(stream or None))
 
 
 def cpml_coeff(p: Params, vppml: float, fpml: float) -> np.ndarray:

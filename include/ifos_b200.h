@@ -181,6 +181,37 @@ int ifosb_moduli(const ifosb_params *p, long long n, const float *vp, const floa
 /* Number of samples per trace ns (src/ifos3d.c:178-179). */
 int ifosb_nsamples(const ifosb_params *p);
 
+/* ---- residual without allocation ---------------------------------------- */
+
+/* No counterpart in the reference (its residual() works on host arrays).
+ *
+ * ifosb_residual_noalloc computes what ifosb_residual computes — the
+ * time-integrated, time-reversed residual of residual() (src/residual.c:35-60)
+ * and the per-shot FP64 misfit, the same bits — for traces that already sit in
+ * the caller's device memory, without an engine and without allocating: no
+ * cudaMalloc/cudaFree and no allocating library call. It is for callers that
+ * cannot allocate at that point: a shot planner that has filled HBM with
+ * wavefield batches and has no room left; a pipeline that evaluates misfits on
+ * one stream while propagation runs on another, where cudaMalloc/cudaFree would
+ * synchronise the device; a host whose device memory all comes from its own pool.
+ *
+ * d_syn, d_obs, d_diff: device [nshots][3][ntr][ns] float (synthetic, observed,
+ * residual out); d_misfit: device [nshots] double. The work is enqueued on
+ * `stream` (a cudaStream_t as void*, NULL = the legacy default stream) and the
+ * call returns without waiting for it — unlike the other entry points.
+ *
+ * The per-trace partial sums live in a fixed device array of
+ * IFOSB_NOALLOC_MAX_TRACES doubles (512 KiB) per device; nothing in it has to be
+ * zero at the start of a call. Limit: nshots*3*ntr <= IFOSB_NOALLOC_MAX_TRACES,
+ * else IFOSB_ETOOBIG and nothing is launched. The first call on each device
+ * looks up that array's address (cudaGetSymbolAddress); make it before any
+ * stream capture. Calls on one stream run in order; calls that overlap in time
+ * on the same device (two streams, two host threads) share the array and race. */
+#define IFOSB_ETOOBIG 7
+#define IFOSB_NOALLOC_MAX_TRACES 65536
+int ifosb_residual_noalloc(int nshots, int ntr, int ns, float dt, const float *d_syn, const float *d_obs,
+                           float *d_diff, double *d_misfit, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
