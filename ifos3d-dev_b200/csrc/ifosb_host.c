@@ -6,6 +6,7 @@
  *   ifosb_cpml_coeff : CPML_coeff.c:87-324
  *   ifosb_wavelet    : wavelet.c:29-99 (shapes 1, 2, 4, 5)
  *   ifosb_moduli     : readmod.c:48-65, 106-129 (the arithmetic, not the file IO)
+ *   ifosb_steplength : steplength.c:26-91, in double
  */
 #include "../../include/ifos_b200.h"
 
@@ -126,5 +127,37 @@ int ifosb_moduli(const ifosb_params *p, long long n, const float *vp, const floa
         pi[o] = piv;
         if (L) { taus[o] = ts; taup[o] = tp; }
     }
+    return IFOSB_OK;
+}
+
+/* steplength (steplength.c:26-91) with every quantity in double: the parabola
+ * through (step[i], L2[i]), i = 0..2, its minimum step[3] limited as the
+ * reference limits it, the parabola's value L2[3] there, and the next test
+ * step step[4]. */
+int ifosb_steplength(double *L2, double *step, int lbfgs, int it_group, double teststep, double *abc) {
+    if (!L2 || !step) return IFOSB_EARG;
+    const double s0 = step[0], s1 = step[1], s2 = step[2];
+    const double a = ((s0 - s1) * (L2[0] - L2[2]) - (s0 - s2) * (L2[0] - L2[1])) /
+                     (s0 * s2 * (s0 - s2) + s0 * s1 * (s1 - s0) + s1 * s2 * (s2 - s1));
+    double b = (L2[0] - L2[1]) / (s0 - s1);
+    b = b - a * (s0 + s1);
+    const double c = L2[0] - a * s0 * s0 - b * s0;
+    step[3] = 0.0;
+    if (a > 0) step[3] = -b / (2 * a);
+    if (a < 0) {
+        if (L2[0] < L2[1] && L2[0] < L2[2]) step[3] = 0.1 * s1;
+        if (L2[1] < L2[0] && L2[1] < L2[2]) step[3] = s1;
+        if (L2[2] < L2[0] && L2[2] < L2[1]) step[3] = s2;
+    }
+    if (step[3] > 2.5 * step[4]) step[3] = 2.5 * step[4];
+    if (lbfgs && it_group > 1 && step[3] > 1.0) step[3] = 1.0;
+    if (step[3] <= 0) step[3] = 0.1 * s1;
+    if (step[3] < 0.1 * s1) step[3] = 0.1 * s1;
+    L2[3] = a * step[3] * step[3] + b * step[3] + c;
+    step[4] = step[3] / 2;
+    if (step[4] < 0.2 * teststep) step[4] = 0.2 * teststep;
+    if (step[4] > teststep) step[4] = teststep;
+    if (lbfgs && it_group > 1) step[4] = 0.5;
+    if (abc) { abc[0] = a; abc[1] = b; abc[2] = c; }
     return IFOSB_OK;
 }

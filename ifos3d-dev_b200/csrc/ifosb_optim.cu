@@ -1,0 +1,433 @@
+// ifosb_optim.cu — the inversion-loop updates of the reference driver on the
+// device, with every reduction in FP64:
+//   conjugate()      src/conjugategrad.c:27-110  (Mora 1987 CG direction)
+//   lbfgs_savegrad() src/lbfgs_save.c:25-56
+//   lbfgs()          src/lbfgs.c:26-181          (two-loop recursion)
+//   modelupdate()    src/modelupdate.c:26-160
+// The reference accumulates its dot products in float (and sums them across
+// ranks with MPI_FLOAT); here every dot product and the L-BFGS work vector are
+// FP64 and the reductions run in a fixed order (fixed grid, per-block tree,
+// one final block), so results are deterministic. The elementwise model update
+// keeps the reference's float/double expressions and is bit-identical to it.
+#include "../../include/ifos_b200.h"
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <string>
+
+namespace {
+
+constexpr int RBLK = 296;  // reduction blocks: 2 per SM on a 148-SM B200
+constexpr int RTHR = 256;
+constexpr int MAXSUM = 6;
+
+#define OCU(call)                                                                \
+    do {                                                                         \
+        cudaError_t _e = (call);                                                 \
+        if (_e != cudaSuccess) {                                                 \
+            o->err = std::string(#call) + ": " + cudaGetErrorString(_e);         \
+            return _e == cudaErrorMemoryAllocation ? IFOSB_ENOMEM : IFOSB_ECUDA; \
+        }                                                                        \
+    } while (0)
+
+// Block-wide sum of K values per thread into part[blockIdx.x*K + q] (fixed order).
+template <int K>
+__device__ void block_sums(double (&v)[K], double *part) {
+    __shared__ double sh[K][RTHR / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+        double x = v[q];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0) sh[q][wid] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < K) {
+        double s = 0.0;
+        for (int w = 0; w < RTHR / 32; ++w) s += sh[threadIdx.x][w];
+        part[blockIdx.x * K + threadIdx.x] = s;
+    }
+}
+
+// Final fixed-order sum of the RBLK partials of K sums: out[q].
+__global__ void k_final(const double *part, int K, double *out) {
+    const int q = threadIdx.x;
+    if (q >= K) return;
+    double s = 0.0;
+    for (int b = 0; b < RBLK; ++b) s += part[b * K + q];
+    out[q] = s;
+}
+
+// conjugategrad.c:59-74: the six sums of Mora's beta, and prior1..3 = grad.
+__global__ void k_cg_sums(const float *g, float *prior, long long n, double *part) {
+    double v[6] = {0, 0, 0, 0, 0, 0};
+    for (long long i = blockIdx.x * (long long)RTHR + threadIdx.x; i < n; i += (long long)RBLK * RTHR) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const double gc = g[c * n + i], pc = prior[c * n + i];
+            v[2 * c] += gc * (gc - pc);
+            v[2 * c + 1] += pc * pc;
+            prior[c * n + i] = (float)gc;
+        }
+    }
+    block_sums<6>(v, part);
+}
+
+// conjugategrad.c:79-91: beta = num/den where den != 0; the clamps test beta[0]
+// only, so beta[0] ends in [0, 0.5] and beta[1], beta[2] are not clamped.
+__global__ void k_cg_beta(const double *sums, int cdf, double *beta) {
+    if (threadIdx.x != 0) return;
+    double b[3] = {0.0, 0.0, 0.0};
+    if (cdf == 0)
+        for (int c = 0; c < 3; ++c)
+            if (fabs(sums[2 * c + 1]) > 0.0) b[c] = sums[2 * c] / sums[2 * c + 1];
+    if (b[0] < 0) b[0] = 0.0;
+    if (b[0] > 0.5) b[0] = 0.5;
+    beta[0] = b[0];
+    beta[1] = b[1];
+    beta[2] = b[2];
+}
+
+// conjugategrad.c:94-107: grad = prior4*beta + grad; prior4 = grad.
+__global__ void k_cg_dir(float *g, float *prior46, const double *beta, long long n) {
+    for (long long i = blockIdx.x * (long long)RTHR + threadIdx.x; i < n; i += (long long)RBLK * RTHR) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const float d = (float)((double)prior46[c * n + i] * beta[c] + (double)g[c * n + i]);
+            g[c * n + i] = d;
+            prior46[c * n + i] = d;
+        }
+    }
+}
+
+// lbfgs.c:49-72: y_w = (previous gradient) - gradient; q = gradient.
+__global__ void k_lb_start(const float *g, double *y, double *q, long long nn) {
+    for (long long i = blockIdx.x * (long long)RTHR + threadIdx.x; i < nn; i += (long long)RBLK * RTHR) {
+        const double gv = g[i];
+        y[i] = y[i] - gv;
+        q[i] = gv;
+    }
+}
+
+__global__ void k_dot(const double *x, const double *y, long long nn, double *part) {
+    double v[1] = {0.0};
+    for (long long i = blockIdx.x * (long long)RTHR + threadIdx.x; i < nn; i += (long long)RBLK * RTHR)
+        v[0] += x[i] * y[i];
+    block_sums<1>(v, part);
+}
+
+__global__ void k_dot2(const double *x, const double *y, long long nn, double *part) {
+    double v[2] = {0.0, 0.0};
+    for (long long i = blockIdx.x * (long long)RTHR + threadIdx.x; i < nn; i += (long long)RBLK * RTHR) {
+        v[0] += x[i] * y[i];
+        v[1] += x[i] * x[i];
+    }
+    block_sums<2>(v, part);
+}
+
+// Scalars of the recursion, kept on the device so no host round trip sits
+// between the passes: sc[0..B-1] rho_w (bfgsscale), sc[B..2B-1] alpha_w,
+// sc[2B] h0, sc[2B+1] the coefficient of the current axpy, sc[2B+2..] raw sums.
+enum { OP_SCALE, OP_ALPHA, OP_BETA };
+__global__ void k_lb_scalar(const double *part, int K, double *sc, int B, int w, int op) {
+    if (threadIdx.x != 0) return;
+    double s[2] = {0.0, 0.0};
+    for (int q = 0; q < K; ++q)
+        for (int b = 0; b < RBLK; ++b) s[q] += part[b * K + q];
+    if (op == OP_SCALE) {  // lbfgs.c:84-87: rho_w = 1/(y.s), h0 = (y.s)/(y.y)
+        sc[w] = 1.0 / s[0];
+        sc[2 * B] = s[0] / s[1];
+        sc[2 * B + 2] = s[0];
+        sc[2 * B + 3] = s[1];
+    } else if (op == OP_ALPHA) {  // lbfgs.c:100-110: alpha_w = rho_w s_w.q; q -= alpha_w y_w
+        sc[B + w] = sc[w] * s[0];
+        sc[2 * B + 1] = -sc[B + w];
+    } else {  // lbfgs.c:146-158: beta = rho_w y_w.q; q += s_w (alpha_w - beta)
+        sc[2 * B + 1] = sc[B + w] - sc[w] * s[0];
+    }
+}
+
+__global__ void k_axpy(double *q, const double *x, const double *coef, long long nn) {
+    const double a = *coef;
+    for (long long i = blockIdx.x * (long long)RTHR + threadIdx.x; i < nn; i += (long long)RBLK * RTHR)
+        q[i] += a * x[i];
+}
+
+__global__ void k_scale(double *q, const double *h0, long long nn) {
+    const double a = *h0;
+    for (long long i = blockIdx.x * (long long)RTHR + threadIdx.x; i < nn; i += (long long)RBLK * RTHR)
+        q[i] = q[i] * a;
+}
+
+// lbfgs.c:161-181: y_w' = gradient (kept for the next call); gradient = q.
+__global__ void k_lb_end(float *g, double *y, const double *q, long long nn) {
+    for (long long i = blockIdx.x * (long long)RTHR + threadIdx.x; i < nn; i += (long long)RBLK * RTHR) {
+        y[i] = g[i];
+        g[i] = (float)q[i];
+    }
+}
+
+__global__ void k_copy_f2d(double *d, const float *s, long long nn) {
+    for (long long i = blockIdx.x * (long long)RTHR + threadIdx.x; i < nn; i += (long long)RBLK * RTHR) d[i] = s[i];
+}
+
+// modelupdate.c:82-102: max |grad_c| (non-negative floats order like their bits).
+__global__ void k_absmax(const float *g, long long n, unsigned int *mx) {
+    unsigned int m[3] = {0u, 0u, 0u};
+    for (long long i = blockIdx.x * (long long)RTHR + threadIdx.x; i < n; i += (long long)RBLK * RTHR)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) m[c] = max(m[c], __float_as_uint(fabsf(g[c * n + i])));
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m[c] = max(m[c], __shfl_down_sync(0xffffffffu, m[c], o));
+        if ((threadIdx.x & 31) == 0) atomicMax(mx + c, m[c]);
+    }
+}
+
+// modelupdate.c:105-117: grad_c /= max_c when max0 > 0 and max1 > 0 (max2 = 0 -> 1).
+__global__ void k_normalise(float *g, long long n, const unsigned int *mx) {
+    const float m0 = __uint_as_float(mx[0]), m1 = __uint_as_float(mx[1]);
+    float m2 = __uint_as_float(mx[2]);
+    if (m2 == 0.0f) m2 = 1.0f;
+    if (!(m0 > 0.0f && m1 > 0.0f)) return;
+    for (long long i = blockIdx.x * (long long)RTHR + threadIdx.x; i < n; i += (long long)RBLK * RTHR) {
+        g[i] = g[i] / m0;
+        g[n + i] = g[n + i] / m1;
+        g[2 * n + i] = g[2 * n + i] / m2;
+    }
+}
+
+struct UpdArgs {
+    int nx, ny, nz;
+    float step, scale1, scale2, scale3, vp0, vs0, rho0;
+    int numpar;
+    double *s;  // L-BFGS model difference of this iteration, or nullptr
+};
+
+// modelupdate.c:119-157 with the reference's promotions: sqrt() of the float
+// ratio in double, the float product step*scale*grad*V0 added in double and the
+// sum stored as float; moduli from the new values in float.
+__global__ void k_modelupdate(const float *g, float *rho, float *pi, float *u, UpdArgs a) {
+    const long long n = (long long)a.nx * a.ny * a.nz;
+    for (long long l = blockIdx.x * (long long)RTHR + threadIdx.x; l < n; l += (long long)RBLK * RTHR) {
+        const int k = (int)(l % a.nz), i = (int)((l / a.nz) % a.nx), j = (int)(l / ((long long)a.nz * a.nx));
+        const long long m = ((long long)(j + 1) * (a.nx + 2) + (i + 1)) * (a.nz + 2) + (k + 1);
+        const float r = rho[m], p = pi[m], mu = u[m];
+        const double vp_old = sqrt((double)(p / r)), vs_old = sqrt((double)(mu / r));
+        const float vpnew = (float)(vp_old + (double)(a.step * a.scale1 * g[l] * a.vp0));
+        const float vsnew = (float)(vs_old + (double)(a.step * a.scale2 * g[n + l] * a.vs0));
+        const float rhonew = r + a.scale3 * a.step * g[2 * n + l] * a.rho0;
+        if (a.s) {
+            a.s[l] = ((double)vpnew - vp_old) / (double)a.vp0;
+            if (a.numpar > 1) a.s[n + l] = ((double)vsnew - vs_old) / (double)a.vs0;
+        }
+        u[m] = rhonew * vsnew * vsnew;
+        pi[m] = rhonew * vpnew * vpnew;
+        rho[m] = rhonew;
+    }
+}
+
+}  // namespace
+
+struct ifosb_optim {
+    int nx = 0, ny = 0, nz = 0, numpar = 1, bfgsnum = 0;
+    long long n = 0;
+    float *d_grad = nullptr;    // [3][n]
+    float *d_prior = nullptr;   // [6][n] gradprior1..6
+    double *d_s = nullptr;      // [bfgsnum][numpar*n] bfgsmod
+    double *d_y = nullptr;      // [bfgsnum][numpar*n] bfgsgrad
+    double *d_q = nullptr;      // [numpar*n]
+    double *d_part = nullptr;   // [RBLK*MAXSUM]
+    double *d_sc = nullptr;     // scalars of the recursion
+    double *d_out = nullptr;    // [MAXSUM]
+    unsigned int *d_max = nullptr;
+    float *d_model = nullptr;   // [3][(ny+2)(nx+2)(nz+2)] rho, pi, u
+    cudaStream_t stream = nullptr;
+    std::string err;
+};
+
+static int ofail(ifosb_optim *o, int code, const char *msg) {
+    if (o) o->err = msg;
+    return code;
+}
+
+extern "C" int ifosb_optim_create(int nx, int ny, int nz, int numpar, int bfgsnum, ifosb_optim **out) {
+    if (!out || nx < 1 || ny < 1 || nz < 1 || numpar < 1 || numpar > 2 || bfgsnum < 0) return IFOSB_EARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return IFOSB_ENODEV;
+    }
+    ifosb_optim *o = new ifosb_optim;
+    o->nx = nx;
+    o->ny = ny;
+    o->nz = nz;
+    o->numpar = numpar;
+    o->bfgsnum = bfgsnum;
+    o->n = (long long)nx * ny * nz;
+    const long long n = o->n, nn = (long long)numpar * n, mg = (long long)(nx + 2) * (ny + 2) * (nz + 2);
+    auto alloc = [&](void **p, size_t bytes) { return cudaMalloc(p, bytes) == cudaSuccess; };
+    bool ok = alloc((void **)&o->d_grad, sizeof(float) * 3 * n) && alloc((void **)&o->d_prior, sizeof(float) * 6 * n) &&
+              alloc((void **)&o->d_part, sizeof(double) * RBLK * MAXSUM) &&
+              alloc((void **)&o->d_sc, sizeof(double) * (2 * bfgsnum + 8)) &&
+              alloc((void **)&o->d_out, sizeof(double) * MAXSUM) && alloc((void **)&o->d_max, sizeof(unsigned) * 3) &&
+              alloc((void **)&o->d_model, sizeof(float) * 3 * mg);
+    if (ok && bfgsnum > 0)
+        ok = alloc((void **)&o->d_s, sizeof(double) * bfgsnum * nn) && alloc((void **)&o->d_y, sizeof(double) * bfgsnum * nn) &&
+             alloc((void **)&o->d_q, sizeof(double) * nn);
+    if (ok) ok = cudaStreamCreateWithFlags(&o->stream, cudaStreamNonBlocking) == cudaSuccess;
+    if (ok) ok = cudaMemsetAsync(o->d_prior, 0, sizeof(float) * 6 * n, o->stream) == cudaSuccess &&
+                 cudaMemsetAsync(o->d_sc, 0, sizeof(double) * (2 * bfgsnum + 8), o->stream) == cudaSuccess;
+    if (ok && bfgsnum > 0)
+        ok = cudaMemsetAsync(o->d_s, 0, sizeof(double) * bfgsnum * nn, o->stream) == cudaSuccess &&
+             cudaMemsetAsync(o->d_y, 0, sizeof(double) * bfgsnum * nn, o->stream) == cudaSuccess;
+    if (ok) ok = cudaStreamSynchronize(o->stream) == cudaSuccess;
+    if (!ok) {
+        cudaGetLastError();
+        ifosb_optim_destroy(o);
+        return IFOSB_ENOMEM;
+    }
+    *out = o;
+    return IFOSB_OK;
+}
+
+extern "C" void ifosb_optim_destroy(ifosb_optim *o) {
+    if (!o) return;
+    for (void *p : {(void *)o->d_grad, (void *)o->d_prior, (void *)o->d_s, (void *)o->d_y, (void *)o->d_q,
+                    (void *)o->d_part, (void *)o->d_sc, (void *)o->d_out, (void *)o->d_max, (void *)o->d_model})
+        if (p) cudaFree(p);
+    if (o->stream) cudaStreamDestroy(o->stream);
+    delete o;
+}
+
+extern "C" const char *ifosb_optim_last_error(const ifosb_optim *o) { return o ? o->err.c_str() : "no optimiser"; }
+
+static int finish(ifosb_optim *o) {
+    OCU(cudaGetLastError());
+    OCU(cudaStreamSynchronize(o->stream));
+    return IFOSB_OK;
+}
+
+extern "C" int ifosb_conjugate(ifosb_optim *o, float *grad, int cdf, double *beta) {
+    if (!o || !grad) return IFOSB_EARG;
+    const long long n = o->n;
+    double *d_beta = o->d_sc + 2 * o->bfgsnum + 4;
+    OCU(cudaMemcpyAsync(o->d_grad, grad, sizeof(float) * 3 * n, cudaMemcpyDefault, o->stream));
+    if (cdf == 1) {  // conjugategrad.c:43-56: both priors start from this gradient
+        OCU(cudaMemcpyAsync(o->d_prior, o->d_grad, sizeof(float) * 3 * n, cudaMemcpyDeviceToDevice, o->stream));
+        OCU(cudaMemcpyAsync(o->d_prior + 3 * n, o->d_grad, sizeof(float) * 3 * n, cudaMemcpyDeviceToDevice, o->stream));
+    } else {
+        k_cg_sums<<<RBLK, RTHR, 0, o->stream>>>(o->d_grad, o->d_prior, n, o->d_part);
+        k_final<<<1, 32, 0, o->stream>>>(o->d_part, 6, o->d_out);
+        k_cg_beta<<<1, 32, 0, o->stream>>>(o->d_out, cdf, d_beta);
+        k_cg_dir<<<RBLK, RTHR, 0, o->stream>>>(o->d_grad, o->d_prior + 3 * n, d_beta, n);
+        OCU(cudaMemcpyAsync(grad, o->d_grad, sizeof(float) * 3 * n, cudaMemcpyDefault, o->stream));
+    }
+    int rc = finish(o);
+    if (rc) return rc;
+    if (beta) {
+        if (cdf == 1) {
+            beta[0] = beta[1] = beta[2] = 0.0;
+        } else {
+            OCU(cudaMemcpy(beta, d_beta, sizeof(double) * 3, cudaMemcpyDeviceToHost));
+        }
+    }
+    return IFOSB_OK;
+}
+
+static int slot(int v, int B) {
+    const int w = v % B;
+    return w == 0 ? B : w;  // 1-based as the reference's bfgs matrices
+}
+
+extern "C" int ifosb_lbfgs_savegrad(ifosb_optim *o, const float *grad) {
+    if (!o || !grad) return IFOSB_EARG;
+    if (o->bfgsnum < 1) return ofail(o, IFOSB_ESTATE, "optimiser created without L-BFGS history");
+    const long long nn = (long long)o->numpar * o->n;
+    OCU(cudaMemcpyAsync(o->d_grad, grad, sizeof(float) * nn, cudaMemcpyDefault, o->stream));
+    k_copy_f2d<<<RBLK, RTHR, 0, o->stream>>>(o->d_y, o->d_grad, nn);  // lbfgs_save.c:31-52: slot 1
+    return finish(o);
+}
+
+extern "C" int ifosb_lbfgs(ifosb_optim *o, float *grad, int it_group) {
+    if (!o || !grad || it_group < 2) return IFOSB_EARG;
+    const int B = o->bfgsnum;
+    if (B < 1) return ofail(o, IFOSB_ESTATE, "optimiser created without L-BFGS history");
+    const long long nn = (long long)o->numpar * o->n;
+    double *sc = o->d_sc;
+    int m = it_group - B;
+    if (m < 1) m = 1;
+    auto S = [&](int w) { return o->d_s + (long long)(w - 1) * nn; };
+    auto Y = [&](int w) { return o->d_y + (long long)(w - 1) * nn; };
+    OCU(cudaMemcpyAsync(o->d_grad, grad, sizeof(float) * nn, cudaMemcpyDefault, o->stream));
+    int w = slot(it_group - 1, B);
+    k_lb_start<<<RBLK, RTHR, 0, o->stream>>>(o->d_grad, Y(w), o->d_q, nn);
+    k_dot2<<<RBLK, RTHR, 0, o->stream>>>(Y(w), S(w), nn, o->d_part);
+    k_lb_scalar<<<1, 32, 0, o->stream>>>(o->d_part, 2, sc, B, w - 1, OP_SCALE);
+    for (int v = it_group - 1; v >= m; --v) {
+        w = slot(v, B);
+        k_dot<<<RBLK, RTHR, 0, o->stream>>>(S(w), o->d_q, nn, o->d_part);
+        k_lb_scalar<<<1, 32, 0, o->stream>>>(o->d_part, 1, sc, B, w - 1, OP_ALPHA);
+        k_axpy<<<RBLK, RTHR, 0, o->stream>>>(o->d_q, Y(w), sc + 2 * B + 1, nn);
+    }
+    k_scale<<<RBLK, RTHR, 0, o->stream>>>(o->d_q, sc + 2 * B, nn);
+    for (int v = m; v <= it_group - 1; ++v) {
+        w = slot(v, B);
+        k_dot<<<RBLK, RTHR, 0, o->stream>>>(Y(w), o->d_q, nn, o->d_part);
+        k_lb_scalar<<<1, 32, 0, o->stream>>>(o->d_part, 1, sc, B, w - 1, OP_BETA);
+        k_axpy<<<RBLK, RTHR, 0, o->stream>>>(o->d_q, S(w), sc + 2 * B + 1, nn);
+    }
+    k_lb_end<<<RBLK, RTHR, 0, o->stream>>>(o->d_grad, Y(slot(it_group, B)), o->d_q, nn);
+    OCU(cudaMemcpyAsync(grad, o->d_grad, sizeof(float) * nn, cudaMemcpyDefault, o->stream));
+    return finish(o);
+}
+
+extern "C" int ifosb_modelupdate(ifosb_optim *o, float *grad, float *rho, float *pi, float *u, float step,
+                                 const float *weight, float vp0, float vs0, float rho0, int lbfgs, int it_group) {
+    if (!o || !grad || !rho || !pi || !u || !weight) return IFOSB_EARG;
+    if (lbfgs && o->bfgsnum < 1) return ofail(o, IFOSB_ESTATE, "optimiser created without L-BFGS history");
+    const long long n = o->n, mg = (long long)(o->nx + 2) * (o->ny + 2) * (o->nz + 2);
+    float *drho = o->d_model, *dpi = o->d_model + mg, *du = o->d_model + 2 * mg;
+    OCU(cudaMemcpyAsync(o->d_grad, grad, sizeof(float) * 3 * n, cudaMemcpyDefault, o->stream));
+    OCU(cudaMemcpyAsync(drho, rho, sizeof(float) * mg, cudaMemcpyDefault, o->stream));
+    OCU(cudaMemcpyAsync(dpi, pi, sizeof(float) * mg, cudaMemcpyDefault, o->stream));
+    OCU(cudaMemcpyAsync(du, u, sizeof(float) * mg, cudaMemcpyDefault, o->stream));
+    if (!lbfgs) {
+        OCU(cudaMemsetAsync(o->d_max, 0, sizeof(unsigned) * 3, o->stream));
+        k_absmax<<<RBLK, RTHR, 0, o->stream>>>(o->d_grad, n, o->d_max);
+        k_normalise<<<RBLK, RTHR, 0, o->stream>>>(o->d_grad, n, o->d_max);
+    }
+    UpdArgs a;
+    a.nx = o->nx;
+    a.ny = o->ny;
+    a.nz = o->nz;
+    a.step = step;
+    a.scale1 = weight[0];
+    a.scale2 = weight[1];
+    a.scale3 = weight[2];
+    a.vp0 = vp0;
+    a.vs0 = vs0;
+    a.rho0 = rho0;
+    a.numpar = o->numpar;
+    a.s = lbfgs ? o->d_s + (long long)(slot(it_group, o->bfgsnum) - 1) * o->numpar * n : nullptr;
+    k_modelupdate<<<RBLK, RTHR, 0, o->stream>>>(o->d_grad, drho, dpi, du, a);
+    if (!lbfgs) OCU(cudaMemcpyAsync(grad, o->d_grad, sizeof(float) * 3 * n, cudaMemcpyDefault, o->stream));
+    OCU(cudaMemcpyAsync(rho, drho, sizeof(float) * mg, cudaMemcpyDefault, o->stream));
+    OCU(cudaMemcpyAsync(pi, dpi, sizeof(float) * mg, cudaMemcpyDefault, o->stream));
+    OCU(cudaMemcpyAsync(u, du, sizeof(float) * mg, cudaMemcpyDefault, o->stream));
+    return finish(o);
+}
+
+extern "C" int ifosb_lbfgs_history(const ifosb_optim *o, double *s, double *y, double *scale) {
+    if (!o || o->bfgsnum < 1) return IFOSB_EARG;
+    const size_t nn = (size_t)o->numpar * o->n * o->bfgsnum;
+    if (s && cudaMemcpy(s, o->d_s, sizeof(double) * nn, cudaMemcpyDeviceToHost) != cudaSuccess) return IFOSB_ECUDA;
+    if (y && cudaMemcpy(y, o->d_y, sizeof(double) * nn, cudaMemcpyDeviceToHost) != cudaSuccess) return IFOSB_ECUDA;
+    if (scale && cudaMemcpy(scale, o->d_sc, sizeof(double) * o->bfgsnum, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return IFOSB_ECUDA;
+    return IFOSB_OK;
+}

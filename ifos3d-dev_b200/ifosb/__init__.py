@@ -93,6 +93,16 @@ def lib():
             "ifosb_kernel_times": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int)]),
             "ifosb_set_stream": (C.c_int, [vp, vp]),
             "ifosb_residual_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_float, vp, vp, vp, vp, vp]),
+            "ifosb_optim_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(vp)]),
+            "ifosb_optim_destroy": (None, [vp]),
+            "ifosb_optim_last_error": (C.c_char_p, [vp]),
+            "ifosb_conjugate": (C.c_int, [vp, vp, C.c_int, vp]),
+            "ifosb_lbfgs_savegrad": (C.c_int, [vp, vp]),
+            "ifosb_lbfgs": (C.c_int, [vp, vp, C.c_int]),
+            "ifosb_modelupdate": (C.c_int, [vp, vp, vp, vp, vp, C.c_float, vp, C.c_float, C.c_float, C.c_float,
+                                            C.c_int, C.c_int]),
+            "ifosb_lbfgs_history": (C.c_int, [vp, vp, vp, vp]),
+            "ifosb_steplength": (C.c_int, [vp, vp, C.c_int, C.c_int, C.c_double, vp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -110,7 +120,9 @@ def exported_symbols():
         "ifosb_adjoint", "ifosb_gradient", "ifosb_zero_gradient", "ifosb_get_gradient", "ifosb_shot_gradient",
         "ifosb_get_field", "ifosb_set_launch_mode", "ifosb_last_launch_count", "ifosb_cpml_coeff",
         "ifosb_wavelet", "ifosb_nsamples", "ifosb_moduli", "ifosb_set_profiling", "ifosb_kernel_times",
-        "ifosb_set_stream", "ifosb_residual_noalloc",
+        "ifosb_set_stream", "ifosb_residual_noalloc", "ifosb_optim_create", "ifosb_optim_destroy",
+        "ifosb_optim_last_error", "ifosb_conjugate", "ifosb_lbfgs_savegrad", "ifosb_lbfgs", "ifosb_modelupdate",
+        "ifosb_lbfgs_history", "ifosb_steplength",
     ]
 
 
@@ -322,3 +334,81 @@ class Engine:
         base = F_DFT_BACK if back else F_DFT_FWD
         return np.stack([np.stack([self.get_field(shot, base + c * self.nf + l) for l in range(self.nf)])
                          for c in range(6)])
+
+
+class Optimizer:
+    """The reference's model-space update state on the device (CG priors,
+    L-BFGS history) with FP64 dot products: conjugate(), lbfgs_savegrad(),
+    lbfgs(), modelupdate() of src/conjugategrad.c, src/lbfgs_save.c,
+    src/lbfgs.c, src/modelupdate.c. Gradients are [3][NY][NX][NZ] float32
+    (updated in place); models the ghosted [NY+2][NX+2][NZ+2] float32 arrays."""
+
+    def __init__(self, nx: int, ny: int, nz: int, numpar: int = 1, bfgsnum: int = 0):
+        self.shape = (ny, nx, nz)
+        self.numpar, self.bfgsnum = numpar, bfgsnum
+        h = C.c_void_p()
+        rc = lib().ifosb_optim_create(nx, ny, nz, numpar, bfgsnum, C.byref(h))
+        if rc != OK:
+            raise IfosbError(rc, "ifosb_optim_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().ifosb_optim_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _c(self, rc):
+        if rc != OK:
+            raise IfosbError(rc, lib().ifosb_optim_last_error(self.h).decode())
+
+    def _grad(self, grad):
+        if not (isinstance(grad, np.ndarray) and grad.dtype == np.float32 and grad.flags.c_contiguous
+                and grad.shape == (3,) + self.shape):
+            raise ValueError(f"gradient must be a C-contiguous float32 array of shape {(3,) + self.shape}")
+        return grad
+
+    def conjugate(self, grad, cdf: int) -> np.ndarray:
+        beta = np.zeros(3, np.float64)
+        self._c(lib().ifosb_conjugate(self.h, _p(self._grad(grad)), cdf, _p(beta)))
+        return beta
+
+    def lbfgs_savegrad(self, grad):
+        self._c(lib().ifosb_lbfgs_savegrad(self.h, _p(self._grad(grad))))
+
+    def lbfgs(self, grad, it_group: int):
+        self._c(lib().ifosb_lbfgs(self.h, _p(self._grad(grad)), it_group))
+
+    def modelupdate(self, grad, rho, pi, u, step, weight, vp0, vs0, rho0, lbfgs=False, it_group=1):
+        mshape = tuple(s + 2 for s in self.shape)
+        for a in (rho, pi, u):
+            if not (isinstance(a, np.ndarray) and a.dtype == np.float32 and a.flags.c_contiguous and a.shape == mshape):
+                raise ValueError(f"model arrays must be C-contiguous float32 of shape {mshape}")
+        w = np.ascontiguousarray(weight, np.float32)
+        self._c(lib().ifosb_modelupdate(self.h, _p(self._grad(grad)), _p(rho), _p(pi), _p(u), step, _p(w), vp0, vs0,
+                                        rho0, int(bool(lbfgs)), it_group))
+
+    def history(self):
+        nn = self.numpar * int(np.prod(self.shape))
+        s = np.zeros((self.bfgsnum, nn), np.float64)
+        y = np.zeros((self.bfgsnum, nn), np.float64)
+        sc = np.zeros(self.bfgsnum, np.float64)
+        self._c(lib().ifosb_lbfgs_history(self.h, _p(s), _p(y), _p(sc)))
+        return s, y, sc
+
+
+def steplength(L2, step, lbfgs=False, it_group=1, teststep=0.0):
+    """steplength() in FP64. L2[4], step[5] float64 arrays updated in place;
+    returns the parabola coefficients (a, b, c)."""
+    if not (isinstance(L2, np.ndarray) and L2.dtype == np.float64 and L2.size >= 4):
+        raise ValueError("L2 must be a float64 array of 4")
+    if not (isinstance(step, np.ndarray) and step.dtype == np.float64 and step.size >= 5):
+        raise ValueError("step must be a float64 array of 5")
+    abc = np.zeros(3, np.float64)
+    _check(None, lib().ifosb_steplength(_p(L2), _p(step), int(bool(lbfgs)), it_group, teststep, _p(abc)))
+    return abc

@@ -181,6 +181,53 @@ int ifosb_moduli(const ifosb_params *p, long long n, const float *vp, const floa
 /* Number of samples per trace ns (src/ifos3d.c:178-179). */
 int ifosb_nsamples(const ifosb_params *p);
 
+/* ---- inversion-loop updates (src/ifos3d.c:1005-1138) -------------------- */
+
+/* The model-space state of the reference's optimiser on the device: the CG
+ * priors gradprior1..6 and the L-BFGS history bfgsmod/bfgsgrad/bfgsscale.
+ * Dot products and the L-BFGS work vector are FP64 (the reference: float and
+ * MPI_FLOAT), reduced in a fixed order. Gradient and model pointers may be
+ * host or device memory. n = NX*NY*NZ; gradients are grad[3][NY][NX][NZ]
+ * (vp, vs, rho: grad1..3 interior); models are the ghosted
+ * [NY+2][NX+2][NZ+2] arrays of ifosb_set_model (interior updated). */
+typedef struct ifosb_optim ifosb_optim;
+
+/* numpar = NUMPAR (1: vp, 2: vp and vs in L-BFGS), bfgsnum = BFGSNUM (0: CG only). */
+int ifosb_optim_create(int nx, int ny, int nz, int numpar, int bfgsnum, ifosb_optim **out);
+void ifosb_optim_destroy(ifosb_optim *o);
+const char *ifosb_optim_last_error(const ifosb_optim *o);
+
+/* conjugate (src/conjugategrad.c:27-110): cdf=1 starts a new sequence (grad
+ * unchanged); otherwise Mora's beta with FP64 sums, the reference's clamp of
+ * beta[0] to [0, 0.5] (beta[1], beta[2] are not clamped there), and
+ * grad = prior*beta + grad in place. beta (optional) gets the three betas. */
+int ifosb_conjugate(ifosb_optim *o, float *grad, int cdf, double *beta);
+
+/* lbfgs_savegrad (src/lbfgs_save.c:25-56): the first iteration's gradient. */
+int ifosb_lbfgs_savegrad(ifosb_optim *o, const float *grad);
+
+/* lbfgs (src/lbfgs.c:26-181) for it_group >= 2: the two-loop recursion over
+ * the last BFGSNUM pairs in FP64; grad (vp[, vs]) is replaced by the direction. */
+int ifosb_lbfgs(ifosb_optim *o, float *grad, int it_group);
+
+/* modelupdate (src/modelupdate.c:26-160): without L-BFGS the gradients are first
+ * normalised by their maxima (in place, as the reference does); then
+ * vp, vs, rho += step*WEIGHT*grad*(VP0, VS0, RHO0) with the reference's float
+ * arithmetic (bit-identical) and rho, pi, u rewritten. With L-BFGS the model
+ * difference of slot it_group%BFGSNUM is recorded in FP64. weight[3] = WEIGHT. */
+int ifosb_modelupdate(ifosb_optim *o, float *grad, float *rho, float *pi, float *u, float step,
+                      const float *weight, float vp0, float vs0, float rho0, int lbfgs, int it_group);
+
+/* The L-BFGS history for inspection: s, y [BFGSNUM][NUMPAR*n], scale [BFGSNUM]. */
+int ifosb_lbfgs_history(const ifosb_optim *o, double *s, double *y, double *scale);
+
+/* steplength (src/steplength.c:26-91) in FP64: L2[0..2] misfits at step[0..2]
+ * (step[0] = 0), step[4] the test step; writes step[3] (the parabola's minimum
+ * with the reference's limits), L2[3] and the next test step step[4].
+ * abc (optional) gets the parabola coefficients a, b, c. Scalar work: it runs
+ * on the host in FP64. */
+int ifosb_steplength(double *L2, double *step, int lbfgs, int it_group, double teststep, double *abc);
+
 /* ---- residual without allocation ---------------------------------------- */
 
 /* No counterpart in the reference (its residual() works on host arrays).
