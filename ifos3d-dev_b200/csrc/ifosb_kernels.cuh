@@ -20,7 +20,10 @@ constexpr int MAXFW = 64;
 constexpr int MAXMECH = 4;
 constexpr int MAXNF = 16;
 constexpr int BX = 32;  // threads along z (contiguous)
-constexpr int BY = 8;   // threads along x
+#ifndef IFOSB_BY
+#define IFOSB_BY 8
+#endif
+constexpr int BY = IFOSB_BY;  // threads along x
 
 // state field slots of a shot. The stresses with a y derivative in the velocity
 // update (syy, sxy, syz) come first, then the in-plane ones (sxx, szz, sxz), then

@@ -32,14 +32,26 @@
 namespace ifosb {
 
 constexpr int TZ = 32;    // tile extent along z (== BX)
-constexpr int TX = 8;     // tile extent along x (== BY), one consumer warp per row
-constexpr int RING = 6;   // stencil planes held: j-2..j+2 and the one being loaded
+constexpr int TX = BY;    // tile extent along x, one consumer warp per row
+#ifndef IFOSB_RING
+#define IFOSB_RING 6
+#endif
+constexpr int RING = IFOSB_RING;  // stencil planes held: j-2..j+2 and RING-5 being loaded
+static_assert(RING >= 6, "the stencil needs planes j-2..j+2 plus one in flight");
 constexpr int HZ = 4;     // z halo (keeps TMA z-coordinates 16-byte aligned)
 constexpr int HX = 2;     // x halo
 constexpr int RZ = TZ + 2 * HZ;              // ring row length
 constexpr int RX = TX + 2 * HX;              // ring rows
 constexpr int RPLANE = RX * RZ;              // floats per field per ring plane
 constexpr int PT = TX * TZ;                  // floats per point-wise field tile
+// TMA writes shared memory only at 128-byte aligned destinations: every box
+// starts on a multiple of 32 floats (padding is empty for TX = 8).
+__host__ __device__ constexpr int a32(int x) { return (x + 31) & ~31; }
+constexpr int RSLOT = a32(3 * RPLANE);       // ring slot stride (3 stencil fields)
+constexpr int VS_PT = a32(3 * RPLANE);       // velocity stage: offset of the v box
+constexpr int VS_MOD = VS_PT + a32(3 * PT);  // velocity stage: offset of the rip/rjp/rkp box
+constexpr int VS_SP = VS_MOD + a32(3 * PT);  // velocity stage stride
+static_assert(RSLOT % 32 == 0 && VS_PT % 32 == 0 && VS_MOD % 32 == 0 && VS_SP % 32 == 0, "TMA alignment");
 constexpr int NTHR = 32 * (TX + 1);          // TX consumer warps + 1 producer warp
 constexpr int NBAR = 2 * RING + 4;           // full/empty per ring slot, full/empty per stage
 
@@ -54,13 +66,26 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *b, uint32_t bytes) {
 __device__ __forceinline__ void mbar_arrive(uint64_t *b) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(su32(b)) : "memory");
 }
+// IFOSB_WAIT_HINT_NS > 0 lets a waiting thread be suspended in hardware for up
+// to that many nanoseconds per try (instead of returning at once and spinning).
+#ifndef IFOSB_WAIT_HINT_NS
+#define IFOSB_WAIT_HINT_NS 0
+#endif
 __device__ __forceinline__ bool mbar_try(uint64_t *b, uint32_t parity) {
     uint32_t ok;
+#if IFOSB_WAIT_HINT_NS > 0
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(su32(b)), "r"(parity), "r"((uint32_t)IFOSB_WAIT_HINT_NS)
+        : "memory");
+#else
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
         : "=r"(ok)
         : "r"(su32(b)), "r"(parity)
         : "memory");
+#endif
     return ok != 0;
 }
 __device__ __forceinline__ uint64_t gtimer() {
@@ -136,10 +161,15 @@ struct StrTma {
 };
 
 __host__ __device__ constexpr size_t vel_tma_smem() {
-    return sizeof(float) * ((size_t)RING * 3 * RPLANE + 2 * ((size_t)3 * RPLANE + 6 * PT)) + 8 * NBAR;
+    return sizeof(float) * ((size_t)RING * RSLOT + 2 * (size_t)VS_SP) + 8 * NBAR;
 }
+// Stress stage: [sigma + memory variables: nsr][model: nm][DFT: ndf] boxes of PT
+// floats per field, each box start rounded up to 32 floats.
+__host__ __device__ inline int str_mod_off(int nsr) { return a32(nsr * PT); }
+__host__ __device__ inline int str_dft_off(int nsr, int nm) { return a32(nsr * PT) + a32(nm * PT); }
+__host__ __device__ inline int str_stage(int nsr, int nm, int ndf) { return str_dft_off(nsr, nm) + a32(ndf * PT); }
 __host__ __device__ inline size_t str_tma_smem(int nsr, int nm, int ndf) {
-    return sizeof(float) * ((size_t)RING * 3 * RPLANE + 2 * (size_t)(nsr + nm + ndf) * PT) + 8 * NBAR;
+    return sizeof(float) * ((size_t)RING * RSLOT + 2 * (size_t)str_stage(nsr, nm, ndf)) + 8 * NBAR;
 }
 
 // CTA start: returns false (for every thread) if an earlier CTA reported a timeout.
@@ -207,6 +237,124 @@ __device__ __forceinline__ void consumer_release(uint64_t *bar, int it, bool rin
     }
 }
 
+// Consumer side of the velocity update: warp tx computes row i0+tx of the tile
+// for planes j0..j1. XZ = the tile touches an x or z PML face (or the grid
+// edge); without it hx = hz = 0 and every lane is active. Ring slots, the
+// slot and parity of the next wait and the cell pointer advance by one plane
+// per iteration (no per-plane division or 64-bit index arithmetic).
+template <bool BACK, bool XZ>
+__device__ __forceinline__ void vel_rows(const VelTma &T, int nt, const float *ring, const float *stg, uint64_t *bar,
+                                         int j0, int j1, int s, int ycn, int k0, int i0) {
+    const VelArgs &a = T.a;
+    const Geo &g = a.g;
+    constexpr int SP = VS_SP;
+    const int tz = threadIdx.x, tx = threadIdx.y;
+    const int k = k0 + tz, i = i0 + tx;
+    const bool active = XZ ? (k <= g.nz && i <= g.nx) : true;
+    int p0, p1;
+    block_points(a.pt_off, g, s, ycn, p0, p1);
+    float *st = a.st + (long long)s * a.st_shot;
+    float *ps = a.psi + (long long)s * a.psi_shot;
+    const long long F = g.field;
+    const float b1 = a.b1, b2 = a.b2, dx = a.dxr, dy = a.dyr, dz = a.dzr;
+    const int hx = XZ ? face_x(g, i) : 0, hz = XZ ? face_z(g, k) : 0;
+    const int cz = tz + HZ, cx = tx + HX;
+    const int probe_j = (a.probe_i == i && a.probe_k == k) ? a.probe_j : -1;
+    // ring planes j-2..j+2 sit in slots 0..4 for j = j0; the next plane enters slot 5
+    const float *Rb = ring + cx * RZ + cz;
+    const float *Rm2 = Rb, *Rm1 = Rb + RSLOT, *R0 = Rb + 2 * RSLOT, *Rp1 = Rb + 3 * RSLOT, *Rp2 = Rb + 4 * RSLOT;
+    int nslot = 5;            // slot of the plane that becomes j+2 next
+    int wslot = 5, wpar = 0;  // slot and phase parity of plane j+2 at it >= 1
+    float *V = st + widx(g, j0, i, k);
+    PsiPre q{};
+    if (active && (hx || hz || face_y(g, j0))) psi_load(q, ps, a.sl, g, j0, i, k, hx, hz);
+    for (int it = 0, j = j0; j <= j1; ++it, ++j, V += g.plane) {
+        bool ok = true;
+        if (it == 0) {
+            for (int r = 0; r < 5; ++r) ok &= mbar_wait(&bar[r], 0);
+        } else {
+            ok &= mbar_wait(&bar[wslot], wpar);
+            if (++wslot == RING) { wslot = 0; wpar ^= 1; }
+        }
+        ok &= mbar_wait(&bar[2 * RING + (it & 1)], (it >> 1) & 1);
+        if (!ok) { if (tz == 0) atomicExch(T.tma_err, 1); return; }
+        // everything this row needs from the stage, so the stage can go back at once
+        float sxx_x = 0.f, sxz_z = 0.f, szz_z = 0.f, sxz_x = 0.f;
+        float vxo = 0.f, vyo = 0.f, vzo = 0.f, rip = 1.f, rjp = 1.f, rkp = 1.f;
+        if (active) {
+            const float *stage = stg + (it & 1) * SP;
+            const float *Ip = stage + cx * RZ + cz;
+            // stage in-plane fields: 0 sxx, 1 szz, 2 sxz
+#define IP(f, x, z) Ip[(f) * RPLANE + (x) * RZ + (z)]
+            sxx_x = dx * (b1 * (IP(0, 1, 0) - IP(0, 0, 0)) + b2 * (IP(0, 2, 0) - IP(0, -1, 0)));
+            sxz_z = dz * (b1 * (IP(2, 0, 0) - IP(2, 0, -1)) + b2 * (IP(2, 0, 1) - IP(2, 0, -2)));
+            szz_z = dz * (b1 * (IP(1, 0, 1) - IP(1, 0, 0)) + b2 * (IP(1, 0, 2) - IP(1, 0, -1)));
+            sxz_x = dx * (b1 * (IP(2, 0, 0) - IP(2, -1, 0)) + b2 * (IP(2, 1, 0) - IP(2, -2, 0)));
+#undef IP
+            const float *pv = stage + VS_PT + tx * TZ + tz, *pm = stage + VS_MOD + tx * TZ + tz;
+            vxo = pv[0]; vyo = pv[PT]; vzo = pv[2 * PT];
+            rip = pm[0]; rjp = pm[PT]; rkp = pm[2 * PT];
+        }
+        consumer_release(bar, it, false, true);
+        if (active) {
+            // ring fields: 0 syy, 1 sxy, 2 syz
+#define RF(Rp, f, x, z) Rp[(f) * RPLANE + (x) * RZ + (z)]
+            float sxy_y = dy * (b1 * (RF(R0, 1, 0, 0) - RF(Rm1, 1, 0, 0)) + b2 * (RF(Rp1, 1, 0, 0) - RF(Rm2, 1, 0, 0)));
+            float syy_y = dy * (b1 * (RF(Rp1, 0, 0, 0) - RF(R0, 0, 0, 0)) + b2 * (RF(Rp2, 0, 0, 0) - RF(Rm1, 0, 0, 0)));
+            float sxy_x = dx * (b1 * (RF(R0, 1, 0, 0) - RF(R0, 1, -1, 0)) + b2 * (RF(R0, 1, 1, 0) - RF(R0, 1, -2, 0)));
+            float syz_z = dz * (b1 * (RF(R0, 2, 0, 0) - RF(R0, 2, 0, -1)) + b2 * (RF(R0, 2, 0, 1) - RF(R0, 2, 0, -2)));
+            float syz_y = dy * (b1 * (RF(R0, 2, 0, 0) - RF(Rm1, 2, 0, 0)) + b2 * (RF(Rp1, 2, 0, 0) - RF(Rm2, 2, 0, 0)));
+#undef RF
+            const int hy = face_y(g, j);
+            const bool frame = hx || hy || hz;
+            if (XZ && hx) {
+                float *p = ps + sxi(g, j, hx, k);
+                const long long o = a.sl.sx;
+                float v0 = CP(BH_X, hx) * q.x[0] + CP(AH_X, hx) * sxx_x; p[0] = v0; sxx_x = sxx_x / CP(KH_X, hx) + v0;
+                float v1 = CP(B_X, hx) * q.x[1] + CP(A_X, hx) * sxy_x; p[o] = v1; sxy_x = sxy_x / CP(K_X, hx) + v1;
+                float v2 = CP(B_X, hx) * q.x[2] + CP(A_X, hx) * sxz_x; p[2 * o] = v2; sxz_x = sxz_x / CP(K_X, hx) + v2;
+            }
+            if (hy) {
+                float *p = ps + 3 * a.sl.sx + syi(g, hy, i, k);
+                const long long o = a.sl.sy;
+                float v0 = CP(B_Y, hy) * q.y[0] + CP(A_Y, hy) * sxy_y; p[0] = v0; sxy_y = sxy_y / CP(K_Y, hy) + v0;
+                float v1 = CP(BH_Y, hy) * q.y[1] + CP(AH_Y, hy) * syy_y; p[o] = v1; syy_y = syy_y / CP(KH_Y, hy) + v1;
+                float v2 = CP(B_Y, hy) * q.y[2] + CP(A_Y, hy) * syz_y; p[2 * o] = v2; syz_y = syz_y / CP(K_Y, hy) + v2;
+            }
+            if (XZ && hz) {
+                float *p = ps + 3 * a.sl.sx + 3 * a.sl.sy + szi(g, j, i, hz);
+                const long long o = a.sl.sz;
+                const float *cg = a.cpg;
+                float v0 = CPG(cg, B_Z, hz) * q.z[0] + CPG(cg, A_Z, hz) * sxz_z; p[0] = v0; sxz_z = sxz_z / CPG(cg, K_Z, hz) + v0;
+                float v1 = CPG(cg, B_Z, hz) * q.z[1] + CPG(cg, A_Z, hz) * syz_z; p[o] = v1; syz_z = syz_z / CPG(cg, K_Z, hz) + v1;
+                float v2 = CPG(cg, BH_Z, hz) * q.z[2] + CPG(cg, AH_Z, hz) * szz_z; p[2 * o] = v2; szz_z = szz_z / CPG(cg, KH_Z, hz) + v2;
+            }
+            // the next plane's PML memory, a plane ahead of its use
+            if (j < j1 && (hx || hz || face_y(g, j + 1))) psi_load(q, ps, a.sl, g, j + 1, i, k, hx, hz);
+            if (p1 > p0) {
+                // cells of this block hold point forces: the order of update_v / update_v_CPML
+                const long long c = V - st;
+                V[VX * F] = vxo; V[VY * F] = vyo; V[VZ * F] = vzo;
+                if (frame) vel_points<BACK>(a, st, p0, p1, j, i, k, nt, c);
+                V[VX * F] = V[VX * F] + (sxx_x + sxy_y + sxz_z) / rip;
+                V[VY * F] = V[VY * F] + (syy_y + sxy_x + syz_z) / rjp;
+                V[VZ * F] = V[VZ * F] + (szz_z + sxz_x + syz_y) / rkp;
+                const int passes = frame ? (BACK ? 1 : 0) : (BACK ? 2 : 1);
+                for (int pass = 0; pass < passes; ++pass) vel_points<BACK>(a, st, p0, p1, j, i, k, nt, c);
+            } else {
+                V[VX * F] = vxo + (sxx_x + sxy_y + sxz_z) / rip;
+                V[VY * F] = vyo + (syy_y + sxy_x + syz_z) / rjp;
+                V[VZ * F] = vzo + (szz_z + sxz_x + syz_y) / rkp;
+            }
+            if (j == probe_j && isnan(V[VY * F])) atomicMin(a.err_step + s, nt);
+        }
+        consumer_release(bar, it, true, false);
+        // planes move down one slot; the plane loaded into slot nslot becomes j+2
+        Rm2 = Rm1; Rm1 = R0; R0 = Rp1; Rp1 = Rp2; Rp2 = Rb + nslot * RSLOT;
+        if (++nslot == RING) nslot = 0;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Velocity update. Stage layout: [sxx|szz|sxz halo planes][vx vy vz][rip rjp rkp].
 template <bool BACK>
@@ -220,8 +368,8 @@ __global__ void __launch_bounds__(NTHR, 3) k_velocity_tma(const __grid_constant_
     const int j0 = ycn * g.cy + 1, j1 = min(j0 + g.cy - 1, g.ny);
     const int n = j1 - j0 + 1;
     float *ring = reinterpret_cast<float *>(smem);
-    constexpr int SP = 3 * RPLANE + 6 * PT;
-    float *stg = ring + RING * 3 * RPLANE;
+    constexpr int SP = VS_SP;
+    float *stg = ring + RING * RSLOT;
     uint64_t *bar = reinterpret_cast<uint64_t *>(stg + 2 * SP);
     const int rfirst = j0 - 2, rlast = j1 + 2;
     if (!pipeline_start(bar, T.tma_err)) return;
@@ -231,16 +379,16 @@ __global__ void __launch_bounds__(NTHR, 3) k_velocity_tma(const __grid_constant_
         auto ring_load = [&](int P) {
             const int sl = (P - rfirst) % RING;
             mbar_expect_tx(&bar[sl], 3 * RPLANE * 4);
-            tma_load5(ring + sl * 3 * RPLANE, &T.m_halo, zc(k0) - HZ, xc(i0) - HX, yc_(P), SYY, s, &bar[sl]);
+            tma_load5(ring + sl * RSLOT, &T.m_halo, zc(k0) - HZ, xc(i0) - HX, yc_(P), SYY, s, &bar[sl]);
         };
         auto stage_load = [&](int it) {
             const int j = j0 + it, b = it & 1;
             float *d = stg + b * SP;
             uint64_t *fb = &bar[2 * RING + b];
-            mbar_expect_tx(fb, SP * 4);
+            mbar_expect_tx(fb, (3 * RPLANE + 6 * PT) * 4);
             tma_load5(d, &T.m_halo, zc(k0) - HZ, xc(i0) - HX, yc_(j), SXX, s, fb);
-            tma_load5(d + 3 * RPLANE, &T.m_pt, zc(k0), xc(i0), yc_(j), VX, s, fb);
-            tma_load4(d + 3 * RPLANE + 3 * PT, &T.m_mod, zc(k0), xc(i0), yc_(j), MD_RIP, fb);
+            tma_load5(d + VS_PT, &T.m_pt, zc(k0), xc(i0), yc_(j), VX, s, fb);
+            tma_load4(d + VS_MOD, &T.m_mod, zc(k0), xc(i0), yc_(j), MD_RIP, fb);
         };
         auto stage_prefetch = [&](int it) {
             const int j = j0 + it;
@@ -271,101 +419,11 @@ __global__ void __launch_bounds__(NTHR, 3) k_velocity_tma(const __grid_constant_
     }
 
     // ---------------- consumer warps: row tx of the tile
-    const int k = k0 + tz, i = i0 + tx;
-    const bool active = k <= g.nz && i <= g.nx;
-    int p0, p1;
-    block_points(a.pt_off, g, s, ycn, p0, p1);
-    float *st = a.st + (long long)s * a.st_shot;
-    float *ps = a.psi + (long long)s * a.psi_shot;
-    const long long F = g.field;
-    const float b1 = a.b1, b2 = a.b2, dx = a.dxr, dy = a.dyr, dz = a.dzr;
-    const int hx = face_x(g, i), hz = face_z(g, k);
-    const int cz = tz + HZ, cx = tx + HX;
-    const bool probe_here = a.probe_i == i && a.probe_k == k;
-    int sl = 2;  // ring slot of plane j (plane j0 has ring index 2)
-    PsiPre q{};
-    if (active && (hx || hz || face_y(g, j0))) psi_load(q, ps, a.sl, g, j0, i, k, hx, hz);
-    for (int it = 0, j = j0; j <= j1; ++it, ++j) {
-        if (!consumer_wait(bar, it, j, j0, rfirst)) { if (tz == 0) atomicExch(T.tma_err, 1); return; }
-        // everything this row needs from the stage, so the stage can go back at once
-        float sxx_x = 0.f, sxz_z = 0.f, szz_z = 0.f, sxz_x = 0.f;
-        float vxo = 0.f, vyo = 0.f, vzo = 0.f, rip = 1.f, rjp = 1.f, rkp = 1.f;
-        if (active) {
-            const float *stage = stg + (it & 1) * SP;
-            const float *Ip = stage + cx * RZ + cz;
-            // stage in-plane fields: 0 sxx, 1 szz, 2 sxz
-#define IP(f, x, z) Ip[(f) * RPLANE + (x) * RZ + (z)]
-            sxx_x = dx * (b1 * (IP(0, 1, 0) - IP(0, 0, 0)) + b2 * (IP(0, 2, 0) - IP(0, -1, 0)));
-            sxz_z = dz * (b1 * (IP(2, 0, 0) - IP(2, 0, -1)) + b2 * (IP(2, 0, 1) - IP(2, 0, -2)));
-            szz_z = dz * (b1 * (IP(1, 0, 1) - IP(1, 0, 0)) + b2 * (IP(1, 0, 2) - IP(1, 0, -1)));
-            sxz_x = dx * (b1 * (IP(2, 0, 0) - IP(2, -1, 0)) + b2 * (IP(2, 1, 0) - IP(2, -2, 0)));
-#undef IP
-            const float *pv = stage + 3 * RPLANE + tx * TZ + tz;
-            vxo = pv[0]; vyo = pv[PT]; vzo = pv[2 * PT];
-            rip = pv[3 * PT]; rjp = pv[4 * PT]; rkp = pv[5 * PT];
-        }
-        consumer_release(bar, it, false, true);
-        if (active) {
-            const int sm2 = sl >= 2 ? sl - 2 : sl + RING - 2, sm1 = sl >= 1 ? sl - 1 : sl + RING - 1;
-            const int sp1 = sl + 1 < RING ? sl + 1 : sl + 1 - RING, sp2 = sl + 2 < RING ? sl + 2 : sl + 2 - RING;
-            const float *R0 = ring + sl * 3 * RPLANE + cx * RZ + cz;
-            const float *Rm2 = ring + sm2 * 3 * RPLANE + cx * RZ + cz, *Rm1 = ring + sm1 * 3 * RPLANE + cx * RZ + cz;
-            const float *Rp1 = ring + sp1 * 3 * RPLANE + cx * RZ + cz, *Rp2 = ring + sp2 * 3 * RPLANE + cx * RZ + cz;
-            // ring fields: 0 syy, 1 sxy, 2 syz
-#define RF(Rp, f, x, z) Rp[(f) * RPLANE + (x) * RZ + (z)]
-            float sxy_y = dy * (b1 * (RF(R0, 1, 0, 0) - RF(Rm1, 1, 0, 0)) + b2 * (RF(Rp1, 1, 0, 0) - RF(Rm2, 1, 0, 0)));
-            float syy_y = dy * (b1 * (RF(Rp1, 0, 0, 0) - RF(R0, 0, 0, 0)) + b2 * (RF(Rp2, 0, 0, 0) - RF(Rm1, 0, 0, 0)));
-            float sxy_x = dx * (b1 * (RF(R0, 1, 0, 0) - RF(R0, 1, -1, 0)) + b2 * (RF(R0, 1, 1, 0) - RF(R0, 1, -2, 0)));
-            float syz_z = dz * (b1 * (RF(R0, 2, 0, 0) - RF(R0, 2, 0, -1)) + b2 * (RF(R0, 2, 0, 1) - RF(R0, 2, 0, -2)));
-            float syz_y = dy * (b1 * (RF(R0, 2, 0, 0) - RF(Rm1, 2, 0, 0)) + b2 * (RF(Rp1, 2, 0, 0) - RF(Rm2, 2, 0, 0)));
-#undef RF
-            const int hy = face_y(g, j);
-            const bool frame = hx || hy || hz;
-            if (hx) {
-                float *p = ps + sxi(g, j, hx, k);
-                const long long o = a.sl.sx;
-                float v0 = CP(BH_X, hx) * q.x[0] + CP(AH_X, hx) * sxx_x; p[0] = v0; sxx_x = sxx_x / CP(KH_X, hx) + v0;
-                float v1 = CP(B_X, hx) * q.x[1] + CP(A_X, hx) * sxy_x; p[o] = v1; sxy_x = sxy_x / CP(K_X, hx) + v1;
-                float v2 = CP(B_X, hx) * q.x[2] + CP(A_X, hx) * sxz_x; p[2 * o] = v2; sxz_x = sxz_x / CP(K_X, hx) + v2;
-            }
-            if (hy) {
-                float *p = ps + 3 * a.sl.sx + syi(g, hy, i, k);
-                const long long o = a.sl.sy;
-                float v0 = CP(B_Y, hy) * q.y[0] + CP(A_Y, hy) * sxy_y; p[0] = v0; sxy_y = sxy_y / CP(K_Y, hy) + v0;
-                float v1 = CP(BH_Y, hy) * q.y[1] + CP(AH_Y, hy) * syy_y; p[o] = v1; syy_y = syy_y / CP(KH_Y, hy) + v1;
-                float v2 = CP(B_Y, hy) * q.y[2] + CP(A_Y, hy) * syz_y; p[2 * o] = v2; syz_y = syz_y / CP(K_Y, hy) + v2;
-            }
-            if (hz) {
-                float *p = ps + 3 * a.sl.sx + 3 * a.sl.sy + szi(g, j, i, hz);
-                const long long o = a.sl.sz;
-                const float *cg = a.cpg;
-                float v0 = CPG(cg, B_Z, hz) * q.z[0] + CPG(cg, A_Z, hz) * sxz_z; p[0] = v0; sxz_z = sxz_z / CPG(cg, K_Z, hz) + v0;
-                float v1 = CPG(cg, B_Z, hz) * q.z[1] + CPG(cg, A_Z, hz) * syz_z; p[o] = v1; syz_z = syz_z / CPG(cg, K_Z, hz) + v1;
-                float v2 = CPG(cg, BH_Z, hz) * q.z[2] + CPG(cg, AH_Z, hz) * szz_z; p[2 * o] = v2; szz_z = szz_z / CPG(cg, KH_Z, hz) + v2;
-            }
-            // the next plane's PML memory, a plane ahead of its use
-            if (j < j1 && (hx || hz || face_y(g, j + 1))) psi_load(q, ps, a.sl, g, j + 1, i, k, hx, hz);
-            const long long c = widx(g, j, i, k);
-            float *V = st + c;
-            if (p1 > p0) {
-                // cells of this block hold point forces: the order of update_v / update_v_CPML
-                V[VX * F] = vxo; V[VY * F] = vyo; V[VZ * F] = vzo;
-                if (frame) vel_points<BACK>(a, st, p0, p1, j, i, k, nt, c);
-                V[VX * F] = V[VX * F] + (sxx_x + sxy_y + sxz_z) / rip;
-                V[VY * F] = V[VY * F] + (syy_y + sxy_x + syz_z) / rjp;
-                V[VZ * F] = V[VZ * F] + (szz_z + sxz_x + syz_y) / rkp;
-                const int passes = frame ? (BACK ? 1 : 0) : (BACK ? 2 : 1);
-                for (int pass = 0; pass < passes; ++pass) vel_points<BACK>(a, st, p0, p1, j, i, k, nt, c);
-            } else {
-                V[VX * F] = vxo + (sxx_x + sxy_y + sxz_z) / rip;
-                V[VY * F] = vyo + (syy_y + sxy_x + syz_z) / rjp;
-                V[VZ * F] = vzo + (szz_z + sxz_x + syz_y) / rkp;
-            }
-            if (probe_here && j == a.probe_j && isnan(V[VY * F])) atomicMin(a.err_step + s, nt);
-        }
-        consumer_release(bar, it, true, false);
-        sl = sl + 1 < RING ? sl + 1 : 0;
-    }
+    // A tile that touches no x or z PML face lies wholly inside the grid: the
+    // lean instance drops the x/z frame code and the bounds test.
+    const bool xz = i0 <= g.fw || i0 + TX - 1 > g.nx - g.fw || k0 <= g.fw || k0 + TZ - 1 > g.nz - g.fw;
+    if (xz) vel_rows<BACK, true>(T, nt, ring, stg, bar, j0, j1, s, ycn, k0, i0);
+    else vel_rows<BACK, false>(T, nt, ring, stg, bar, j0, j1, s, ycn, k0, i0);
 }
 
 // ---------------------------------------------------------------------------
@@ -377,8 +435,20 @@ __device__ __forceinline__ float ddiv(float a, float d, float inv) {
     else return a / d;
 }
 
+// Register cap of the stress kernel. An SM sub-partition holds 16,384 registers
+// and a CTA's TX+1 warps spread over the 4 sub-partitions, so the cap decides
+// how many CTAs share an SM: with 9-warp CTAs, two need 5 warps on one
+// sub-partition, i.e. at most 96 registers per thread. The elastic kernel fits
+// 96 without spilling (2 CTAs per SM); with memory variables 96 spills heavily,
+// so those keep 112 (1 CTA per SM), which measured faster.
+#ifndef IFOSB_STR_MAXNREG
+#define IFOSB_STR_MAXNREG 112
+#endif
+#ifndef IFOSB_STR_MAXNREG_ELASTIC
+#define IFOSB_STR_MAXNREG_ELASTIC 96
+#endif
 template <int L, bool P2>
-__global__ void __maxnreg__(112) k_stress_tma(const __grid_constant__ StrTma T, int nt, int do_dft, int sample) {
+__global__ void __maxnreg__(L == 0 ? IFOSB_STR_MAXNREG_ELASTIC : IFOSB_STR_MAXNREG) k_stress_tma(const __grid_constant__ StrTma T, int nt, int do_dft, int sample) {
     extern __shared__ __align__(128) unsigned char smem[];
     const StrArgs &a = T.a;
     const Geo &g = a.g;
@@ -388,9 +458,9 @@ __global__ void __maxnreg__(112) k_stress_tma(const __grid_constant__ StrTma T, 
     const int j0 = ycn * g.cy + 1, j1 = min(j0 + g.cy - 1, g.ny);
     const int n = j1 - j0 + 1;
     const int nsr = T.nsr, nm = T.nm, ndf = do_dft ? T.ndf : 0;
-    const int SP = (nsr + nm + T.ndf) * PT;
+    const int SP = str_stage(nsr, nm, T.ndf), MOFF = str_mod_off(nsr), DOFF = str_dft_off(nsr, nm);
     float *ring = reinterpret_cast<float *>(smem);
-    float *stg = ring + RING * 3 * RPLANE;
+    float *stg = ring + RING * RSLOT;
     uint64_t *bar = reinterpret_cast<uint64_t *>(stg + 2 * SP);
     const int rfirst = j0 - 2, rlast = j1 + 2;
     if (!pipeline_start(bar, T.tma_err)) return;
@@ -401,7 +471,7 @@ __global__ void __maxnreg__(112) k_stress_tma(const __grid_constant__ StrTma T, 
         auto ring_load = [&](int P) {
             const int sl = (P - rfirst) % RING;
             mbar_expect_tx(&bar[sl], 3 * RPLANE * 4);
-            tma_load5(ring + sl * 3 * RPLANE, &T.m_halo, zc(k0) - HZ, xc(i0) - HX, yc_(P), VX, s, &bar[sl]);
+            tma_load5(ring + sl * RSLOT, &T.m_halo, zc(k0) - HZ, xc(i0) - HX, yc_(P), VX, s, &bar[sl]);
         };
         auto stage_load = [&](int it) {
             const int j = j0 + it, b = it & 1;
@@ -409,8 +479,8 @@ __global__ void __maxnreg__(112) k_stress_tma(const __grid_constant__ StrTma T, 
             uint64_t *fb = &bar[2 * RING + b];
             mbar_expect_tx(fb, stage_bytes);
             tma_load5(d, &T.m_sr, zc(k0), xc(i0), yc_(j), SYY, s, fb);
-            tma_load4(d + nsr * PT, &T.m_mod, zc(k0), xc(i0), yc_(j), 0, fb);
-            if (ndf) tma_load5(d + (nsr + nm) * PT, &T.m_dft, zc(k0), xc(i0), yc_(j), 0, s, fb);
+            tma_load4(d + MOFF, &T.m_mod, zc(k0), xc(i0), yc_(j), 0, fb);
+            if (ndf) tma_load5(d + DOFF, &T.m_dft, zc(k0), xc(i0), yc_(j), 0, s, fb);
         };
         auto stage_prefetch = [&](int it) {
             const int j = j0 + it;
@@ -462,9 +532,9 @@ __global__ void __maxnreg__(112) k_stress_tma(const __grid_constant__ StrTma T, 
             const float *stage = stg + (it & 1) * SP;
             const int sm2 = sl >= 2 ? sl - 2 : sl + RING - 2, sm1 = sl >= 1 ? sl - 1 : sl + RING - 1;
             const int sp1 = sl + 1 < RING ? sl + 1 : sl + 1 - RING, sp2 = sl + 2 < RING ? sl + 2 : sl + 2 - RING;
-            const float *R0 = ring + sl * 3 * RPLANE + cx * RZ + cz;
-            const float *Rm2 = ring + sm2 * 3 * RPLANE + cx * RZ + cz, *Rm1 = ring + sm1 * 3 * RPLANE + cx * RZ + cz;
-            const float *Rp1 = ring + sp1 * 3 * RPLANE + cx * RZ + cz, *Rp2 = ring + sp2 * 3 * RPLANE + cx * RZ + cz;
+            const float *R0 = ring + sl * RSLOT + cx * RZ + cz;
+            const float *Rm2 = ring + sm2 * RSLOT + cx * RZ + cz, *Rm1 = ring + sm1 * RSLOT + cx * RZ + cz;
+            const float *Rp1 = ring + sp1 * RSLOT + cx * RZ + cz, *Rp2 = ring + sp2 * RSLOT + cx * RZ + cz;
 #define RF(Rp, f, x, z) Rp[(f) * RPLANE + (x) * RZ + (z)]
             const float vx0 = RF(R0, 0, 0, 0), vy0 = RF(R0, 1, 0, 0), vz0 = RF(R0, 2, 0, 0);
             float vxx = ddiv<P2>(b1 * (vx0 - RF(R0, 0, -1, 0)) + b2 * (RF(R0, 0, 1, 0) - RF(R0, 0, -2, 0)), DX, iX);
@@ -507,7 +577,7 @@ __global__ void __maxnreg__(112) k_stress_tma(const __grid_constant__ StrTma T, 
             // the next plane's PML memory, a plane ahead of its use
             if (j < j1 && (hx || hz || face_y(g, j + 1))) psi_load(q, ps, a.sl, g, j + 1, i, k, hx, hz);
             const float *S = stage + tx * TZ + tz;      // sigma + memory variables (old values)
-            const float *Mo = S + nsr * PT;             // model
+            const float *Mo = S + MOFF;                 // model
             const float pim = Mo[MD_PI * PT], um = Mo[MD_U * PT];
             const float uipjp = Mo[MD_UIPJP * PT], ujpkp = Mo[MD_UJPKP * PT], uipkp = Mo[MD_UIPKP * PT];
             const float vxyyx = vxy + vyx, vyzzy = vyz + vzy, vxzzx = vxz + vzx;
@@ -596,7 +666,7 @@ __global__ void __maxnreg__(112) k_stress_tma(const __grid_constant__ StrTma T, 
                 }
             }
             if (ndf) {
-                const float *Fs = S + (nsr + nm) * PT;
+                const float *Fs = S + DOFF;
                 float *Fd = a.dft + (long long)s * a.dft_shot + c;
                 const double *tr = a.trig + (long long)(nt - 1) * a.nf * 2;
                 for (int l = 0; l < a.nf; ++l) {
