@@ -53,7 +53,12 @@ constexpr int VS_MOD = VS_PT + a32(3 * PT);  // velocity stage: offset of the ri
 constexpr int VS_SP = VS_MOD + a32(3 * PT);  // velocity stage stride
 static_assert(RSLOT % 32 == 0 && VS_PT % 32 == 0 && VS_MOD % 32 == 0 && VS_SP % 32 == 0, "TMA alignment");
 constexpr int NTHR = 32 * (TX + 1);          // TX consumer warps + 1 producer warp
-constexpr int NBAR = 2 * RING + 4;           // full/empty per ring slot, full/empty per stage
+#ifndef IFOSB_NSTAGE
+#define IFOSB_NSTAGE 2
+#endif
+constexpr int NSTAGE = IFOSB_NSTAGE;         // stage buffers (point-wise fields of NSTAGE planes in flight)
+static_assert(NSTAGE >= 2, "two stages at least");
+constexpr int NBAR = 2 * RING + 2 * NSTAGE;  // full/empty per ring slot, full/empty per stage
 
 __device__ __forceinline__ uint32_t su32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -161,7 +166,7 @@ struct StrTma {
 };
 
 __host__ __device__ constexpr size_t vel_tma_smem() {
-    return sizeof(float) * ((size_t)RING * RSLOT + 2 * (size_t)VS_SP) + 8 * NBAR;
+    return sizeof(float) * ((size_t)RING * RSLOT + NSTAGE * (size_t)VS_SP) + 8 * NBAR;
 }
 // Stress stage: [sigma + memory variables: nsr][model: nm][DFT: ndf] boxes of PT
 // floats per field, each box start rounded up to 32 floats.
@@ -169,7 +174,7 @@ __host__ __device__ inline int str_mod_off(int nsr) { return a32(nsr * PT); }
 __host__ __device__ inline int str_dft_off(int nsr, int nm) { return a32(nsr * PT) + a32(nm * PT); }
 __host__ __device__ inline int str_stage(int nsr, int nm, int ndf) { return str_dft_off(nsr, nm) + a32(ndf * PT); }
 __host__ __device__ inline size_t str_tma_smem(int nsr, int nm, int ndf) {
-    return sizeof(float) * ((size_t)RING * RSLOT + 2 * (size_t)str_stage(nsr, nm, ndf)) + 8 * NBAR;
+    return sizeof(float) * ((size_t)RING * RSLOT + NSTAGE * (size_t)str_stage(nsr, nm, ndf)) + 8 * NBAR;
 }
 
 // CTA start: returns false (for every thread) if an earlier CTA reported a timeout.
@@ -182,9 +187,9 @@ __device__ __forceinline__ bool pipeline_start(uint64_t *bar, const int *err) {
                 mbar_init(&bar[q], 1);             // full ring slot
                 mbar_init(&bar[RING + q], TX);     // empty ring slot
             }
-            for (int b = 0; b < 2; ++b) {
-                mbar_init(&bar[2 * RING + b], 1);  // full stage
-                mbar_init(&bar[2 * RING + 2 + b], TX);  // empty stage
+            for (int b = 0; b < NSTAGE; ++b) {
+                mbar_init(&bar[2 * RING + b], 1);            // full stage
+                mbar_init(&bar[2 * RING + NSTAGE + b], TX);  // empty stage
             }
             asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         }
@@ -202,7 +207,7 @@ __device__ __forceinline__ bool consumer_wait(uint64_t *bar, int it, int j, int 
         const int r = j + 2 - rfirst;
         ok &= mbar_wait(&bar[r % RING], (r / RING) & 1);
     }
-    ok &= mbar_wait(&bar[2 * RING + (it & 1)], (it >> 1) & 1);
+    ok &= mbar_wait(&bar[2 * RING + it % NSTAGE], (it / NSTAGE) & 1);
     return ok;
 }
 
@@ -233,7 +238,7 @@ __device__ __forceinline__ void consumer_release(uint64_t *bar, int it, bool rin
     __syncwarp();
     if (threadIdx.x == 0) {
         if (ring_slot) mbar_arrive(&bar[RING + it % RING]);
-        if (stage) mbar_arrive(&bar[2 * RING + 2 + (it & 1)]);
+        if (stage) mbar_arrive(&bar[2 * RING + NSTAGE + it % NSTAGE]);
     }
 }
 
@@ -276,13 +281,13 @@ __device__ __forceinline__ void vel_rows(const VelTma &T, int nt, const float *r
             ok &= mbar_wait(&bar[wslot], wpar);
             if (++wslot == RING) { wslot = 0; wpar ^= 1; }
         }
-        ok &= mbar_wait(&bar[2 * RING + (it & 1)], (it >> 1) & 1);
+        ok &= mbar_wait(&bar[2 * RING + it % NSTAGE], (it / NSTAGE) & 1);
         if (!ok) { if (tz == 0) atomicExch(T.tma_err, 1); return; }
         // everything this row needs from the stage, so the stage can go back at once
         float sxx_x = 0.f, sxz_z = 0.f, szz_z = 0.f, sxz_x = 0.f;
         float vxo = 0.f, vyo = 0.f, vzo = 0.f, rip = 1.f, rjp = 1.f, rkp = 1.f;
         if (active) {
-            const float *stage = stg + (it & 1) * SP;
+            const float *stage = stg + (it % NSTAGE) * SP;
             const float *Ip = stage + cx * RZ + cz;
             // stage in-plane fields: 0 sxx, 1 szz, 2 sxz
 #define IP(f, x, z) Ip[(f) * RPLANE + (x) * RZ + (z)]
@@ -370,7 +375,7 @@ __global__ void __launch_bounds__(NTHR, 3) k_velocity_tma(const __grid_constant_
     float *ring = reinterpret_cast<float *>(smem);
     constexpr int SP = VS_SP;
     float *stg = ring + RING * RSLOT;
-    uint64_t *bar = reinterpret_cast<uint64_t *>(stg + 2 * SP);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(stg + NSTAGE * SP);
     const int rfirst = j0 - 2, rlast = j1 + 2;
     if (!pipeline_start(bar, T.tma_err)) return;
 
@@ -382,7 +387,7 @@ __global__ void __launch_bounds__(NTHR, 3) k_velocity_tma(const __grid_constant_
             tma_load5(ring + sl * RSLOT, &T.m_halo, zc(k0) - HZ, xc(i0) - HX, yc_(P), SYY, s, &bar[sl]);
         };
         auto stage_load = [&](int it) {
-            const int j = j0 + it, b = it & 1;
+            const int j = j0 + it, b = it % NSTAGE;
             float *d = stg + b * SP;
             uint64_t *fb = &bar[2 * RING + b];
             mbar_expect_tx(fb, (3 * RPLANE + 6 * PT) * 4);
@@ -398,9 +403,9 @@ __global__ void __launch_bounds__(NTHR, 3) k_velocity_tma(const __grid_constant_
         };
         auto ring_prefetch = [&](int P) { tma_prefetch5(&T.m_halo, zc(k0) - HZ, xc(i0) - HX, yc_(P), SYY, s); };
         for (int P = rfirst; P <= min(rfirst + RING - 1, rlast); ++P) ring_load(P);
-        for (int it = 0; it < 2 && it < n; ++it) stage_load(it);
+        for (int it = 0; it < NSTAGE && it < n; ++it) stage_load(it);
         for (int q = 0; q < L2AHEAD; ++q) {
-            if (2 + q < n) stage_prefetch(2 + q);
+            if (NSTAGE + q < n) stage_prefetch(NSTAGE + q);
             if (rfirst + RING + q <= rlast) ring_prefetch(rfirst + RING + q);
         }
         for (int it = 0; it < n; ++it) {
@@ -409,10 +414,13 @@ __global__ void __launch_bounds__(NTHR, 3) k_velocity_tma(const __grid_constant_
                 ring_load(rfirst + it + RING);
                 if (rfirst + it + RING + L2AHEAD <= rlast) ring_prefetch(rfirst + it + RING + L2AHEAD);
             }
-            if (it + 2 < n) {
-                if (!mbar_wait(&bar[2 * RING + 2 + (it & 1)], (it >> 1) & 1)) { atomicExch(T.tma_err, 1); return; }
-                stage_load(it + 2);
-                if (it + 2 + L2AHEAD < n) stage_prefetch(it + 2 + L2AHEAD);
+            if (it + NSTAGE < n) {
+                if (!mbar_wait(&bar[2 * RING + NSTAGE + it % NSTAGE], (it / NSTAGE) & 1)) {
+                    atomicExch(T.tma_err, 1);
+                    return;
+                }
+                stage_load(it + NSTAGE);
+                if (it + NSTAGE + L2AHEAD < n) stage_prefetch(it + NSTAGE + L2AHEAD);
             }
         }
         return;
@@ -461,7 +469,7 @@ __global__ void __maxnreg__(L == 0 ? IFOSB_STR_MAXNREG_ELASTIC : IFOSB_STR_MAXNR
     const int SP = str_stage(nsr, nm, T.ndf), MOFF = str_mod_off(nsr), DOFF = str_dft_off(nsr, nm);
     float *ring = reinterpret_cast<float *>(smem);
     float *stg = ring + RING * RSLOT;
-    uint64_t *bar = reinterpret_cast<uint64_t *>(stg + 2 * SP);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(stg + NSTAGE * SP);
     const int rfirst = j0 - 2, rlast = j1 + 2;
     if (!pipeline_start(bar, T.tma_err)) return;
 
@@ -474,7 +482,7 @@ __global__ void __maxnreg__(L == 0 ? IFOSB_STR_MAXNREG_ELASTIC : IFOSB_STR_MAXNR
             tma_load5(ring + sl * RSLOT, &T.m_halo, zc(k0) - HZ, xc(i0) - HX, yc_(P), VX, s, &bar[sl]);
         };
         auto stage_load = [&](int it) {
-            const int j = j0 + it, b = it & 1;
+            const int j = j0 + it, b = it % NSTAGE;
             float *d = stg + b * SP;
             uint64_t *fb = &bar[2 * RING + b];
             mbar_expect_tx(fb, stage_bytes);
@@ -490,9 +498,9 @@ __global__ void __maxnreg__(L == 0 ? IFOSB_STR_MAXNREG_ELASTIC : IFOSB_STR_MAXNR
         };
         auto ring_prefetch = [&](int P) { tma_prefetch5(&T.m_halo, zc(k0) - HZ, xc(i0) - HX, yc_(P), VX, s); };
         for (int P = rfirst; P <= min(rfirst + RING - 1, rlast); ++P) ring_load(P);
-        for (int it = 0; it < 2 && it < n; ++it) stage_load(it);
+        for (int it = 0; it < NSTAGE && it < n; ++it) stage_load(it);
         for (int q = 0; q < L2AHEAD; ++q) {
-            if (2 + q < n) stage_prefetch(2 + q);
+            if (NSTAGE + q < n) stage_prefetch(NSTAGE + q);
             if (rfirst + RING + q <= rlast) ring_prefetch(rfirst + RING + q);
         }
         for (int it = 0; it < n; ++it) {
@@ -501,10 +509,13 @@ __global__ void __maxnreg__(L == 0 ? IFOSB_STR_MAXNREG_ELASTIC : IFOSB_STR_MAXNR
                 ring_load(rfirst + it + RING);
                 if (rfirst + it + RING + L2AHEAD <= rlast) ring_prefetch(rfirst + it + RING + L2AHEAD);
             }
-            if (it + 2 < n) {
-                if (!mbar_wait(&bar[2 * RING + 2 + (it & 1)], (it >> 1) & 1)) { atomicExch(T.tma_err, 1); return; }
-                stage_load(it + 2);
-                if (it + 2 + L2AHEAD < n) stage_prefetch(it + 2 + L2AHEAD);
+            if (it + NSTAGE < n) {
+                if (!mbar_wait(&bar[2 * RING + NSTAGE + it % NSTAGE], (it / NSTAGE) & 1)) {
+                    atomicExch(T.tma_err, 1);
+                    return;
+                }
+                stage_load(it + NSTAGE);
+                if (it + NSTAGE + L2AHEAD < n) stage_prefetch(it + NSTAGE + L2AHEAD);
             }
         }
         return;
@@ -529,7 +540,7 @@ __global__ void __maxnreg__(L == 0 ? IFOSB_STR_MAXNREG_ELASTIC : IFOSB_STR_MAXNR
     for (int it = 0, j = j0; j <= j1; ++it, ++j) {
         if (!consumer_wait(bar, it, j, j0, rfirst)) { if (tz == 0) atomicExch(T.tma_err, 1); return; }
         if (active) {
-            const float *stage = stg + (it & 1) * SP;
+            const float *stage = stg + (it % NSTAGE) * SP;
             const int sm2 = sl >= 2 ? sl - 2 : sl + RING - 2, sm1 = sl >= 1 ? sl - 1 : sl + RING - 1;
             const int sp1 = sl + 1 < RING ? sl + 1 : sl + 1 - RING, sp2 = sl + 2 < RING ? sl + 2 : sl + 2 - RING;
             const float *R0 = ring + sl * RSLOT + cx * RZ + cz;
