@@ -15,6 +15,7 @@
 
 #include <cmath>
 #include <string>
+#include <vector>
 
 namespace {
 
@@ -230,6 +231,83 @@ __global__ void k_modelupdate(const float *g, float *rho, float *pi, float *u, U
     }
 }
 
+// precongrad.c:28-336 on one cell: the source and receiver damping factors
+// (functions of the integer squared distance, tabulated on the host with the
+// reference's double expressions) and the per-axis edge factors, multiplied in
+// the reference's order; factors that are exactly 1.0f are skipped (exact).
+struct PreArgs {
+    int nx, ny, nz, type;
+    int nsrc, ntr, ds, dr;            // table lengths: factors beyond them are 1.0f
+    const int *src, *rec;             // [nsrc][3], [ntr][3]: x, y, z grid indices
+    const float *lut_s, *lut_r;       // by squared distance
+    const float *ty, *tx, *tz;        // [2][ny], [2][nx], [2][nz] edge factor pairs
+};
+__global__ void k_precon(float *g, PreArgs a) {
+    const long long n = (long long)a.nx * a.ny * a.nz;
+    for (long long l = blockIdx.x * (long long)RTHR + threadIdx.x; l < n; l += (long long)RBLK * RTHR) {
+        const int k = (int)(l % a.nz) + 1, i = (int)((l / a.nz) % a.nx) + 1, j = (int)(l / ((long long)a.nz * a.nx)) + 1;
+        float g0 = g[l], g1 = g[n + l], g2 = g[2 * n + l];
+        if (a.type == 2)
+            for (int q = 0; q < a.nsrc; ++q) {
+                const int ex = i - a.src[3 * q], ey = j - a.src[3 * q + 1], ez = k - a.src[3 * q + 2];
+                const int d2 = ey * ey + ex * ex + ez * ez;
+                if (d2 < a.ds) {
+                    const float G = a.lut_s[d2];
+                    g0 = g0 * G; g1 = g1 * G; g2 = g2 * G;
+                }
+            }
+        if (a.type == 1 || a.type == 2)
+            for (int q = 0; q < a.ntr; ++q) {
+                const int ex = i - a.rec[3 * q], ey = j - a.rec[3 * q + 1], ez = k - a.rec[3 * q + 2];
+                const int d2 = ey * ey + ex * ex + ez * ez;
+                if (d2 < a.dr) {
+                    const float G = a.lut_r[d2];
+                    g0 = g0 * G; g1 = g1 * G; g2 = g2 * G;
+                }
+            }
+        const float y0 = a.ty[j - 1], y1 = a.ty[a.ny + j - 1];
+        g0 = g0 * y0 * y1; g1 = g1 * y0 * y1; g2 = g2 * y0 * y1;
+        const float x0 = a.tx[i - 1], x1 = a.tx[a.nx + i - 1];
+        g0 = g0 * x0 * x1; g1 = g1 * x0 * x1; g2 = g2 * x0 * x1;
+        const float z0 = a.tz[k - 1], z1 = a.tz[a.nz + k - 1];
+        g0 = g0 * z0 * z1; g1 = g1 * z0 * z1; g2 = g2 * z0 * z1;
+        g[l] = g0; g[n + l] = g1; g[2 * n + l] = g2;
+    }
+}
+
+// constant_boundary (constant_boundary.c:27-222): one region of one phase.
+// mode 0: copy from (j, a0, k); 1: copy from (j, i, a0); 2: average around
+// (j, a0, k) with (j, a1, k); 3: average around (j, i, a0) with (j, i, a1). The
+// averages are the reference's double sums divided by 8.0.
+struct CbPhase {
+    int j0, j1, i0, i1, k0, k1, mode, a0, a1;
+};
+__global__ void k_cbound(float *rho, float *pi, float *u, int nx, int nz, CbPhase ph) {
+    const int ni = ph.i1 - ph.i0 + 1, nk = ph.k1 - ph.k0 + 1;
+    const long long n = (long long)(ph.j1 - ph.j0 + 1) * ni * nk;
+    const long long sj = (long long)(nx + 2) * (nz + 2), si = nz + 2;
+    float *f[3] = {u, pi, rho};
+    for (long long l = blockIdx.x * (long long)RTHR + threadIdx.x; l < n; l += (long long)RBLK * RTHR) {
+        const int k = ph.k0 + (int)(l % nk), i = ph.i0 + (int)((l / nk) % ni), j = ph.j0 + (int)(l / ((long long)nk * ni));
+        const long long d = j * sj + i * si + k;
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            float *a = f[q];
+            if (ph.mode == 0) {
+                a[d] = a[j * sj + ph.a0 * si + k];
+            } else if (ph.mode == 1) {
+                a[d] = a[j * sj + i * si + ph.a0];
+            } else if (ph.mode == 2) {
+                const long long c = j * sj + ph.a0 * si + k;
+                a[d] = (float)((3.0 * a[c] + a[c - sj] + a[c + sj] + a[c - 1] + a[c + 1] + a[j * sj + ph.a1 * si + k]) / 8.0);
+            } else {
+                const long long c = j * sj + i * si + ph.a0;
+                a[d] = (float)((3.0 * a[c] + a[c - sj] + a[c + sj] + a[c - si] + a[c + si] + a[j * sj + i * si + ph.a1]) / 8.0);
+            }
+        }
+    }
+}
+
 }  // namespace
 
 struct ifosb_optim {
@@ -430,4 +508,165 @@ extern "C" int ifosb_lbfgs_history(const ifosb_optim *o, double *s, double *y, d
     if (scale && cudaMemcpy(scale, o->d_sc, sizeof(double) * o->bfgsnum, cudaMemcpyDeviceToHost) != cudaSuccess)
         return IFOSB_ECUDA;
     return IFOSB_OK;
+}
+
+// Host side of precon_grad: the factor tables, computed with the reference's
+// expressions (float variables, double exp and division).
+static float damp_rec(int d2) {  // precongrad.c:53-58: 1/(1+1000 exp(-0.7 r^2))
+    const float r = (float)sqrt((double)d2);
+    return (float)(1 / (1 + 1000 * exp(-0.7 * r * r)));
+}
+static float damp_src(int d2) {  // precongrad.c:133-143: 1/(1+1000 exp(-0.7 r))
+    const float r = (float)sqrt((double)d2);
+    return (float)(1 / (1 + 1000 * exp(-0.7 * r)));
+}
+static float damp_edge(int x) {  // 1/(1+2000 exp(-0.6 r)), r = x
+    const float r = (float)(x * 1.0);
+    return (float)(1 / (1 + 2000 * exp(-0.6 * r)));
+}
+// Table of f(d2) up to the first d2 from which f is exactly 1.0f (checked on to
+// 4 times that length); returns the length.
+static std::vector<float> damp_table(float (*f)(int)) {
+    std::vector<float> t;
+    int d2 = 0;
+    for (; d2 < (1 << 22); ++d2) {
+        const float v = f(d2);
+        if (v == 1.0f) {
+            bool ones = true;
+            for (int q = d2; q < 4 * d2 + 64 && ones; ++q) ones = f(q) == 1.0f;
+            if (ones) break;
+        }
+        t.push_back(v);
+    }
+    return t;
+}
+
+extern "C" int ifosb_precon_grad(ifosb_optim *o, float *grad, int damptype, int free_surf, int fw, float dx, float dy,
+                                 float dz, int nsrc, const float *srcpos, int ntr, const int *recpos) {
+    if (!o || !grad || damptype < 0 || damptype > 3 || nsrc < 0 || ntr < 0) return IFOSB_EARG;
+    if ((nsrc > 0 && !srcpos) || (ntr > 0 && !recpos)) return IFOSB_EARG;
+    const int NX = o->nx, NY = o->ny, NZ = o->nz;
+    const long long n = o->n;
+    // edge factor pairs per axis; types 0 and 3 read ii, jj, kk, which those
+    // branches never assign (they stay 0, precongrad.c:34): constant tables
+    std::vector<float> ty(2 * NY), tx(2 * NX), tz(2 * NZ);
+    const bool pos = damptype == 1 || damptype == 2;
+    for (int j = 1; j <= NY; ++j) {
+        const int jj = pos ? j : 0;
+        float a, b;
+        if (damptype == 3) {  // precongrad.c:226-234
+            const int sh = fw + 40, rh = fw + 40;
+            float r = (float)((jj - sh) * 1.0);
+            a = r < 0 ? 0.0f : (float)(1 / (1 + 1000 * exp(-0.7 * r * r)));
+            r = (float)((NY - jj - rh) * 1.0);
+            b = r < 0 ? 0.0f : (float)(1 / (1 + 1000 * exp(-0.7 * r)));
+        } else {
+            a = free_surf ? 0.0f : damp_edge(jj);
+            b = damp_edge(NY - jj);
+        }
+        ty[j - 1] = a;
+        ty[NY + j - 1] = b;
+    }
+    for (int i = 1; i <= NX; ++i) {
+        const int ii = pos ? i : 0;
+        tx[i - 1] = damp_edge(ii);  // r = ii >= 0, so type 3's r < 0 test never fires
+        tx[NX + i - 1] = (NX - ii) < 0 ? 0.0f : damp_edge(NX - ii);
+    }
+    for (int k = 1; k <= NZ; ++k) {
+        const int kk = pos ? k : 0;
+        tz[k - 1] = damp_edge(kk);
+        tz[NZ + k - 1] = (NZ - kk) < 0 ? 0.0f : damp_edge(NZ - kk);
+    }
+    static const std::vector<float> lut_r = damp_table(damp_rec), lut_s = damp_table(damp_src);
+    std::vector<int> src(3 * (size_t)nsrc), rec(3 * (size_t)ntr);
+    for (int q = 0; q < nsrc; ++q) {  // iround(srcpos/DX) (fd.h:35) of the positions in metres
+        src[3 * q] = (int)floor(srcpos[3 * q] / dx + 0.5);
+        src[3 * q + 1] = (int)floor(srcpos[3 * q + 1] / dy + 0.5);
+        src[3 * q + 2] = (int)floor(srcpos[3 * q + 2] / dz + 0.5);
+    }
+    for (int q = 0; q < 3 * ntr; ++q) rec[q] = recpos[q];
+    // one device block for all tables
+    const size_t nf = ty.size() + tx.size() + tz.size() + lut_r.size() + lut_s.size();
+    const size_t ni = src.size() + rec.size();
+    float *dt = nullptr;
+    int *di = nullptr;
+    OCU(cudaMalloc(&dt, sizeof(float) * nf));
+    if (ni) {
+        cudaError_t ce = cudaMalloc(&di, sizeof(int) * ni);
+        if (ce != cudaSuccess) {
+            cudaFree(dt);
+            OCU(ce);
+        }
+    }
+    std::vector<float> hf;
+    hf.reserve(nf);
+    hf.insert(hf.end(), ty.begin(), ty.end());
+    hf.insert(hf.end(), tx.begin(), tx.end());
+    hf.insert(hf.end(), tz.begin(), tz.end());
+    hf.insert(hf.end(), lut_r.begin(), lut_r.end());
+    hf.insert(hf.end(), lut_s.begin(), lut_s.end());
+    std::vector<int> hi(src);
+    hi.insert(hi.end(), rec.begin(), rec.end());
+    PreArgs a;
+    a.nx = NX; a.ny = NY; a.nz = NZ; a.type = damptype;
+    a.nsrc = nsrc; a.ntr = ntr;
+    a.dr = (int)lut_r.size(); a.ds = (int)lut_s.size();
+    a.ty = dt; a.tx = dt + ty.size(); a.tz = a.tx + tx.size();
+    a.lut_r = a.tz + tz.size(); a.lut_s = a.lut_r + lut_r.size();
+    a.src = di; a.rec = di ? di + src.size() : nullptr;
+    int rc = IFOSB_OK;
+    cudaError_t ce = cudaMemcpyAsync(dt, hf.data(), sizeof(float) * nf, cudaMemcpyHostToDevice, o->stream);
+    if (ce == cudaSuccess && ni) ce = cudaMemcpyAsync(di, hi.data(), sizeof(int) * ni, cudaMemcpyHostToDevice, o->stream);
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(o->d_grad, grad, sizeof(float) * 3 * n, cudaMemcpyDefault, o->stream);
+    if (ce == cudaSuccess) {
+        k_precon<<<RBLK, RTHR, 0, o->stream>>>(o->d_grad, a);
+        ce = cudaGetLastError();
+    }
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(grad, o->d_grad, sizeof(float) * 3 * n, cudaMemcpyDefault, o->stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(o->stream);
+    if (ce != cudaSuccess) {
+        o->err = std::string("precon_grad: ") + cudaGetErrorString(ce);
+        rc = IFOSB_ECUDA;
+    }
+    cudaFree(dt);
+    if (di) cudaFree(di);
+    return rc;
+}
+
+extern "C" int ifosb_constant_boundary(ifosb_optim *o, float *rho, float *pi, float *u, int fw) {
+    if (!o || !rho || !pi || !u || fw < 1) return IFOSB_EARG;
+    const int NX = o->nx, NY = o->ny, NZ = o->nz, dist = 4;
+    if (NX < 2 * fw + dist + 2 || NZ < 2 * fw + dist + 2 || NY < 3) return ofail(o, IFOSB_EARG, "grid too small");
+    // one rank: the interior bounds of CPML_ini_elastic (CPML_ini_elastic.c:28-54)
+    const int nx1 = fw + 1, nx2 = NX - fw, nz1 = fw + 1, nz2 = NZ - fw;
+    const int a = fw + 1 + dist, b = fw + 2 + dist, c = nx2 - dist, cz = nz2 - dist;
+    // the reference's loops in their order; later faces read cells earlier ones rewrote
+    const CbPhase ph[] = {
+        {1, 1, 1, fw + dist, nz1, nz2, 0, a, 0},                      // x front, top row
+        {NY, NY, 1, fw + dist, nz1, nz2, 0, a, 0},                    // x front, bottom row
+        {2, NY - 1, 1, fw + dist, nz1, nz2, 2, a, b},                 // x front
+        {1, 1, nx2 + 1 - dist, nx2 + fw, nz1, nz2, 0, c, 0},          // x back, top row
+        {NY, NY, nx2 + 1 - dist, nx2 + fw, nz1, nz2, 0, c, 0},        // x back, bottom row
+        {2, NY - 1, nx2 + 1 - dist, nx2 + fw, nz1, nz2, 2, c, c - 1}, // x back
+        {1, 1, 1, NX, 1, fw + dist, 1, a, 0},                         // z front, top row
+        {NY, NY, 1, NX, 1, fw + dist, 1, a, 0},                       // z front, bottom row
+        {2, NY - 1, 1, fw + dist, 1, fw + dist, 1, a, 0},             // z front, x-front corner
+        {2, NY - 1, nx2 + 1 - dist, nx2 + fw, 1, fw + dist, 1, a, 0}, // z front, x-back corner
+        {2, NY - 1, nx1, nx2, 1, fw + dist, 3, a, b},                 // z front
+        {1, 1, 1, NX, nz2 + 1 - dist, nz2 + fw, 1, cz, 0},            // z back, top row
+        {NY, NY, 1, NX, nz2 + 1 - dist, nz2 + fw, 1, cz, 0},          // z back, bottom row
+        {2, NY - 1, 1, fw + dist, nz2 + 1 - dist, nz2 + fw, 1, cz, 0},
+        {2, NY - 1, nx2 + 1 - dist, nx2 + fw, nz2 + 1 - dist, nz2 + fw, 1, cz, 0},
+        {2, NY - 1, nx1, nx2, nz2 + 1 - dist, nz2 + fw, 3, cz, cz - 1}, // z back
+    };
+    const long long mg = (long long)(NX + 2) * (NY + 2) * (NZ + 2);
+    float *drho = o->d_model, *dpi = o->d_model + mg, *du = o->d_model + 2 * mg;
+    OCU(cudaMemcpyAsync(drho, rho, sizeof(float) * mg, cudaMemcpyDefault, o->stream));
+    OCU(cudaMemcpyAsync(dpi, pi, sizeof(float) * mg, cudaMemcpyDefault, o->stream));
+    OCU(cudaMemcpyAsync(du, u, sizeof(float) * mg, cudaMemcpyDefault, o->stream));
+    for (const CbPhase &q : ph) k_cbound<<<RBLK, RTHR, 0, o->stream>>>(drho, dpi, du, NX, NZ, q);
+    OCU(cudaMemcpyAsync(rho, drho, sizeof(float) * mg, cudaMemcpyDefault, o->stream));
+    OCU(cudaMemcpyAsync(pi, dpi, sizeof(float) * mg, cudaMemcpyDefault, o->stream));
+    OCU(cudaMemcpyAsync(u, du, sizeof(float) * mg, cudaMemcpyDefault, o->stream));
+    return finish(o);
 }

@@ -103,6 +103,9 @@ def lib():
                                             C.c_int, C.c_int]),
             "ifosb_lbfgs_history": (C.c_int, [vp, vp, vp, vp]),
             "ifosb_steplength": (C.c_int, [vp, vp, C.c_int, C.c_int, C.c_double, vp]),
+            "ifosb_constant_boundary": (C.c_int, [vp, vp, vp, vp, C.c_int]),
+            "ifosb_precon_grad": (C.c_int, [vp, vp, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float,
+                                            C.c_int, vp, C.c_int, vp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -122,7 +125,7 @@ def exported_symbols():
         "ifosb_wavelet", "ifosb_nsamples", "ifosb_moduli", "ifosb_set_profiling", "ifosb_kernel_times",
         "ifosb_set_stream", "ifosb_residual_noalloc", "ifosb_optim_create", "ifosb_optim_destroy",
         "ifosb_optim_last_error", "ifosb_conjugate", "ifosb_lbfgs_savegrad", "ifosb_lbfgs", "ifosb_modelupdate",
-        "ifosb_lbfgs_history", "ifosb_steplength",
+        "ifosb_lbfgs_history", "ifosb_steplength", "ifosb_precon_grad", "ifosb_constant_boundary",
     ]
 
 
@@ -392,6 +395,23 @@ class Optimizer:
         w = np.ascontiguousarray(weight, np.float32)
         self._c(lib().ifosb_modelupdate(self.h, _p(self._grad(grad)), _p(rho), _p(pi), _p(u), step, _p(w), vp0, vs0,
                                         rho0, int(bool(lbfgs)), it_group))
+
+    def precon_grad(self, grad, damptype, free_surf, fw, dh, srcpos_m, recpos):
+        """precon_grad on grad [3][NY][NX][NZ] in place; srcpos_m [nsrc][3] metres,
+        recpos [ntr][3] grid indices; dh = (DX, DY, DZ)."""
+        src = np.ascontiguousarray(np.atleast_2d(srcpos_m), np.float32) if len(srcpos_m) else None
+        rec = np.ascontiguousarray(np.atleast_2d(recpos), np.int32) if len(recpos) else None
+        self._c(lib().ifosb_precon_grad(self.h, _p(self._grad(grad)), damptype, int(bool(free_surf)), fw, dh[0], dh[1],
+                                        dh[2], 0 if src is None else src.shape[0], _p(src),
+                                        0 if rec is None else rec.shape[0], _p(rec)))
+
+    def constant_boundary(self, rho, pi, u, fw):
+        """constant_boundary on the ghosted model arrays in place."""
+        mshape = tuple(s + 2 for s in self.shape)
+        for a in (rho, pi, u):
+            if not (isinstance(a, np.ndarray) and a.dtype == np.float32 and a.flags.c_contiguous and a.shape == mshape):
+                raise ValueError(f"model arrays must be C-contiguous float32 of shape {mshape}")
+        self._c(lib().ifosb_constant_boundary(self.h, _p(rho), _p(pi), _p(u), fw))
 
     def history(self):
         nn = self.numpar * int(np.prod(self.shape))

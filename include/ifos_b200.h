@@ -218,6 +218,25 @@ int ifosb_lbfgs(ifosb_optim *o, float *grad, int it_group);
 int ifosb_modelupdate(ifosb_optim *o, float *grad, float *rho, float *pi, float *u, float step,
                       const float *weight, float vp0, float vs0, float rho0, int lbfgs, int it_group);
 
+/* precon_grad (src/precongrad.c:28-336): damping of grad[3][NY][NX][NZ] in place
+ * around sources (damptype 2), receivers (1, 2) and towards the model edges, as
+ * DAMPTYPE selects, with the reference's float results (the factors come from
+ * its double expressions, tabulated on the host). Quirks kept: with free_surf
+ * the y factor at the top is 0, so types 0-2 zero the gradient; types 0 and 3
+ * evaluate their edge factors at index 0 (the loop variables they read are
+ * never set). srcpos[nsrc][3]: source x, y, z in metres (srcpos[1..3][l]);
+ * recpos[ntr][3]: receiver grid indices (recpos[1..3][n]). */
+int ifosb_precon_grad(ifosb_optim *o, float *grad, int damptype, int free_surf, int fw, float dx, float dy, float dz,
+                      int nsrc, const float *srcpos, int ntr, const int *recpos);
+
+/* constant_boundary (src/constant_boundary.c:27-222), one rank, on the ghosted
+ * model rho, pi, u [NY+2][NX+2][NZ+2] in place: the model in the x and z CPML
+ * frames (and 4 cells more) replaced by copies and 6-point averages of the
+ * cells just inside, in the reference's order (later faces read cells earlier
+ * faces rewrote), with its double averages. The driver calls it after a model
+ * update when FREE_SURF (src/ifos3d.c:682, :1035). */
+int ifosb_constant_boundary(ifosb_optim *o, float *rho, float *pi, float *u, int fw);
+
 /* The L-BFGS history for inspection: s, y [BFGSNUM][NUMPAR*n], scale [BFGSNUM]. */
 int ifosb_lbfgs_history(const ifosb_optim *o, double *s, double *y, double *scale);
 

@@ -116,3 +116,52 @@ int ifo_ref_modelupdate(int nx, int ny, int nz, float *grad, float *rho, float *
     for (int c = 0; c < 3; c++) g_free(nx, ny, nz, g[c], grad + c * n);
     return 0;
 }
+
+extern int DAMPTYPE, FREE_SURF, FW, NXG, NYG, NZG, POS[4], NPROCX, NPROCY, NPROCZ;
+extern float DX, DY, DZ;
+
+/* precon_grad with DAMPTYPE, FREE_SURF, FW as given; srcpos [nsrc][3] metres,
+ * recpos [ntr][3] grid indices (the reference's srcpos[1..3][l], recpos[1..3][n]). */
+int ifo_ref_precon_grad(int nx, int ny, int nz, float *grad, int damptype, int free_surf, int fw, float dx, float dy,
+                        float dz, int nsrc, const float *srcpos, int ntr, const int *recpos) {
+    quiet();
+    NX = NXG = nx; NY = NYG = ny; NZ = NZG = nz;
+    DAMPTYPE = damptype; FREE_SURF = free_surf; FW = fw; DX = dx; DY = dy; DZ = dz;
+    POS[1] = POS[2] = POS[3] = 0;
+    const size_t n = (size_t)nx * ny * nz;
+    float ***g[3];
+    for (int c = 0; c < 3; c++) g[c] = g_alloc(nx, ny, nz, grad + c * n);
+    float **S = fmatrix(1, 7, 1, nsrc > 0 ? nsrc : 1);
+    for (int l = 1; l <= nsrc; l++)
+        for (int c = 1; c <= 3; c++) S[c][l] = srcpos[3 * (l - 1) + c - 1];
+    int **R = imatrix(1, 3, 1, ntr > 0 ? ntr : 1);
+    for (int t = 1; t <= ntr; t++)
+        for (int c = 1; c <= 3; c++) R[c][t] = recpos[3 * (t - 1) + c - 1];
+    precon_grad(nx, ny, nz, g[0], g[1], g[2], nsrc, S, ntr, R, 0.0f, 1, 0);
+    free_matrix(S, 1, 7, 1, nsrc > 0 ? nsrc : 1);
+    free_imatrix(R, 1, 3, 1, ntr > 0 ? ntr : 1);
+    for (int c = 0; c < 3; c++) g_free(nx, ny, nz, g[c], grad + c * n);
+    return 0;
+}
+
+/* constant_boundary on ghosted models [ny+2][nx+2][nz+2] with the one-rank
+ * interior bounds of CPML_ini_elastic (xb = FW+1..NX-FW, zb = FW+1..NZ-FW). */
+int ifo_ref_constant_boundary(int nx, int ny, int nz, int fw, float *rho, float *pi, float *u) {
+    quiet();
+    NX = nx; NY = ny; NZ = nz; FW = fw;
+    POS[1] = POS[2] = POS[3] = 0;
+    NPROCX = NPROCY = NPROCZ = 1;
+    const size_t mg = (size_t)(nx + 2) * (ny + 2) * (nz + 2);
+    float *src[3] = {rho, pi, u};
+    float ***m[3];
+    for (int c = 0; c < 3; c++) {
+        m[c] = f3tensor(0, ny + 1, 0, nx + 1, 0, nz + 1);
+        memcpy(&m[c][0][0][0], src[c], sizeof(float) * mg);
+    }
+    constant_boundary(fw + 1, nx - fw, 1, ny, fw + 1, nz - fw, m[1], m[2], m[0]);
+    for (int c = 0; c < 3; c++) {
+        memcpy(src[c], &m[c][0][0][0], sizeof(float) * mg);
+        free_f3tensor(m[c], 0, ny + 1, 0, nx + 1, 0, nz + 1);
+    }
+    return 0;
+}
