@@ -134,7 +134,8 @@ __device__ __forceinline__ void tma_prefetch4(const CUtensorMap *m, int c0, int 
                  : "memory");
 }
 
-// Planes are prefetched into L2 this many iterations before their shared-memory load.
+// Planes are prefetched into L2 this many iterations before their shared-memory load
+// (0: no L2 prefetch).
 #ifndef IFOSB_L2_AHEAD
 #define IFOSB_L2_AHEAD 3
 #endif
@@ -412,7 +413,7 @@ __global__ void __launch_bounds__(NTHR, 3) k_velocity_tma(const __grid_constant_
             if (rfirst + it + RING <= rlast) {
                 if (!mbar_wait(&bar[RING + it % RING], (it / RING) & 1)) { atomicExch(T.tma_err, 1); return; }
                 ring_load(rfirst + it + RING);
-                if (rfirst + it + RING + L2AHEAD <= rlast) ring_prefetch(rfirst + it + RING + L2AHEAD);
+                if (L2AHEAD > 0 && rfirst + it + RING + L2AHEAD <= rlast) ring_prefetch(rfirst + it + RING + L2AHEAD);
             }
             if (it + NSTAGE < n) {
                 if (!mbar_wait(&bar[2 * RING + NSTAGE + it % NSTAGE], (it / NSTAGE) & 1)) {
@@ -420,7 +421,7 @@ __global__ void __launch_bounds__(NTHR, 3) k_velocity_tma(const __grid_constant_
                     return;
                 }
                 stage_load(it + NSTAGE);
-                if (it + NSTAGE + L2AHEAD < n) stage_prefetch(it + NSTAGE + L2AHEAD);
+                if (L2AHEAD > 0 && it + NSTAGE + L2AHEAD < n) stage_prefetch(it + NSTAGE + L2AHEAD);
             }
         }
         return;
@@ -507,7 +508,7 @@ __global__ void __maxnreg__(L == 0 ? IFOSB_STR_MAXNREG_ELASTIC : IFOSB_STR_MAXNR
             if (rfirst + it + RING <= rlast) {
                 if (!mbar_wait(&bar[RING + it % RING], (it / RING) & 1)) { atomicExch(T.tma_err, 1); return; }
                 ring_load(rfirst + it + RING);
-                if (rfirst + it + RING + L2AHEAD <= rlast) ring_prefetch(rfirst + it + RING + L2AHEAD);
+                if (L2AHEAD > 0 && rfirst + it + RING + L2AHEAD <= rlast) ring_prefetch(rfirst + it + RING + L2AHEAD);
             }
             if (it + NSTAGE < n) {
                 if (!mbar_wait(&bar[2 * RING + NSTAGE + it % NSTAGE], (it / NSTAGE) & 1)) {
@@ -515,7 +516,7 @@ __global__ void __maxnreg__(L == 0 ? IFOSB_STR_MAXNREG_ELASTIC : IFOSB_STR_MAXNR
                     return;
                 }
                 stage_load(it + NSTAGE);
-                if (it + NSTAGE + L2AHEAD < n) stage_prefetch(it + NSTAGE + L2AHEAD);
+                if (L2AHEAD > 0 && it + NSTAGE + L2AHEAD < n) stage_prefetch(it + NSTAGE + L2AHEAD);
             }
         }
         return;
