@@ -224,7 +224,8 @@ def workload_config(wl, world):
     return {"workload": "elastic128: elastic FWI shot-gradient (forward+residual+adjoint+DFT gradient), 128^3, "
                         "NT=2000, 2 frequencies, 25 receivers, 1 shot per GPU",
             "grid": [128, 128, 128], "nt": 2000, "nmech": 0, "nf": 2, "shots_per_gpu": 1, "receivers": 25,
-            "parallelism": f"shot-sharded x{world}", "l2_flush": "state+DFT 0.37 GB per shot > 126 MB L2"}
+            "parallelism": f"shot-sharded x{world}" + (", FP64 gradient all-reduce per step" if world > 1 else ""),
+            "l2_flush": "state+DFT 0.37 GB per shot > 126 MB L2"}
 
 
 def main():
@@ -281,8 +282,19 @@ def main():
         obs = eng.forward(shots)
         eng.set_model(m["rho"], m["pi"], m["u"], m["taus"], m["taup"], m["eta"])
 
+    if wl == "elastic128" and dist:
+        # N ranks: one shot each, then the exchange step of a gradient iteration, the
+        # FP64 all-reduce of the gradient and misfits (ifosb.dist); the entries of the
+        # other ranks' shots are placeholders (each rank computes only its own)
+        from ifosb.dist import distributed_shot_gradient
+        all_shots = [shots[0]] * world
+        all_obs = np.zeros((world,) + obs.shape[1:], np.float32)
+        all_obs[rank] = obs[0]
+
     def step():
-        if wl == "elastic128":
+        if wl == "elastic128" and dist:
+            distributed_shot_gradient(eng, all_shots, all_obs, max_batch=1, dist=dist)
+        elif wl == "elastic128":
             eng.shot_gradient(shots, obs)
         else:
             eng.forward(shots, want_sections=False)
