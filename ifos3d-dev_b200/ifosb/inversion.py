@@ -1,0 +1,150 @@
+"""The reference driver's inversion iteration on the engine and the device optimiser.
+
+One iteration of src/ifos3d.c:669-1148, in its order:
+  constant_boundary (FREE_SURF) and the averaged model            :681-683
+  frequency-stage bookkeeping: cdf = 1 on a stage's first iteration :690-701
+  shot gradients: forward, residual, adjoint, gradient_F per shot   :712-975
+  precon_grad, then lbfgs / lbfgs_savegrad or conjugate             :1005-1015
+  two test steps: modelupdate on a copy, forwards of NSHOTS_STEP
+  shots, misfits                                                   :1021-1129
+  steplength (parabola), modelupdate of the model                   :1133-1138
+The differences are the ones the engine makes everywhere: shots run in batches,
+misfits are summed in FP64, and the optimiser's dot products and the step-length
+parabola are FP64. Models are the ghosted [NY+2][NX+2][NZ+2] rho, pi, u arrays of
+the reference; their ghost layers are refreshed by the engine (matcopy's wrap).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import Engine, Optimizer, Params, steplength
+
+
+@dataclass
+class Stage:
+    finv: list                     # DFT frequencies of the stage (readinv)
+    itmax: int                     # iterations of the stage (itpergroup[1])
+
+
+@dataclass
+class Settings:
+    teststep: float = 0.02         # TESTSTEP
+    weight: tuple = (1.0, 1.0, 1.0)  # WEIGHT[3]
+    vp0: float = 3000.0            # VP0, VS0, RHO0
+    vs0: float = 1732.0
+    rho0: float = 2000.0
+    damptype: int = 2              # DAMPTYPE
+    lbfgs: bool = False            # LBFGS
+    numpar: int = 1                # NUMPAR
+    bfgsnum: int = 3               # BFGSNUM
+    nshots_step: int = 1           # NSHOTS_STEP (shots of the step-length test forwards)
+    tast: int = 100                # TAST (DFT sampling: ntast = 1 / (f_max TAST DT))
+    max_batch: int = 4             # shots per engine launch
+
+
+@dataclass
+class History:
+    misfit: list = field(default_factory=list)   # misfit[0] of every iteration (FP64)
+    step: list = field(default_factory=list)     # the accepted step[3]
+    beta: list = field(default_factory=list)
+
+
+class Inversion:
+    def __init__(self, p: Params, cpml, recpos, shots, obs, srcpos_m, rho, pi, u, stages, cfg: Settings):
+        self.p, self.cfg, self.stages = p, cfg, list(stages)
+        self.shots, self.obs = list(shots), np.ascontiguousarray(obs, np.float32)
+        self.recpos = np.ascontiguousarray(recpos, np.int32)
+        self.srcpos_m = np.ascontiguousarray(srcpos_m, np.float32)
+        self.model = [np.ascontiguousarray(a, np.float32).copy() for a in (rho, pi, u)]
+        nf_max = max(len(s.finv) for s in self.stages)
+        self.eng = Engine(p, max_shots=min(cfg.max_batch, len(self.shots)), max_nf=nf_max)
+        self.eng.set_cpml(cpml)
+        self.eng.set_receivers(self.recpos)
+        self.opt = Optimizer(p.nx, p.ny, p.nz, numpar=cfg.numpar, bfgsnum=cfg.bfgsnum if cfg.lbfgs else 0)
+        self.step = np.zeros(5, np.float64)    # step[0..4] (vector(0,4): zeros)
+        self.stage_i, self.it_group, self.itmax, self.iteration = -1, 0, 0, 0
+        self.hist = History()
+
+    # -- helpers --------------------------------------------------------------
+    def _set_model(self, m):
+        self.eng.set_model(*(a[1:-1, 1:-1, 1:-1] for a in m), None, None, None)
+
+    def _batches(self, idx):
+        b = self.cfg.max_batch
+        return [idx[i:i + b] for i in range(0, len(idx), b)]
+
+    def _test_shots(self):
+        n, k = len(self.shots), self.cfg.nshots_step
+        return [(n // k) * q for q in range(k)]  # ishot1 = (nshots/NSHOTS_STEP)*(ishot-1)+1
+
+    def _forward_misfit(self, m):
+        self._set_model(m)
+        total = 0.0
+        for chunk in self._batches(self._test_shots()):
+            self.eng.forward([self.shots[i] for i in chunk], want_sections=False)
+            total += float(np.sum(self.eng.residual(self.obs[chunk])))
+        return total
+
+    # -- one iteration ----------------------------------------------------------
+    def iterate(self):
+        p, cfg = self.p, self.cfg
+        self.iteration += 1
+        if p.free_surf:
+            self.opt.constant_boundary(*self.model, p.fw)
+        if self.it_group >= self.itmax or self.iteration == 1:  # next frequency stage
+            self.stage_i += 1
+            st = self.stages[self.stage_i]
+            self.finv = np.asarray(st.finv, np.float32)
+            ntast = int(1.0 / (float(self.finv[-1]) * cfg.tast * p.dt)) or 1
+            self.eng.set_frequencies(self.finv, ntast)
+            cdf, self.itmax, self.it_group = 1, st.itmax, 1
+        else:
+            cdf = 0
+            self.it_group += 1
+        # shot gradients and misfit[0] over the NSHOTS_STEP shots
+        self._set_model(self.model)
+        self.eng.zero_gradient()
+        mis = np.zeros(len(self.shots))
+        for chunk in self._batches(list(range(len(self.shots)))):
+            mis[chunk] = self.eng.shot_gradient([self.shots[i] for i in chunk], self.obs[chunk])
+        L2 = np.zeros(4, np.float64)
+        L2[0] = float(np.sum(mis[self._test_shots()]))
+        g = self.eng.get_gradient()
+        self.opt.precon_grad(g, cfg.damptype, p.free_surf, p.fw, (p.dx, p.dy, p.dz), self.srcpos_m, self.recpos)
+        beta = None
+        if cfg.lbfgs:
+            if self.it_group > 1:
+                self.opt.lbfgs(g, self.it_group)
+            else:
+                self.opt.lbfgs_savegrad(g)
+        else:
+            beta = self.opt.conjugate(g, cdf)
+        # step length: two test models
+        for steptest in (1, 2):
+            if cdf == 1:
+                self.step[4] = cfg.teststep
+            self.step[steptest] = self.step[4] * steptest
+            test = [a.copy() for a in self.model]
+            self.opt.modelupdate(g, *test, self.step[steptest], cfg.weight, cfg.vp0, cfg.vs0, cfg.rho0,
+                                 lbfgs=cfg.lbfgs, it_group=self.it_group)
+            if p.free_surf:
+                self.opt.constant_boundary(*test, p.fw)
+            L2[steptest] = self._forward_misfit(test)
+        steplength(L2, self.step, cfg.lbfgs, self.it_group, cfg.teststep)
+        self.opt.modelupdate(g, *self.model, self.step[3], cfg.weight, cfg.vp0, cfg.vs0, cfg.rho0,
+                             lbfgs=cfg.lbfgs, it_group=self.it_group)
+        self.hist.misfit.append(L2[0])
+        self.hist.step.append(float(self.step[3]))
+        self.hist.beta.append(None if beta is None else beta.tolist())
+        return L2[0]
+
+    def run(self, iterations: int):
+        for _ in range(iterations):
+            self.iterate()
+        return self.hist
+
+    def close(self):
+        self.eng.close()
+        self.opt.close()

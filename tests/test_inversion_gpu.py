@@ -1,0 +1,84 @@
+"""The reference driver's inversion iteration (ifosb.inversion: shot gradients,
+precon_grad, conjugate / L-BFGS, two test forwards, the step-length parabola,
+modelupdate) on a small elastic problem: with CG the FP64 misfit falls at every
+iteration (by 7 % over the first three updates). Over so few iterations the
+update is not yet aligned with the true anomaly, so no model-error claim is made."""
+import math
+
+import numpy as np
+import pytest
+
+import ifosb
+from ifosb import synth
+from ifosb.inversion import Inversion, Settings, Stage
+
+pytestmark = pytest.mark.gpu
+
+NX, NY, NZ, FW, NT, FC = 44, 40, 40, 6, 300, 300.0
+
+
+def _problem(free_surf):
+    p = ifosb.make_params(NX, NY, NZ, dh=1.0, dt=1e-4, nt=NT, fdcoeff=2, free_surf=free_surf, fw=FW, nmech=0)
+    jj, ii, kk = np.meshgrid(np.arange(1, NY + 1), np.arange(1, NX + 1), np.arange(1, NZ + 1), indexing="ij")
+    blob = np.exp(-((jj - 22) ** 2 + (ii - 22) ** 2 + (kk - 20) ** 2) / (2 * 4.0 ** 2)).astype(np.float32)
+    vp0 = np.full((NY, NX, NZ), 3000.0, np.float32)
+    vpT = (vp0 * (1 + 0.08 * blob)).astype(np.float32)
+    rho = np.full_like(vp0, 2000.0)
+    src = [synth._src(x, FW + 3, z, FC) for x, z in ((12, 12), (32, 12), (12, 28), (32, 28))]
+    shots = [(sp, ifosb.wavelet(p, 4, sp)) for sp in src]
+    rec = synth._grid_receivers(NX, NZ, 6, FW + 2, FW + 3)
+    cp = ifosb.cpml_coeff(p, 3000.0, FC)
+    e = ifosb.Engine(p, max_shots=len(shots), max_nf=0)
+    e.set_cpml(cp)
+    e.set_receivers(rec)
+    mT = ifosb.moduli(p, vpT.ravel(), (vpT / np.float32(math.sqrt(3))).ravel(), rho.ravel())
+    e.set_model(*(mT[k].reshape(NY, NX, NZ) for k in ("rho", "pi", "u")), None, None, None)
+    obs = e.forward(shots)
+    e.close()
+    m0 = ifosb.moduli(p, vp0.ravel(), (vp0 / np.float32(math.sqrt(3))).ravel(), rho.ravel())
+    ghost = [ifosb.ghost_wrap(m0[k].reshape(NY, NX, NZ)) for k in ("rho", "pi", "u")]
+    srcpos_m = np.array([[s[0][0, 0], s[0][0, 1], s[0][0, 2]] for s in shots], np.float32)  # DH = 1 m
+    return p, cp, rec, shots, obs, srcpos_m, ghost, vp0, vpT
+
+
+def test_inversion_reduces_misfit():
+    p, cp, rec, shots, obs, srcpos_m, ghost, vp0, vpT = _problem(free_surf=0)
+    cfg = Settings(teststep=0.02, damptype=2, lbfgs=False, nshots_step=4, max_batch=4, weight=(1.0, 0.0, 0.0))
+    inv = Inversion(p, cp, rec, shots, obs, srcpos_m, *ghost, [Stage([300.0, 450.0, 600.0], 4)], cfg)
+    hist = inv.run(4)
+    rho, pi, u = inv.model
+    vp = np.sqrt((pi / rho)[1:-1, 1:-1, 1:-1].astype(np.float64)).astype(np.float32)
+    inv.close()
+    assert all(np.isfinite(hist.misfit)) and all(s > 0 for s in hist.step)
+    assert all(b < a for a, b in zip(hist.misfit, hist.misfit[1:])), hist.misfit  # falls every iteration
+    assert hist.misfit[-1] < 0.95 * hist.misfit[0], hist.misfit
+    assert np.any(vp != vp0)
+
+
+def test_lbfgs_iterations_run():
+    """L-BFGS as the reference runs it: its first update uses the raw gradient
+    (modelupdate normalises only without L-BFGS), so on this problem the steps are
+    tiny; the check is that the iterations run, stay finite and fill the history."""
+    p, cp, rec, shots, obs, srcpos_m, ghost, vp0, vpT = _problem(free_surf=0)
+    cfg = Settings(teststep=0.02, damptype=2, lbfgs=True, numpar=1, bfgsnum=3, nshots_step=2, max_batch=4)
+    inv = Inversion(p, cp, rec, shots, obs, srcpos_m, *ghost, [Stage([300.0, 450.0], 3)], cfg)
+    hist = inv.run(3)
+    s_hist, y_hist, scale = inv.opt.history()
+    inv.close()
+    assert all(np.isfinite(hist.misfit)) and all(np.isfinite(hist.step))
+    assert np.any(y_hist[0] != 0) and np.any(s_hist != 0)
+
+
+def test_free_surface_with_reference_damping_leaves_the_model():
+    """With FREE_SURF, precon_grad's top factor is 0 for damping types 0-2 (the
+    reference's behaviour): the gradient vanishes; inside the frame that
+    constant_boundary rewrites, the model changes only by the rounding of the
+    vp -> pi round trip of modelupdate."""
+    p, cp, rec, shots, obs, srcpos_m, ghost, vp0, vpT = _problem(free_surf=1)
+    cfg = Settings(teststep=0.01, damptype=2, nshots_step=2, max_batch=4)
+    inv = Inversion(p, cp, rec, shots, obs, srcpos_m, *ghost, [Stage([300.0, 450.0], 2)], cfg)
+    inv.run(1)
+    rho, pi, u = inv.model
+    inner = (slice(2, NY - 1), slice(FW + 6, NX - FW - 4), slice(FW + 6, NZ - FW - 4))
+    np.testing.assert_allclose(pi[inner], ghost[1][inner], rtol=1e-6, atol=0)
+    inv.close()
