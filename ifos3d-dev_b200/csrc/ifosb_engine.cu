@@ -17,6 +17,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -80,6 +81,10 @@ struct ifosb_engine {
     int t_steps = 0;
     std::vector<cudaEvent_t> events;
     cudaStream_t own_stream = nullptr;
+    // launch shapes picked by ifosb_autotune per batch size: y planes per CTA chunk
+    // and the L2 prefetch distance; nt_limit > 0 shortens the time loop while tuning
+    std::map<int, std::pair<int, int>> tuned;
+    int nt_limit = 0;
     // TMA staging (default) and its wait-timeout flag
     int use_tma = 1;
     int *d_tma_err = nullptr;
@@ -495,6 +500,12 @@ struct Loop {
 // about four CTAs per SM in flight over the whole batch.
 static Geo launch_geo(const ifosb_engine *e, int nshots) {
     Geo g = e->g;
+    auto t = e->tuned.find(nshots);
+    if (t != e->tuned.end()) {
+        g.cy = t->second.first;
+        g.nyc = (g.ny + g.cy - 1) / g.cy;
+        return g;
+    }
     int dev = 0, sms = 148;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaGetLastError();
@@ -631,6 +642,10 @@ static bool setup_tma(ifosb_engine *e, Loop &L, float *dft) {
     L.vt.a = L.va;
     L.stt.a = L.sa;
     L.vt.tma_err = L.stt.tma_err = e->d_tma_err;
+    {
+        auto t = e->tuned.find(L.nshots);
+        L.vt.l2ahead = L.stt.l2ahead = t != e->tuned.end() ? t->second.second : L2AHEAD_DEFAULT;
+    }
     L.stt.nsr = nsr;
     L.stt.nm = nm;
     L.stt.ndf = ndf;
@@ -713,7 +728,8 @@ static void enqueue_loop(ifosb_engine *e, const Loop &L) {
 // Kernel-by-kernel launches with an event pair around each kernel (kernel timing).
 static int run_loop_profiled(ifosb_engine *e, const Loop &L) {
     const ifosb_params &p = e->p;
-    const size_t need = (size_t)3 * p.nt;
+    const int nsteps = e->nt_limit > 0 ? std::min(e->nt_limit, p.nt) : p.nt;  // the autotuner times a few steps
+    const size_t need = (size_t)3 * nsteps;
     while (e->events.size() < need) {
         cudaEvent_t ev;
         CU(cudaEventCreate(&ev));
@@ -721,7 +737,7 @@ static int run_loop_profiled(ifosb_engine *e, const Loop &L) {
     }
     dim3 grd(L.lg.ntk, L.lg.nti, L.lg.nyc * L.nshots);
     int lsamp = p.ndtshift + 1, nlsamp = 0;
-    for (int nt = 1; nt <= p.nt; ++nt) {
+    for (int nt = 1; nt <= nsteps; ++nt) {
         cudaEvent_t *ev = &e->events[(size_t)3 * (nt - 1)];
         CU(cudaEventRecord(ev[0], e->stream));
         launch_vel(L, grd, e->stream, nt);
@@ -735,7 +751,7 @@ static int run_loop_profiled(ifosb_engine *e, const Loop &L) {
     if (rc) return rc;
     CU(cudaStreamSynchronize(e->stream));
     double tv = 0.0, ts = 0.0;
-    for (int nt = 1; nt <= p.nt; ++nt) {
+    for (int nt = 1; nt <= nsteps; ++nt) {
         cudaEvent_t *ev = &e->events[(size_t)3 * (nt - 1)];
         float a = 0.f, b = 0.f;
         CU(cudaEventElapsedTime(&a, ev[0], ev[1]));
@@ -745,7 +761,7 @@ static int run_loop_profiled(ifosb_engine *e, const Loop &L) {
     }
     e->t_vel_ms = tv;
     e->t_str_ms = ts;
-    e->t_steps = p.nt;
+    e->t_steps = nsteps;
     return IFOSB_OK;
 }
 
@@ -1064,4 +1080,49 @@ extern "C" int ifosb_residual_noalloc(int nshots, int ntr, int ns, float dt, con
     k_residual<<<(nthr + 127) / 128, 128, 0, s>>>(d_syn, d_obs, d_diff, part, nshots, ntr, ns, dt);
     k_misfit<<<nshots, 32, 0, s>>>(part, d_misfit, 3 * ntr);
     return cudaGetLastError() == cudaSuccess ? IFOSB_OK : IFOSB_ECUDA;
+}
+
+// Autotuner: for a batch of nshots shots, times `steps` forward time steps
+// (kernel-by-kernel, CUDA events) for each launch shape — y planes per CTA chunk
+// and the L2 prefetch distance of the TMA kernels — and keeps the fastest for
+// later calls with that batch size. The shape changes no arithmetic: results
+// stay bit-identical. The wavefield of the batch is left undefined.
+extern "C" int ifosb_autotune(ifosb_engine *e, int nshots, const ifosb_shot *shots, int steps, int *cy_out,
+                              int *l2_out) {
+    if (!e || !shots || nshots < 1 || nshots > e->max_shots || steps < 1) return IFOSB_EARG;
+    const int saved_profile = e->profile;
+    e->tuned.erase(nshots);
+    const Geo h = launch_geo(e, nshots);  // the heuristic shape is a candidate too
+    std::vector<int> cys = {8, 16, 32, 64, h.cy};
+    double best = 1e30;
+    std::pair<int, int> pick(h.cy, L2AHEAD_DEFAULT);
+    int rc = IFOSB_OK;
+    e->profile = 1;
+    e->nt_limit = steps;
+    for (int cy : cys) {
+        if (cy > e->p.ny || (long long)((e->p.ny + cy - 1) / cy) * nshots > 65535) continue;
+        for (int l2 : {0, 1, 3}) {
+            e->tuned[nshots] = {cy, l2};
+            if ((rc = ifosb_forward(e, nshots, shots, nullptr))) break;
+            const double ms = e->t_vel_ms + e->t_str_ms;
+            if (ms < best) {
+                best = ms;
+                pick = {cy, l2};
+            }
+        }
+        if (rc) break;
+    }
+    e->nt_limit = 0;
+    e->profile = saved_profile;
+    e->fwd_ok = e->res_ok = e->adj_ok = false;
+    if (rc) {
+        e->tuned.erase(nshots);
+        return rc;
+    }
+    e->tuned[nshots] = pick;
+    release_graph(e->gfwd);
+    release_graph(e->gadj);
+    if (cy_out) *cy_out = pick.first;
+    if (l2_out) *l2_out = pick.second;
+    return IFOSB_OK;
 }

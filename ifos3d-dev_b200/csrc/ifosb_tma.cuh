@@ -134,12 +134,9 @@ __device__ __forceinline__ void tma_prefetch4(const CUtensorMap *m, int c0, int 
                  : "memory");
 }
 
-// Planes are prefetched into L2 this many iterations before their shared-memory load
-// (0: no L2 prefetch).
-#ifndef IFOSB_L2_AHEAD
-#define IFOSB_L2_AHEAD 3
-#endif
-constexpr int L2AHEAD = IFOSB_L2_AHEAD;
+// Planes are prefetched into L2 `l2ahead` iterations before their shared-memory
+// load (a launch argument, 0 = no L2 prefetch; the engine's autotuner picks it).
+constexpr int L2AHEAD_DEFAULT = 3;
 
 // Tensor-map coordinates of a cell: z index k+7, row i+1, plane j+2.
 __device__ __forceinline__ int zc(int k) { return k + 7; }
@@ -152,6 +149,7 @@ struct VelTma {
     CUtensorMap m_mod;   // model, box {TZ, TX, 1, 3}
     VelArgs a;
     int *tma_err;
+    int l2ahead;
 };
 
 struct StrTma {
@@ -164,6 +162,7 @@ struct StrTma {
     float utaus, utaup, uts_avg;  // uniform taus, taup and their staggered averages (nm == 5)
     float idx, idy, idz;          // exact 1/DX, 1/DY, 1/DZ (power-of-two spacings)
     int *tma_err;
+    int l2ahead;
 };
 
 __host__ __device__ constexpr size_t vel_tma_smem() {
@@ -405,7 +404,7 @@ __global__ void __launch_bounds__(NTHR, 3) k_velocity_tma(const __grid_constant_
         auto ring_prefetch = [&](int P) { tma_prefetch5(&T.m_halo, zc(k0) - HZ, xc(i0) - HX, yc_(P), SYY, s); };
         for (int P = rfirst; P <= min(rfirst + RING - 1, rlast); ++P) ring_load(P);
         for (int it = 0; it < NSTAGE && it < n; ++it) stage_load(it);
-        for (int q = 0; q < L2AHEAD; ++q) {
+        for (int q = 0; q < T.l2ahead; ++q) {
             if (NSTAGE + q < n) stage_prefetch(NSTAGE + q);
             if (rfirst + RING + q <= rlast) ring_prefetch(rfirst + RING + q);
         }
@@ -413,7 +412,7 @@ __global__ void __launch_bounds__(NTHR, 3) k_velocity_tma(const __grid_constant_
             if (rfirst + it + RING <= rlast) {
                 if (!mbar_wait(&bar[RING + it % RING], (it / RING) & 1)) { atomicExch(T.tma_err, 1); return; }
                 ring_load(rfirst + it + RING);
-                if (L2AHEAD > 0 && rfirst + it + RING + L2AHEAD <= rlast) ring_prefetch(rfirst + it + RING + L2AHEAD);
+                if (T.l2ahead > 0 && rfirst + it + RING + T.l2ahead <= rlast) ring_prefetch(rfirst + it + RING + T.l2ahead);
             }
             if (it + NSTAGE < n) {
                 if (!mbar_wait(&bar[2 * RING + NSTAGE + it % NSTAGE], (it / NSTAGE) & 1)) {
@@ -421,7 +420,7 @@ __global__ void __launch_bounds__(NTHR, 3) k_velocity_tma(const __grid_constant_
                     return;
                 }
                 stage_load(it + NSTAGE);
-                if (L2AHEAD > 0 && it + NSTAGE + L2AHEAD < n) stage_prefetch(it + NSTAGE + L2AHEAD);
+                if (T.l2ahead > 0 && it + NSTAGE + T.l2ahead < n) stage_prefetch(it + NSTAGE + T.l2ahead);
             }
         }
         return;
@@ -500,7 +499,7 @@ __global__ void __maxnreg__(L == 0 ? IFOSB_STR_MAXNREG_ELASTIC : IFOSB_STR_MAXNR
         auto ring_prefetch = [&](int P) { tma_prefetch5(&T.m_halo, zc(k0) - HZ, xc(i0) - HX, yc_(P), VX, s); };
         for (int P = rfirst; P <= min(rfirst + RING - 1, rlast); ++P) ring_load(P);
         for (int it = 0; it < NSTAGE && it < n; ++it) stage_load(it);
-        for (int q = 0; q < L2AHEAD; ++q) {
+        for (int q = 0; q < T.l2ahead; ++q) {
             if (NSTAGE + q < n) stage_prefetch(NSTAGE + q);
             if (rfirst + RING + q <= rlast) ring_prefetch(rfirst + RING + q);
         }
@@ -508,7 +507,7 @@ __global__ void __maxnreg__(L == 0 ? IFOSB_STR_MAXNREG_ELASTIC : IFOSB_STR_MAXNR
             if (rfirst + it + RING <= rlast) {
                 if (!mbar_wait(&bar[RING + it % RING], (it / RING) & 1)) { atomicExch(T.tma_err, 1); return; }
                 ring_load(rfirst + it + RING);
-                if (L2AHEAD > 0 && rfirst + it + RING + L2AHEAD <= rlast) ring_prefetch(rfirst + it + RING + L2AHEAD);
+                if (T.l2ahead > 0 && rfirst + it + RING + T.l2ahead <= rlast) ring_prefetch(rfirst + it + RING + T.l2ahead);
             }
             if (it + NSTAGE < n) {
                 if (!mbar_wait(&bar[2 * RING + NSTAGE + it % NSTAGE], (it / NSTAGE) & 1)) {
@@ -516,7 +515,7 @@ __global__ void __maxnreg__(L == 0 ? IFOSB_STR_MAXNREG_ELASTIC : IFOSB_STR_MAXNR
                     return;
                 }
                 stage_load(it + NSTAGE);
-                if (L2AHEAD > 0 && it + NSTAGE + L2AHEAD < n) stage_prefetch(it + NSTAGE + L2AHEAD);
+                if (T.l2ahead > 0 && it + NSTAGE + T.l2ahead < n) stage_prefetch(it + NSTAGE + T.l2ahead);
             }
         }
         return;

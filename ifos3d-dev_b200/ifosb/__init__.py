@@ -92,6 +92,7 @@ def lib():
             "ifosb_set_profiling": (C.c_int, [vp, C.c_int]),
             "ifosb_kernel_times": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int)]),
             "ifosb_set_stream": (C.c_int, [vp, vp]),
+            "ifosb_autotune": (C.c_int, [vp, C.c_int, C.POINTER(Shot), C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
             "ifosb_residual_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_float, vp, vp, vp, vp, vp]),
             "ifosb_optim_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(vp)]),
             "ifosb_optim_destroy": (None, [vp]),
@@ -123,7 +124,7 @@ def exported_symbols():
         "ifosb_adjoint", "ifosb_gradient", "ifosb_zero_gradient", "ifosb_get_gradient", "ifosb_shot_gradient",
         "ifosb_get_field", "ifosb_set_launch_mode", "ifosb_last_launch_count", "ifosb_cpml_coeff",
         "ifosb_wavelet", "ifosb_nsamples", "ifosb_moduli", "ifosb_set_profiling", "ifosb_kernel_times",
-        "ifosb_set_stream", "ifosb_residual_noalloc", "ifosb_optim_create", "ifosb_optim_destroy",
+        "ifosb_set_stream", "ifosb_autotune", "ifosb_residual_noalloc", "ifosb_optim_create", "ifosb_optim_destroy",
         "ifosb_optim_last_error", "ifosb_conjugate", "ifosb_lbfgs_savegrad", "ifosb_lbfgs", "ifosb_modelupdate",
         "ifosb_lbfgs_history", "ifosb_steplength", "ifosb_precon_grad", "ifosb_constant_boundary",
     ]
@@ -291,6 +292,13 @@ class Engine:
         out = np.zeros((len(shots), 3, self.ntr, self.ns), np.float32) if (want_sections and self.ntr) else None
         self._c(lib().ifosb_forward(self.h, len(shots), arr, _p(out)))
         return out
+
+    def autotune(self, shots, steps=20):
+        """Pick the launch shape for batches of len(shots) shots; returns (cy, l2ahead)."""
+        arr, keep = self._shots(shots)
+        cy, l2 = C.c_int(), C.c_int()
+        self._c(lib().ifosb_autotune(self.h, len(shots), arr, steps, C.byref(cy), C.byref(l2)))
+        return cy.value, l2.value
 
     def residual(self, obs, want_l2_ref=False):
         obs = _f32(obs)

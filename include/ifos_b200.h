@@ -160,6 +160,15 @@ long long ifosb_last_launch_count(const ifosb_engine *e);
 int ifosb_set_profiling(ifosb_engine *e, int profile);
 int ifosb_kernel_times(const ifosb_engine *e, double *vel_ms, double *str_ms, int *steps);
 
+/* Autotuner: times `steps` forward time steps of this batch (the same shots a
+ * later ifosb_forward / ifosb_shot_gradient will use) for each launch shape —
+ * y planes per CTA chunk (8, 16, 32, 64 and the built-in choice) and the L2
+ * prefetch distance of the TMA kernels (0, 1, 3 planes) — and keeps the fastest
+ * for every later call with nshots shots. Results do not depend on the shape
+ * (bit-identical). The batch's wavefield is undefined afterwards. cy_out, l2_out
+ * (optional) get the choice. */
+int ifosb_autotune(ifosb_engine *e, int nshots, const ifosb_shot *shots, int steps, int *cy_out, int *l2_out);
+
 /* Run the engine's work on the caller's CUDA stream (a cudaStream_t passed as
  * void*; NULL = the engine's own stream). Calls stay synchronous at return. */
 int ifosb_set_stream(ifosb_engine *e, void *stream);

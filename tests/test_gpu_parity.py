@@ -186,3 +186,24 @@ def test_call_order_errors():
     with pytest.raises(ifosb.IfosbError) as ei:
         e.forward(bad)
     assert ei.value.code == ifosb.EARG
+
+
+def test_autotuned_launch_shape_gives_the_same_bits():
+    """ifosb_autotune picks a launch shape (y planes per CTA chunk, L2 prefetch
+    distance); forward traces and the shot gradient are the same bits as with
+    the built-in shape."""
+    c = synth.small_case(nx=37, ny=70, nz=45, nt=40, fw=6, nshots=3, seed=17)
+    e1, m, cp, shots = engine_for(c)
+    e2, _, _, _ = engine_for(c)
+    cy, l2 = e2.autotune(shots, steps=4)
+    assert cy in (8, 16, 32, 64) or 8 <= cy <= 64
+    assert l2 in (0, 1, 3)
+    out = []
+    for e in (e1, e2):
+        sec = e.forward(shots)
+        obs = (sec * np.float32(0.9)).astype(np.float32)
+        mis = e.shot_gradient(shots, obs)
+        out.append((sec, mis, e.get_gradient()))
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
+    assert np.array_equal(out[0][2], out[1][2])
