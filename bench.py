@@ -442,6 +442,8 @@ def shot_gradient_comparison(torch, ifosb, synth, dev, stream, nt_override, nsho
         e.set_cpml(cp)
         e.set_receivers(c["recpos"])
         e.set_frequencies(c["finv"], c["ntast"])
+        e.set_model(m["rho"], m["pi"], m["u"], m["taus"], m["taup"], m["eta"])
+        e.autotune(shots[:nb], steps=20)  # each path with its own best launch shape
         return e
 
     eb = make(nshots, 0)

@@ -1093,7 +1093,9 @@ extern "C" int ifosb_autotune(ifosb_engine *e, int nshots, const ifosb_shot *sho
     const int saved_profile = e->profile;
     e->tuned.erase(nshots);
     const Geo h = launch_geo(e, nshots);  // the heuristic shape is a candidate too
-    std::vector<int> cys = {8, 16, 32, 64, h.cy};
+    std::vector<int> cys = {2, 3, 4, 6, 8, 12, 16, 24, 32, 64, h.cy};
+    std::sort(cys.begin(), cys.end());
+    cys.erase(std::unique(cys.begin(), cys.end()), cys.end());
     double best = 1e30;
     std::pair<int, int> pick(h.cy, L2AHEAD_DEFAULT);
     int rc = IFOSB_OK;
@@ -1101,7 +1103,7 @@ extern "C" int ifosb_autotune(ifosb_engine *e, int nshots, const ifosb_shot *sho
     e->nt_limit = steps;
     for (int cy : cys) {
         if (cy > e->p.ny || (long long)((e->p.ny + cy - 1) / cy) * nshots > 65535) continue;
-        for (int l2 : {0, 1, 3}) {
+        for (int l2 : {0, 1, 2, 3}) {
             e->tuned[nshots] = {cy, l2};
             if ((rc = ifosb_forward(e, nshots, shots, nullptr))) break;
             const double ms = e->t_vel_ms + e->t_str_ms;

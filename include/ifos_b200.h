@@ -162,8 +162,8 @@ int ifosb_kernel_times(const ifosb_engine *e, double *vel_ms, double *str_ms, in
 
 /* Autotuner: times `steps` forward time steps of this batch (the same shots a
  * later ifosb_forward / ifosb_shot_gradient will use) for each launch shape —
- * y planes per CTA chunk (8, 16, 32, 64 and the built-in choice) and the L2
- * prefetch distance of the TMA kernels (0, 1, 3 planes) — and keeps the fastest
+ * y planes per CTA chunk (2 to 64, and the built-in choice) and
+ * the L2 prefetch distance of the TMA kernels (0-3 planes) — and keeps the fastest
  * for every later call with nshots shots. Results do not depend on the shape
  * (bit-identical). The batch's wavefield is undefined afterwards. cy_out, l2_out
  * (optional) get the choice. */
