@@ -167,7 +167,7 @@ static int check_launch(ifosb_engine *e, const char *what) {
 }
 
 static int block_of(const Geo &g, int j, int i, int k) {
-    const int bx = (k - 1) / BX, by = (i - 1) / BY, yc = (j - 1) / g.cy;
+    const int bx = (k - 1) / BX, by = (i - 1) / g.by, yc = (j - 1) / g.cy;
     return (yc * g.nti + by) * g.ntk + bx;
 }
 
@@ -231,8 +231,19 @@ extern "C" int ifosb_create(const ifosb_params *p, int max_shots, int max_nf, if
     g.field = (long long)(p->ny + 5) * g.plane;
     g.cy = DEFAULT_CY;
     g.nyc = (p->ny + g.cy - 1) / g.cy;
+    {
+        const char *v = getenv("IFOSB_TMA");
+        if (v && v[0] == '0') e->use_tma = 0;
+    }
+    // tile rows: 7 (8-warp CTAs, two per SM) when the stress kernel carries memory
+    // variables, else 8; IFOSB_TILE_ROWS=7|8 overrides (tests, tuning experiments)
+    g.by = (e->use_tma && p->nmech > 0) ? 7 : 8;
+    if (const char *v = getenv("IFOSB_TILE_ROWS")) {
+        const int t = atoi(v);
+        if (t == 7 || t == 8) g.by = t;
+    }
     g.ntk = (p->nz + BX - 1) / BX;
-    g.nti = (p->nx + BY - 1) / BY;
+    g.nti = (p->nx + g.by - 1) / g.by;
     if ((long long)g.nyc * max_shots > 65535) { delete e; return IFOSB_EARG; }
     e->sl.sx = (long long)p->ny * 2 * p->fw * p->nz;
     e->sl.sy = (long long)2 * p->fw * p->nx * p->nz;
@@ -257,10 +268,6 @@ extern "C" int ifosb_create(const ifosb_params *p, int max_shots, int max_nf, if
         (rc = dalloc(e, &e->d_err, (size_t)max_shots)) || (rc = dalloc(e, &e->d_tma_err, 1))) {
         ifosb_destroy(e);
         return rc;
-    }
-    {
-        const char *v = getenv("IFOSB_TMA");
-        if (v && v[0] == '0') e->use_tma = 0;
     }
     if (max_nf > 0) {
         if ((rc = dalloc(e, &e->d_dftf, (size_t)(e->dft_shot * max_shots))) ||
@@ -480,7 +487,7 @@ extern "C" int ifosb_set_frequencies(ifosb_engine *e, int nf, const float *finv,
 // ---------------------------------------------------------------------------
 // the time loop
 
-static_assert(TZ == BX && TX == BY, "TMA tiles and plain blocks share one block geometry");
+static_assert(TZ == BX, "TMA tiles and plain blocks share one block geometry along z");
 
 // Everything one forward or adjoint call launches with.
 struct Loop {
@@ -591,11 +598,21 @@ static bool encode(CUtensorMap *m, void *base, int rank, const cuuint64_t *dims,
 }
 
 template <int M>
-static void smem_attrs(size_t vel, size_t str) {
-    cudaFuncSetAttribute(k_velocity_tma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vel);
-    cudaFuncSetAttribute(k_velocity_tma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vel);
-    cudaFuncSetAttribute(k_stress_tma<M, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)str);
-    cudaFuncSetAttribute(k_stress_tma<M, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)str);
+static void smem_attrs(int by, size_t vel, size_t str) {
+    const auto set = [](const void *f, size_t b) {
+        cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b);
+    };
+    if (by == 7) {
+        set((const void *)t7::k_velocity_tma<true>, vel);
+        set((const void *)t7::k_velocity_tma<false>, vel);
+        set((const void *)t7::k_stress_tma<M, true>, str);
+        set((const void *)t7::k_stress_tma<M, false>, str);
+    } else {
+        set((const void *)t8::k_velocity_tma<true>, vel);
+        set((const void *)t8::k_velocity_tma<false>, vel);
+        set((const void *)t8::k_stress_tma<M, true>, str);
+        set((const void *)t8::k_stress_tma<M, false>, str);
+    }
 }
 
 // An exact reciprocal exists for a power-of-two spacing: x/h == x*(1/h) bit for bit.
@@ -613,7 +630,10 @@ static bool setup_tma(ifosb_engine *e, Loop &L, float *dft) {
     const int nsr = 6 + 6 * p.nmech;
     const int nm = (p.nmech == 0 || e->unif_tau) ? 5 : 10;
     const int ndf = (dft && e->nf > 0) ? 6 * e->nf : 0;
-    const size_t vs = vel_tma_smem(), ss = str_tma_smem(nsr, nm, ndf);
+    const bool t7 = g.by == 7;
+    const size_t vs = t7 ? t7::vel_tma_smem() : t8::vel_tma_smem();
+    const size_t ss = t7 ? t7::str_tma_smem(nsr, nm, ndf) : t8::str_tma_smem(nsr, nm, ndf);
+    const cuuint32_t TX = (cuuint32_t)g.by, RX = TX + 2 * HX;
     if (vs > 227 * 1024 || ss > 227 * 1024) return false;
     const cuuint64_t sdims[5] = {(cuuint64_t)g.pz, (cuuint64_t)g.px, (cuuint64_t)(p.ny + 5), (cuuint64_t)nslot,
                                  (cuuint64_t)e->max_shots};
@@ -621,9 +641,9 @@ static bool setup_tma(ifosb_engine *e, Loop &L, float *dft) {
                                 (cuuint64_t)e->st_shot * 4};
     const cuuint64_t mdims[4] = {(cuuint64_t)g.pz, (cuuint64_t)g.px, (cuuint64_t)(p.ny + 5), (cuuint64_t)NMODEL};
     const cuuint64_t mstr[3] = {(cuuint64_t)g.pz * 4, (cuuint64_t)g.plane * 4, (cuuint64_t)g.field * 4};
-    const cuuint32_t bhalo[5] = {RZ, RX, 1, 3, 1}, bpt[5] = {TZ, TX, 1, 3, 1};
-    const cuuint32_t bsr[5] = {TZ, TX, 1, (cuuint32_t)nsr, 1};
-    const cuuint32_t bmv[4] = {TZ, TX, 1, 3}, bms[4] = {TZ, TX, 1, (cuuint32_t)nm};
+    const cuuint32_t bhalo[5] = {(cuuint32_t)RZ, RX, 1, 3, 1}, bpt[5] = {(cuuint32_t)TZ, TX, 1, 3, 1};
+    const cuuint32_t bsr[5] = {(cuuint32_t)TZ, TX, 1, (cuuint32_t)nsr, 1};
+    const cuuint32_t bmv[4] = {(cuuint32_t)TZ, TX, 1, 3}, bms[4] = {(cuuint32_t)TZ, TX, 1, (cuuint32_t)nm};
     L.vt = VelTma{};
     L.stt = StrTma{};
     if (!encode(&L.vt.m_halo, e->d_state, 5, sdims, sstr, bhalo) || !encode(&L.vt.m_pt, e->d_state, 5, sdims, sstr, bpt) ||
@@ -636,7 +656,7 @@ static bool setup_tma(ifosb_engine *e, Loop &L, float *dft) {
                                      (cuuint64_t)(6 * e->max_nf), (cuuint64_t)e->max_shots};
         const cuuint64_t dstr[4] = {(cuuint64_t)g.pz * 4, (cuuint64_t)g.plane * 4, (cuuint64_t)g.field * 4,
                                     (cuuint64_t)e->dft_shot * 4};
-        const cuuint32_t bd[5] = {TZ, TX, 1, (cuuint32_t)ndf, 1};
+        const cuuint32_t bd[5] = {(cuuint32_t)TZ, TX, 1, (cuuint32_t)ndf, 1};
         if (!encode(&L.stt.m_dft, dft, 5, ddims, dstr, bd)) return false;
     }
     L.vt.a = L.va;
@@ -659,23 +679,29 @@ static bool setup_tma(ifosb_engine *e, Loop &L, float *dft) {
     L.vel_smem = vs;
     L.str_smem = ss;
     switch (p.nmech) {
-    case 0: smem_attrs<0>(vs, ss); break;
-    case 1: smem_attrs<1>(vs, ss); break;
-    case 2: smem_attrs<2>(vs, ss); break;
-    case 3: smem_attrs<3>(vs, ss); break;
-    default: smem_attrs<4>(vs, ss); break;
+    case 0: smem_attrs<0>(g.by, vs, ss); break;
+    case 1: smem_attrs<1>(g.by, vs, ss); break;
+    case 2: smem_attrs<2>(g.by, vs, ss); break;
+    case 3: smem_attrs<3>(g.by, vs, ss); break;
+    default: smem_attrs<4>(g.by, vs, ss); break;
     }
     return cudaGetLastError() == cudaSuccess;
 }
 
 template <int M>
 static void launch_str_m(const Loop &L, dim3 grd, cudaStream_t st, int nt, int do_dft, int sample) {
+    const int by = L.lg.by;
     if (L.tma) {
-        const dim3 blk(TZ, TX + 1);
-        if (L.p2) k_stress_tma<M, true><<<grd, blk, L.str_smem, st>>>(L.stt, nt, do_dft, sample);
-        else k_stress_tma<M, false><<<grd, blk, L.str_smem, st>>>(L.stt, nt, do_dft, sample);
+        const dim3 blk(TZ, by + 1);
+        if (by == 7) {
+            if (L.p2) t7::k_stress_tma<M, true><<<grd, blk, L.str_smem, st>>>(L.stt, nt, do_dft, sample);
+            else t7::k_stress_tma<M, false><<<grd, blk, L.str_smem, st>>>(L.stt, nt, do_dft, sample);
+        } else {
+            if (L.p2) t8::k_stress_tma<M, true><<<grd, blk, L.str_smem, st>>>(L.stt, nt, do_dft, sample);
+            else t8::k_stress_tma<M, false><<<grd, blk, L.str_smem, st>>>(L.stt, nt, do_dft, sample);
+        }
     } else {
-        k_stress<M><<<grd, dim3(BX, BY), 0, st>>>(L.sa, nt, do_dft, sample);
+        k_stress<M><<<grd, dim3(BX, by), 0, st>>>(L.sa, nt, do_dft, sample);
     }
 }
 
@@ -690,12 +716,18 @@ static void launch_str(int nmech, const Loop &L, dim3 grd, cudaStream_t st, int 
 }
 
 static void launch_vel(const Loop &L, dim3 grd, cudaStream_t st, int nt) {
+    const int by = L.lg.by;
     if (L.tma) {
-        const dim3 blk(TZ, TX + 1);
-        if (L.back) k_velocity_tma<true><<<grd, blk, L.vel_smem, st>>>(L.vt, nt);
-        else k_velocity_tma<false><<<grd, blk, L.vel_smem, st>>>(L.vt, nt);
+        const dim3 blk(TZ, by + 1);
+        if (by == 7) {
+            if (L.back) t7::k_velocity_tma<true><<<grd, blk, L.vel_smem, st>>>(L.vt, nt);
+            else t7::k_velocity_tma<false><<<grd, blk, L.vel_smem, st>>>(L.vt, nt);
+        } else {
+            if (L.back) t8::k_velocity_tma<true><<<grd, blk, L.vel_smem, st>>>(L.vt, nt);
+            else t8::k_velocity_tma<false><<<grd, blk, L.vel_smem, st>>>(L.vt, nt);
+        }
     } else {
-        const dim3 blk(BX, BY);
+        const dim3 blk(BX, by);
         if (L.back) k_velocity<true><<<grd, blk, 0, st>>>(L.va, nt);
         else k_velocity<false><<<grd, blk, 0, st>>>(L.va, nt);
     }

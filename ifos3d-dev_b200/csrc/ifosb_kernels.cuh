@@ -44,6 +44,7 @@ struct Geo {
     long long field;    // (NY+5)*plane
     int cy, nyc;        // y planes per block, y chunks
     int ntk, nti;       // blocks along z and x
+    int by;             // rows (x) per block: the tile height of the kernels in use
 };
 
 __host__ __device__ __forceinline__ long long widx(const Geo &g, int j, int i, int k) {
@@ -184,7 +185,7 @@ template <bool BACK>
 __global__ void __launch_bounds__(BX *BY) k_velocity(VelArgs a, int nt) {
     const Geo &g = a.g;
     const int k = blockIdx.x * BX + threadIdx.x + 1;
-    const int i = blockIdx.y * BY + threadIdx.y + 1;
+    const int i = blockIdx.y * blockDim.y + threadIdx.y + 1;  // blockDim.y == g.by
     const int yc = blockIdx.z % g.nyc, s = blockIdx.z / g.nyc;
     int p0, p1;
     block_points(a.pt_off, g, s, yc, p0, p1);
@@ -268,7 +269,7 @@ template <int L>
 __global__ void __launch_bounds__(BX *BY) k_stress(StrArgs a, int nt, int do_dft, int sample) {
     const Geo &g = a.g;
     const int k = blockIdx.x * BX + threadIdx.x + 1;
-    const int i = blockIdx.y * BY + threadIdx.y + 1;
+    const int i = blockIdx.y * blockDim.y + threadIdx.y + 1;  // blockDim.y == g.by
     const int yc = blockIdx.z % g.nyc, s = blockIdx.z / g.nyc;
     int p0, p1;
     block_points(a.pt_off, g, s, yc, p0, p1);

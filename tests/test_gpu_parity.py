@@ -207,3 +207,14 @@ def test_autotuned_launch_shape_gives_the_same_bits():
     assert np.array_equal(out[0][0], out[1][0])
     assert np.array_equal(out[0][1], out[1][1])
     assert np.array_equal(out[0][2], out[1][2])
+
+
+@pytest.mark.parametrize("rows", [7, 8])
+@pytest.mark.parametrize("nmech", [0, 3])
+def test_tile_heights_match(rows, nmech, oracle, request, monkeypatch):
+    """Both tile heights of the TMA kernels (7-row tiles, chosen with memory
+    variables, and 8-row tiles) give the reference's bits for either model kind,
+    on a grid that is not a multiple of either."""
+    monkeypatch.setenv("IFOSB_TILE_ROWS", str(rows))
+    c = synth.small_case(nx=37, ny=30, nz=35, nt=40, fw=5, nmech=nmech, nshots=2, seed=23)
+    check_case(c, pick_oracle(nmech, oracle, request))
