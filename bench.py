@@ -292,7 +292,7 @@ def main():
         all_obs[rank] = obs[0]
 
     # launch shape for this batch from the engine's autotuner (not timed)
-    tuned_cy, tuned_l2 = eng.autotune(shots, steps=min(20, p.nt))
+    tuned = eng.autotune(shots, steps=min(60, p.nt))
 
     def step():
         if wl == "elastic128" and dist:
@@ -390,9 +390,7 @@ def main():
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 2), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": dict(workload_config(wl, world), launch_shape={"y_planes_per_cta": tuned_cy,
-                                                                  "l2_prefetch_planes": tuned_l2,
-                                                                  "picked_by": "ifosb_autotune"}),
+        "config": dict(workload_config(wl, world), launch_shape=dict(tuned, picked_by="ifosb_autotune")),
         "clocks": clocks,
         "e2e": {"value": round(e2e, 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(launches), "roofline": roofline,

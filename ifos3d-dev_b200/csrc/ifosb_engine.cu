@@ -83,7 +83,11 @@ struct ifosb_engine {
     cudaStream_t own_stream = nullptr;
     // launch shapes picked by ifosb_autotune per batch size: y planes per CTA chunk
     // and the L2 prefetch distance; nt_limit > 0 shortens the time loop while tuning
-    std::map<int, std::pair<int, int>> tuned;
+    struct Shape {
+        int cyv, l2v, cys, l2s;  // velocity and stress kernels: y planes per chunk, L2 prefetch
+    };
+    std::map<int, Shape> tuned;
+    int vby = 8;  // rows per tile of the velocity kernel
     int nt_limit = 0;
     // TMA staging (default) and its wait-timeout flag
     int use_tma = 1;
@@ -242,6 +246,11 @@ extern "C" int ifosb_create(const ifosb_params *p, int max_shots, int max_nf, if
         const int t = atoi(v);
         if (t == 7 || t == 8) g.by = t;
     }
+    if (const char *v = getenv("IFOSB_VEL_TILE_ROWS")) {
+        const int t = atoi(v);
+        if (t == 7 || t == 8) e->vby = t;
+    }
+    if (!e->use_tma) e->vby = g.by;
     g.ntk = (p->nz + BX - 1) / BX;
     g.nti = (p->nx + g.by - 1) / g.by;
     if ((long long)g.nyc * max_shots > 65535) { delete e; return IFOSB_EARG; }
@@ -491,7 +500,8 @@ static_assert(TZ == BX, "TMA tiles and plain blocks share one block geometry alo
 
 // Everything one forward or adjoint call launches with.
 struct Loop {
-    Geo lg;  // launch geometry of this call (the y chunking depends on the batch size)
+    Geo lg;   // launch geometry of the stress kernel (the y chunking depends on the batch size)
+    Geo lgv;  // launch geometry of the velocity kernel
     VelArgs va;
     StrArgs sa;
     VelTma vt;
@@ -505,11 +515,15 @@ struct Loop {
 
 // y planes per CTA: long chunks amortise the ring prologue; enough chunks keep
 // about four CTAs per SM in flight over the whole batch.
-static Geo launch_geo(const ifosb_engine *e, int nshots) {
+static Geo launch_geo(const ifosb_engine *e, int nshots, bool vel) {
     Geo g = e->g;
+    if (vel) {
+        g.by = e->vby;
+        g.nti = (g.nx + g.by - 1) / g.by;
+    }
     auto t = e->tuned.find(nshots);
     if (t != e->tuned.end()) {
-        g.cy = t->second.first;
+        g.cy = vel ? t->second.cyv : t->second.cys;
         g.nyc = (g.ny + g.cy - 1) / g.cy;
         return g;
     }
@@ -531,7 +545,8 @@ static void fill_common(ifosb_engine *e, Loop &L) {
     StrArgs &sa = L.sa;
     va = VelArgs{};
     sa = StrArgs{};
-    va.g = sa.g = L.lg;
+    va.g = L.lgv;
+    sa.g = L.lg;
     va.sl = sa.sl = e->sl;
     va.st = sa.st = e->d_state;
     va.st_shot = sa.st_shot = e->st_shot;
@@ -597,21 +612,24 @@ static bool encode(CUtensorMap *m, void *base, int rank, const cuuint64_t *dims,
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+static void smem_set(const void *f, size_t bytes) {
+    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
 template <int M>
-static void smem_attrs(int by, size_t vel, size_t str) {
-    const auto set = [](const void *f, size_t b) {
-        cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b);
-    };
-    if (by == 7) {
-        set((const void *)t7::k_velocity_tma<true>, vel);
-        set((const void *)t7::k_velocity_tma<false>, vel);
-        set((const void *)t7::k_stress_tma<M, true>, str);
-        set((const void *)t7::k_stress_tma<M, false>, str);
+static void smem_attrs(int vby, int sby, size_t vel, size_t str) {
+    if (vby == 7) {
+        smem_set((const void *)t7::k_velocity_tma<true>, vel);
+        smem_set((const void *)t7::k_velocity_tma<false>, vel);
     } else {
-        set((const void *)t8::k_velocity_tma<true>, vel);
-        set((const void *)t8::k_velocity_tma<false>, vel);
-        set((const void *)t8::k_stress_tma<M, true>, str);
-        set((const void *)t8::k_stress_tma<M, false>, str);
+        smem_set((const void *)t8::k_velocity_tma<true>, vel);
+        smem_set((const void *)t8::k_velocity_tma<false>, vel);
+    }
+    if (sby == 7) {
+        smem_set((const void *)t7::k_stress_tma<M, true>, str);
+        smem_set((const void *)t7::k_stress_tma<M, false>, str);
+    } else {
+        smem_set((const void *)t8::k_stress_tma<M, true>, str);
+        smem_set((const void *)t8::k_stress_tma<M, false>, str);
     }
 }
 
@@ -630,10 +648,10 @@ static bool setup_tma(ifosb_engine *e, Loop &L, float *dft) {
     const int nsr = 6 + 6 * p.nmech;
     const int nm = (p.nmech == 0 || e->unif_tau) ? 5 : 10;
     const int ndf = (dft && e->nf > 0) ? 6 * e->nf : 0;
-    const bool t7 = g.by == 7;
-    const size_t vs = t7 ? t7::vel_tma_smem() : t8::vel_tma_smem();
-    const size_t ss = t7 ? t7::str_tma_smem(nsr, nm, ndf) : t8::str_tma_smem(nsr, nm, ndf);
-    const cuuint32_t TX = (cuuint32_t)g.by, RX = TX + 2 * HX;
+    const size_t vs = L.lgv.by == 7 ? t7::vel_tma_smem() : t8::vel_tma_smem();
+    const size_t ss = L.lg.by == 7 ? t7::str_tma_smem(nsr, nm, ndf) : t8::str_tma_smem(nsr, nm, ndf);
+    const cuuint32_t TXV = (cuuint32_t)L.lgv.by, RXV = TXV + 2 * HX;  // velocity tile rows, ring rows
+    const cuuint32_t TX = (cuuint32_t)L.lg.by, RX = TX + 2 * HX;      // stress tile rows, ring rows
     if (vs > 227 * 1024 || ss > 227 * 1024) return false;
     const cuuint64_t sdims[5] = {(cuuint64_t)g.pz, (cuuint64_t)g.px, (cuuint64_t)(p.ny + 5), (cuuint64_t)nslot,
                                  (cuuint64_t)e->max_shots};
@@ -641,16 +659,17 @@ static bool setup_tma(ifosb_engine *e, Loop &L, float *dft) {
                                 (cuuint64_t)e->st_shot * 4};
     const cuuint64_t mdims[4] = {(cuuint64_t)g.pz, (cuuint64_t)g.px, (cuuint64_t)(p.ny + 5), (cuuint64_t)NMODEL};
     const cuuint64_t mstr[3] = {(cuuint64_t)g.pz * 4, (cuuint64_t)g.plane * 4, (cuuint64_t)g.field * 4};
-    const cuuint32_t bhalo[5] = {(cuuint32_t)RZ, RX, 1, 3, 1}, bpt[5] = {(cuuint32_t)TZ, TX, 1, 3, 1};
-    const cuuint32_t bsr[5] = {(cuuint32_t)TZ, TX, 1, (cuuint32_t)nsr, 1};
-    const cuuint32_t bmv[4] = {(cuuint32_t)TZ, TX, 1, 3}, bms[4] = {(cuuint32_t)TZ, TX, 1, (cuuint32_t)nm};
+    const cuuint32_t bhalov[5] = {(cuuint32_t)RZ, RXV, 1, 3, 1}, bpt[5] = {(cuuint32_t)TZ, TXV, 1, 3, 1};
+    const cuuint32_t bmv[4] = {(cuuint32_t)TZ, TXV, 1, 3};
+    const cuuint32_t bhalo[5] = {(cuuint32_t)RZ, RX, 1, 3, 1}, bsr[5] = {(cuuint32_t)TZ, TX, 1, (cuuint32_t)nsr, 1};
+    const cuuint32_t bms[4] = {(cuuint32_t)TZ, TX, 1, (cuuint32_t)nm};
     L.vt = VelTma{};
     L.stt = StrTma{};
-    if (!encode(&L.vt.m_halo, e->d_state, 5, sdims, sstr, bhalo) || !encode(&L.vt.m_pt, e->d_state, 5, sdims, sstr, bpt) ||
-        !encode(&L.vt.m_mod, e->d_model, 4, mdims, mstr, bmv) || !encode(&L.stt.m_sr, e->d_state, 5, sdims, sstr, bsr) ||
-        !encode(&L.stt.m_mod, e->d_model, 4, mdims, mstr, bms))
+    if (!encode(&L.vt.m_halo, e->d_state, 5, sdims, sstr, bhalov) ||
+        !encode(&L.vt.m_pt, e->d_state, 5, sdims, sstr, bpt) || !encode(&L.vt.m_mod, e->d_model, 4, mdims, mstr, bmv) ||
+        !encode(&L.stt.m_halo, e->d_state, 5, sdims, sstr, bhalo) ||
+        !encode(&L.stt.m_sr, e->d_state, 5, sdims, sstr, bsr) || !encode(&L.stt.m_mod, e->d_model, 4, mdims, mstr, bms))
         return false;
-    L.stt.m_halo = L.vt.m_halo;
     if (ndf) {
         const cuuint64_t ddims[5] = {(cuuint64_t)g.pz, (cuuint64_t)g.px, (cuuint64_t)(p.ny + 5),
                                      (cuuint64_t)(6 * e->max_nf), (cuuint64_t)e->max_shots};
@@ -664,7 +683,8 @@ static bool setup_tma(ifosb_engine *e, Loop &L, float *dft) {
     L.vt.tma_err = L.stt.tma_err = e->d_tma_err;
     {
         auto t = e->tuned.find(L.nshots);
-        L.vt.l2ahead = L.stt.l2ahead = t != e->tuned.end() ? t->second.second : L2AHEAD_DEFAULT;
+        L.vt.l2ahead = t != e->tuned.end() ? t->second.l2v : L2AHEAD_DEFAULT;
+        L.stt.l2ahead = t != e->tuned.end() ? t->second.l2s : L2AHEAD_DEFAULT;
     }
     L.stt.nsr = nsr;
     L.stt.nm = nm;
@@ -679,11 +699,11 @@ static bool setup_tma(ifosb_engine *e, Loop &L, float *dft) {
     L.vel_smem = vs;
     L.str_smem = ss;
     switch (p.nmech) {
-    case 0: smem_attrs<0>(g.by, vs, ss); break;
-    case 1: smem_attrs<1>(g.by, vs, ss); break;
-    case 2: smem_attrs<2>(g.by, vs, ss); break;
-    case 3: smem_attrs<3>(g.by, vs, ss); break;
-    default: smem_attrs<4>(g.by, vs, ss); break;
+    case 0: smem_attrs<0>(L.lgv.by, L.lg.by, vs, ss); break;
+    case 1: smem_attrs<1>(L.lgv.by, L.lg.by, vs, ss); break;
+    case 2: smem_attrs<2>(L.lgv.by, L.lg.by, vs, ss); break;
+    case 3: smem_attrs<3>(L.lgv.by, L.lg.by, vs, ss); break;
+    default: smem_attrs<4>(L.lgv.by, L.lg.by, vs, ss); break;
     }
     return cudaGetLastError() == cudaSuccess;
 }
@@ -716,7 +736,7 @@ static void launch_str(int nmech, const Loop &L, dim3 grd, cudaStream_t st, int 
 }
 
 static void launch_vel(const Loop &L, dim3 grd, cudaStream_t st, int nt) {
-    const int by = L.lg.by;
+    const int by = L.lgv.by;
     if (L.tma) {
         const dim3 blk(TZ, by + 1);
         if (by == 7) {
@@ -747,10 +767,10 @@ static void step_flags(const ifosb_engine *e, bool back, int nt, int &lsamp, int
 // Enqueue the NT steps (two kernels per step) on the engine stream.
 static void enqueue_loop(ifosb_engine *e, const Loop &L) {
     const ifosb_params &p = e->p;
-    dim3 grd(L.lg.ntk, L.lg.nti, L.lg.nyc * L.nshots);
+    const dim3 grd(L.lg.ntk, L.lg.nti, L.lg.nyc * L.nshots), grdv(L.lgv.ntk, L.lgv.nti, L.lgv.nyc * L.nshots);
     int lsamp = p.ndtshift + 1, nlsamp = 0;
     for (int nt = 1; nt <= p.nt; ++nt) {
-        launch_vel(L, grd, e->stream, nt);
+        launch_vel(L, grdv, e->stream, nt);
         int do_dft, sample;
         step_flags(e, L.back, nt, lsamp, nlsamp, do_dft, sample);
         launch_str(p.nmech, L, grd, e->stream, nt, do_dft, sample);
@@ -767,12 +787,12 @@ static int run_loop_profiled(ifosb_engine *e, const Loop &L) {
         CU(cudaEventCreate(&ev));
         e->events.push_back(ev);
     }
-    dim3 grd(L.lg.ntk, L.lg.nti, L.lg.nyc * L.nshots);
+    const dim3 grd(L.lg.ntk, L.lg.nti, L.lg.nyc * L.nshots), grdv(L.lgv.ntk, L.lgv.nti, L.lgv.nyc * L.nshots);
     int lsamp = p.ndtshift + 1, nlsamp = 0;
     for (int nt = 1; nt <= nsteps; ++nt) {
         cudaEvent_t *ev = &e->events[(size_t)3 * (nt - 1)];
         CU(cudaEventRecord(ev[0], e->stream));
-        launch_vel(L, grd, e->stream, nt);
+        launch_vel(L, grdv, e->stream, nt);
         CU(cudaEventRecord(ev[1], e->stream));
         int do_dft, sample;
         step_flags(e, L.back, nt, lsamp, nlsamp, do_dft, sample);
@@ -895,9 +915,10 @@ extern "C" int ifosb_forward(ifosb_engine *e, int nshots, const ifosb_shot *shot
     Loop L;
     L.nshots = nshots;
     L.back = false;
-    L.lg = launch_geo(e, nshots);
+    L.lg = launch_geo(e, nshots, false);
+    L.lgv = launch_geo(e, nshots, true);
     int rc;
-    if ((rc = upload_points(e, L.lg, nshots, vp, &e->d_voff, &e->cap_voff, &e->d_vpts, &e->cap_vpts)) ||
+    if ((rc = upload_points(e, L.lgv, nshots, vp, &e->d_voff, &e->cap_voff, &e->d_vpts, &e->cap_vpts)) ||
         (rc = upload_points(e, L.lg, nshots, sp, &e->d_soff, &e->cap_soff, &e->d_spts, &e->cap_spts)) ||
         (rc = dgrow(e, &e->d_amp, &e->cap_amp, amp.size())))
         return rc;
@@ -964,9 +985,10 @@ extern "C" int ifosb_adjoint(ifosb_engine *e, const float *diff) {
     Loop L;
     L.nshots = nshots;
     L.back = true;
-    L.lg = launch_geo(e, nshots);
+    L.lg = launch_geo(e, nshots, false);
+    L.lgv = launch_geo(e, nshots, true);
     int rc;
-    if ((rc = upload_points(e, L.lg, nshots, vp, &e->d_voff, &e->cap_voff, &e->d_vpts, &e->cap_vpts))) return rc;
+    if ((rc = upload_points(e, L.lgv, nshots, vp, &e->d_voff, &e->cap_voff, &e->d_vpts, &e->cap_vpts))) return rc;
     if ((rc = reset_state(e, nshots, e->d_dftb))) return rc;
     fill_common(e, L);
     VelArgs &va = L.va;
@@ -1119,30 +1141,27 @@ extern "C" int ifosb_residual_noalloc(int nshots, int ntr, int ns, float dt, con
 // and the L2 prefetch distance of the TMA kernels — and keeps the fastest for
 // later calls with that batch size. The shape changes no arithmetic: results
 // stay bit-identical. The wavefield of the batch is left undefined.
-extern "C" int ifosb_autotune(ifosb_engine *e, int nshots, const ifosb_shot *shots, int steps, int *cy_out,
-                              int *l2_out) {
+extern "C" int ifosb_autotune(ifosb_engine *e, int nshots, const ifosb_shot *shots, int steps, int *shape) {
     if (!e || !shots || nshots < 1 || nshots > e->max_shots || steps < 1) return IFOSB_EARG;
     const int saved_profile = e->profile;
     e->tuned.erase(nshots);
-    const Geo h = launch_geo(e, nshots);  // the heuristic shape is a candidate too
-    std::vector<int> cys = {2, 3, 4, 6, 8, 12, 16, 24, 32, 64, h.cy};
+    const Geo hv = launch_geo(e, nshots, true), hs = launch_geo(e, nshots, false);  // built-in choices
+    std::vector<int> cys = {2, 3, 4, 6, 8, 12, 16, 24, 32, 64, hv.cy, hs.cy};
     std::sort(cys.begin(), cys.end());
     cys.erase(std::unique(cys.begin(), cys.end()), cys.end());
-    double best = 1e30;
-    std::pair<int, int> pick(h.cy, L2AHEAD_DEFAULT);
+    double bv = 1e30, bs = 1e30;
+    ifosb_engine::Shape pick{hv.cy, L2AHEAD_DEFAULT, hs.cy, L2AHEAD_DEFAULT};
     int rc = IFOSB_OK;
     e->profile = 1;
     e->nt_limit = steps;
     for (int cy : cys) {
         if (cy > e->p.ny || (long long)((e->p.ny + cy - 1) / cy) * nshots > 65535) continue;
         for (int l2 : {0, 1, 2, 3}) {
-            e->tuned[nshots] = {cy, l2};
+            e->tuned[nshots] = {cy, l2, cy, l2};
             if ((rc = ifosb_forward(e, nshots, shots, nullptr))) break;
-            const double ms = e->t_vel_ms + e->t_str_ms;
-            if (ms < best) {
-                best = ms;
-                pick = {cy, l2};
-            }
+            // the two kernels are timed separately: each keeps its own best shape
+            if (e->t_vel_ms < bv) { bv = e->t_vel_ms; pick.cyv = cy; pick.l2v = l2; }
+            if (e->t_str_ms < bs) { bs = e->t_str_ms; pick.cys = cy; pick.l2s = l2; }
         }
         if (rc) break;
     }
@@ -1156,7 +1175,11 @@ extern "C" int ifosb_autotune(ifosb_engine *e, int nshots, const ifosb_shot *sho
     e->tuned[nshots] = pick;
     release_graph(e->gfwd);
     release_graph(e->gadj);
-    if (cy_out) *cy_out = pick.first;
-    if (l2_out) *l2_out = pick.second;
+    if (shape) {
+        shape[0] = pick.cyv;
+        shape[1] = pick.l2v;
+        shape[2] = pick.cys;
+        shape[3] = pick.l2s;
+    }
     return IFOSB_OK;
 }

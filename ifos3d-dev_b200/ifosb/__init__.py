@@ -92,7 +92,7 @@ def lib():
             "ifosb_set_profiling": (C.c_int, [vp, C.c_int]),
             "ifosb_kernel_times": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int)]),
             "ifosb_set_stream": (C.c_int, [vp, vp]),
-            "ifosb_autotune": (C.c_int, [vp, C.c_int, C.POINTER(Shot), C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+            "ifosb_autotune": (C.c_int, [vp, C.c_int, C.POINTER(Shot), C.c_int, vp]),
             "ifosb_residual_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_float, vp, vp, vp, vp, vp]),
             "ifosb_optim_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(vp)]),
             "ifosb_optim_destroy": (None, [vp]),
@@ -294,11 +294,13 @@ class Engine:
         return out
 
     def autotune(self, shots, steps=20):
-        """Pick the launch shape for batches of len(shots) shots; returns (cy, l2ahead)."""
+        """Pick the launch shapes for batches of len(shots) shots; returns a dict with
+        the y planes per CTA chunk and L2 prefetch distance of each kernel."""
         arr, keep = self._shots(shots)
-        cy, l2 = C.c_int(), C.c_int()
-        self._c(lib().ifosb_autotune(self.h, len(shots), arr, steps, C.byref(cy), C.byref(l2)))
-        return cy.value, l2.value
+        shape = np.zeros(4, np.int32)
+        self._c(lib().ifosb_autotune(self.h, len(shots), arr, steps, _p(shape)))
+        return {"velocity": {"y_planes_per_cta": int(shape[0]), "l2_prefetch_planes": int(shape[1])},
+                "stress": {"y_planes_per_cta": int(shape[2]), "l2_prefetch_planes": int(shape[3])}}
 
     def residual(self, obs, want_l2_ref=False):
         obs = _f32(obs)

@@ -162,12 +162,13 @@ int ifosb_kernel_times(const ifosb_engine *e, double *vel_ms, double *str_ms, in
 
 /* Autotuner: times `steps` forward time steps of this batch (the same shots a
  * later ifosb_forward / ifosb_shot_gradient will use) for each launch shape —
- * y planes per CTA chunk (2 to 64, and the built-in choice) and
- * the L2 prefetch distance of the TMA kernels (0-3 planes) — and keeps the fastest
- * for every later call with nshots shots. Results do not depend on the shape
- * (bit-identical). The batch's wavefield is undefined afterwards. cy_out, l2_out
- * (optional) get the choice. */
-int ifosb_autotune(ifosb_engine *e, int nshots, const ifosb_shot *shots, int steps, int *cy_out, int *l2_out);
+ * y planes per CTA chunk (2 to 64, and the built-in choice) and the L2 prefetch
+ * distance of the TMA kernels (0-3 planes) — and keeps, for each of the two
+ * time-step kernels, its fastest shape for every later call with nshots shots.
+ * Results do not depend on the shape (bit-identical). The batch's wavefield is
+ * undefined afterwards. shape (optional, int[4]) gets the choice: velocity
+ * kernel planes per chunk and prefetch distance, then the stress kernel's. */
+int ifosb_autotune(ifosb_engine *e, int nshots, const ifosb_shot *shots, int steps, int *shape);
 
 /* Run the engine's work on the caller's CUDA stream (a cudaStream_t passed as
  * void*; NULL = the engine's own stream). Calls stay synchronous at return. */

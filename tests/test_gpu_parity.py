@@ -195,9 +195,10 @@ def test_autotuned_launch_shape_gives_the_same_bits():
     c = synth.small_case(nx=37, ny=70, nz=45, nt=40, fw=6, nshots=3, seed=17)
     e1, m, cp, shots = engine_for(c)
     e2, _, _, _ = engine_for(c)
-    cy, l2 = e2.autotune(shots, steps=4)
-    assert 2 <= cy <= 64
-    assert l2 in (0, 1, 2, 3)
+    shape = e2.autotune(shots, steps=4)
+    for k in ("velocity", "stress"):
+        assert 2 <= shape[k]["y_planes_per_cta"] <= 64
+        assert shape[k]["l2_prefetch_planes"] in (0, 1, 2, 3)
     out = []
     for e in (e1, e2):
         sec = e.forward(shots)
@@ -212,9 +213,11 @@ def test_autotuned_launch_shape_gives_the_same_bits():
 @pytest.mark.parametrize("rows", [7, 8])
 @pytest.mark.parametrize("nmech", [0, 3])
 def test_tile_heights_match(rows, nmech, oracle, request, monkeypatch):
-    """Both tile heights of the TMA kernels (7-row tiles, chosen with memory
-    variables, and 8-row tiles) give the reference's bits for either model kind,
-    on a grid that is not a multiple of either."""
+    """Both tile heights of both TMA kernels (by default the velocity kernel
+    uses 8-row tiles, the stress kernel 7-row tiles with memory variables and
+    8-row tiles without) give the reference's bits for either model kind, on a
+    grid that is not a multiple of either."""
     monkeypatch.setenv("IFOSB_TILE_ROWS", str(rows))
+    monkeypatch.setenv("IFOSB_VEL_TILE_ROWS", str(rows))
     c = synth.small_case(nx=37, ny=30, nz=35, nt=40, fw=5, nmech=nmech, nshots=2, seed=23)
     check_case(c, pick_oracle(nmech, oracle, request))
