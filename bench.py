@@ -393,7 +393,7 @@ def main():
         "config": dict(workload_config(wl, world), launch_shape=dict(tuned, picked_by="ifosb_autotune")),
         "clocks": clocks,
         "e2e": {"value": round(e2e, 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
-        "gpu_launches": int(launches), "roofline": roofline,
+        "gpu_launches": int(launches), "roofline": roofline, "graph_captures": eng.graph_captures,
     }
     if wl == "elastic128":
         out["shot_gradients_per_s"] = round(world * args.steps / (ms / 1000.0), 4)

@@ -89,6 +89,8 @@ struct ifosb_engine {
     std::map<int, Shape> tuned;
     int vby = 8;  // rows per tile of the velocity kernel
     int nt_limit = 0;
+    long long captures = 0;  // time-loop graphs captured (a replay reuses one)
+    float *d_mstage = nullptr;  // ifosb_set_model's staging of the raw model (5 ghosted fields)
     // TMA staging (default) and its wait-timeout flag
     int use_tma = 1;
     int *d_tma_err = nullptr;
@@ -306,7 +308,8 @@ extern "C" void ifosb_destroy(ifosb_engine *e) {
     release_graph(e->gadj);
     void *bufs[] = {e->d_state, e->d_psi, e->d_model, e->d_rho_w, e->d_dftf, e->d_dftb, e->d_grad, e->d_grad64,
                     e->d_err, e->d_sec, e->d_diff, e->d_obs, e->d_part, e->d_misfit, e->d_l2, e->d_trig_f,
-                    e->d_trig_b, e->d_voff, e->d_soff, e->d_vpts, e->d_spts, e->d_amp, e->d_tma_err, e->d_cpg};
+                    e->d_trig_b, e->d_voff, e->d_soff, e->d_vpts, e->d_spts, e->d_amp, e->d_tma_err, e->d_cpg,
+                    e->d_mstage};
     for (void *b : bufs)
         if (b) cudaFree(b);
     for (cudaEvent_t ev : e->events) cudaEventDestroy(ev);
@@ -340,6 +343,7 @@ extern "C" int ifosb_set_stream(ifosb_engine *e, void *stream) {
 extern "C" const char *ifosb_last_error(const ifosb_engine *e) { return e ? e->err.c_str() : "no engine"; }
 extern "C" long long ifosb_device_bytes(const ifosb_engine *e) { return e ? e->dev_bytes : 0; }
 extern "C" long long ifosb_last_launch_count(const ifosb_engine *e) { return e ? e->launches : 0; }
+extern "C" long long ifosb_graph_captures(const ifosb_engine *e) { return e ? e->captures : 0; }
 
 extern "C" int ifosb_set_launch_mode(ifosb_engine *e, int mode) {
     if (!e || (mode != 0 && mode != 1)) return IFOSB_EARG;
@@ -378,9 +382,11 @@ extern "C" int ifosb_set_model(ifosb_engine *e, const float *rho, const float *p
             return fail(e, IFOSB_EARG, "model value not positive and finite at ghosted index " + std::to_string(q));
     for (int l = 0; l < p.nmech; ++l)
         if (!std::isfinite(eta[l])) return fail(e, IFOSB_EARG, "eta not finite");
-    float *tmp = nullptr;
-    int rc = dalloc(e, &tmp, ng * 5);
-    if (rc) return rc;
+    if (!e->d_mstage) {  // staging for the raw model, kept for the engine's lifetime
+        const int rc = dalloc(e, &e->d_mstage, ng * 5);
+        if (rc) return rc;
+    }
+    float *tmp = e->d_mstage;
     CU(cudaMemcpyAsync(tmp, rho, ng * sizeof(float), cudaMemcpyHostToDevice, e->stream));
     CU(cudaMemcpyAsync(tmp + ng, pi, ng * sizeof(float), cudaMemcpyHostToDevice, e->stream));
     CU(cudaMemcpyAsync(tmp + 2 * ng, u, ng * sizeof(float), cudaMemcpyHostToDevice, e->stream));
@@ -397,7 +403,6 @@ extern "C" int ifosb_set_model(ifosb_engine *e, const float *rho, const float *p
     k_av_mat<<<grd, blk, 0, e->stream>>>(a);
     cudaError_t le = cudaGetLastError();
     cudaError_t se = cudaStreamSynchronize(e->stream);
-    dfree(e, &tmp, ng * 5);
     if (le != cudaSuccess || se != cudaSuccess)
         return fail(e, IFOSB_ECUDA, std::string("av_mat: ") + cudaGetErrorString(le != cudaSuccess ? le : se));
     for (int l = 0; l < MAXMECH; ++l) e->eta[l] = l < p.nmech ? eta[l] : 0.f;
@@ -845,6 +850,7 @@ static int run_loop(ifosb_engine *e, const Loop &L) {
             return fail(e, IFOSB_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
         }
         gc.key = key;
+        ++e->captures;
     }
     CU(cudaGraphLaunch(gc.exec, e->stream));
     return IFOSB_OK;
@@ -913,6 +919,7 @@ extern "C" int ifosb_forward(ifosb_engine *e, int nshots, const ifosb_shot *shot
         for (int t = 0; t < e->ntr; ++t) sp.push_back({s, e->rec[3 * t + 1], e->rec[3 * t], e->rec[3 * t + 2], PT_RECEIVER, t});
     }
     Loop L;
+    std::memset(static_cast<void *>(&L), 0, sizeof(L));  // the graph cache compares Loops bytewise, padding included
     L.nshots = nshots;
     L.back = false;
     L.lg = launch_geo(e, nshots, false);
@@ -983,6 +990,7 @@ extern "C" int ifosb_adjoint(ifosb_engine *e, const float *diff) {
     for (int s = 0; s < nshots; ++s)
         for (int t = 0; t < ntr; ++t) vp.push_back({s, e->rec[3 * t + 1], e->rec[3 * t], e->rec[3 * t + 2], PT_ADJOINT, s * 3 * ntr + t});
     Loop L;
+    std::memset(static_cast<void *>(&L), 0, sizeof(L));  // the graph cache compares Loops bytewise, padding included
     L.nshots = nshots;
     L.back = true;
     L.lg = launch_geo(e, nshots, false);

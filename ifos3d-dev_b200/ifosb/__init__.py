@@ -85,6 +85,7 @@ def lib():
             "ifosb_get_field": (C.c_int, [vp, C.c_int, C.c_int, vp]),
             "ifosb_set_launch_mode": (C.c_int, [vp, C.c_int]),
             "ifosb_last_launch_count": (C.c_longlong, [vp]),
+            "ifosb_graph_captures": (C.c_longlong, [vp]),
             "ifosb_cpml_coeff": (C.c_int, [C.POINTER(Params), C.c_float, C.c_float, vp]),
             "ifosb_wavelet": (C.c_int, [C.POINTER(Params), C.c_int, C.c_int, vp, vp]),
             "ifosb_nsamples": (C.c_int, [C.POINTER(Params)]),
@@ -122,7 +123,7 @@ def exported_symbols():
         "ifosb_create", "ifosb_destroy", "ifosb_last_error", "ifosb_device_bytes", "ifosb_set_cpml",
         "ifosb_set_model", "ifosb_set_receivers", "ifosb_set_frequencies", "ifosb_forward", "ifosb_residual",
         "ifosb_adjoint", "ifosb_gradient", "ifosb_zero_gradient", "ifosb_get_gradient", "ifosb_shot_gradient",
-        "ifosb_get_field", "ifosb_set_launch_mode", "ifosb_last_launch_count", "ifosb_cpml_coeff",
+        "ifosb_get_field", "ifosb_set_launch_mode", "ifosb_last_launch_count", "ifosb_graph_captures", "ifosb_cpml_coeff",
         "ifosb_wavelet", "ifosb_nsamples", "ifosb_moduli", "ifosb_set_profiling", "ifosb_kernel_times",
         "ifosb_set_stream", "ifosb_autotune", "ifosb_residual_noalloc", "ifosb_optim_create", "ifosb_optim_destroy",
         "ifosb_optim_last_error", "ifosb_conjugate", "ifosb_lbfgs_savegrad", "ifosb_lbfgs", "ifosb_modelupdate",
@@ -258,6 +259,10 @@ class Engine:
 
     def set_launch_mode(self, mode: int):
         self._c(lib().ifosb_set_launch_mode(self.h, mode))
+
+    @property
+    def graph_captures(self) -> int:
+        return lib().ifosb_graph_captures(self.h)
 
     @property
     def launch_count(self) -> int:

@@ -153,6 +153,10 @@ int ifosb_set_launch_mode(ifosb_engine *e, int mode);
 /* Kernels launched by the last forward/adjoint call (per-step kernels x steps). */
 long long ifosb_last_launch_count(const ifosb_engine *e);
 
+/* Time-loop CUDA graphs captured so far: a call with the same batch shape and
+ * inputs as an earlier one replays its graph instead of capturing a new one. */
+long long ifosb_graph_captures(const ifosb_engine *e);
+
 /* Kernel timing: with profile=1 the time loops launch kernel by kernel with a
  * CUDA event pair around every launch on the engine's stream; after a forward
  * or adjoint call ifosb_kernel_times returns the summed device milliseconds of

@@ -221,3 +221,22 @@ def test_tile_heights_match(rows, nmech, oracle, request, monkeypatch):
     monkeypatch.setenv("IFOSB_VEL_TILE_ROWS", str(rows))
     c = synth.small_case(nx=37, ny=30, nz=35, nt=40, fw=5, nmech=nmech, nshots=2, seed=23)
     check_case(c, pick_oracle(nmech, oracle, request))
+
+
+def test_time_loop_graph_is_reused():
+    """Repeated shot gradients with the same batch shape replay the captured
+    forward and adjoint graphs, also across model changes: no new capture once
+    the first shot gradient after a model change has run."""
+    c = synth.small_case(nt=30, nshots=2, seed=29)
+    e, m, cp, shots = engine_for(c)
+    sec = e.forward(shots)
+    obs = (sec * np.float32(0.9)).astype(np.float32)
+    e.shot_gradient(shots, obs)
+    e.set_model(m["rho"], m["pi"], m["u"], m["taus"], m["taup"], m["eta"])
+    e.shot_gradient(shots, obs)
+    steady = e.graph_captures
+    assert 2 <= steady <= 4
+    for _ in range(3):
+        e.set_model(m["rho"], m["pi"], m["u"], m["taus"], m["taup"], m["eta"])
+        e.shot_gradient(shots, obs)
+    assert e.graph_captures == steady
