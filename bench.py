@@ -241,6 +241,8 @@ def main():
     ap.add_argument("--cpu-procs", type=int, default=0)
     ap.add_argument("--cpu-nt", type=int, default=40)
     ap.add_argument("--cpu-warmup", action="store_true")
+    ap.add_argument("--shape", default=None,
+                    help="launch shape cy_vel,l2_vel,cy_str,l2_str instead of autotuning (profiling runs)")
     args = ap.parse_args()
     world, rank, local, dist = setup_dist(args)
     if args.impl == "reference":
@@ -292,7 +294,13 @@ def main():
         all_obs[rank] = obs[0]
 
     # launch shape for this batch from the engine's autotuner (not timed)
-    tuned = eng.autotune(shots, steps=min(60, p.nt))
+    if args.shape:
+        sh = [int(x) for x in args.shape.split(",")]
+        eng.set_launch_shape(len(shots), sh)
+        tuned = {"velocity": {"y_planes_per_cta": sh[0], "l2_prefetch_planes": sh[1]},
+                 "stress": {"y_planes_per_cta": sh[2], "l2_prefetch_planes": sh[3]}}
+    else:
+        tuned = eng.autotune(shots, steps=min(60, p.nt))
 
     def step():
         if wl == "elastic128" and dist:
@@ -390,7 +398,8 @@ def main():
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 2), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": dict(workload_config(wl, world), launch_shape=dict(tuned, picked_by="ifosb_autotune")),
+        "config": dict(workload_config(wl, world),
+                       launch_shape=dict(tuned, picked_by="--shape" if args.shape else "ifosb_autotune")),
         "clocks": clocks,
         "e2e": {"value": round(e2e, 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(launches), "roofline": roofline, "graph_captures": eng.graph_captures,

@@ -1191,3 +1191,19 @@ extern "C" int ifosb_autotune(ifosb_engine *e, int nshots, const ifosb_shot *sho
     }
     return IFOSB_OK;
 }
+
+// Sets the launch shapes for batches of nshots shots (as ifosb_autotune leaves
+// them): shape[4] = velocity kernel y planes per chunk and L2 prefetch distance,
+// then the stress kernel's. Lets a caller reuse a tuned shape without re-timing.
+extern "C" int ifosb_set_launch_shape(ifosb_engine *e, int nshots, const int *shape) {
+    if (!e || !shape || nshots < 1 || nshots > e->max_shots) return IFOSB_EARG;
+    for (int q : {0, 2})
+        if (shape[q] < 1 || shape[q] > e->p.ny || (long long)((e->p.ny + shape[q] - 1) / shape[q]) * nshots > 65535)
+            return fail(e, IFOSB_EARG, "y planes per chunk out of range");
+    for (int q : {1, 3})
+        if (shape[q] < 0 || shape[q] > 8) return fail(e, IFOSB_EARG, "L2 prefetch distance out of range (0-8)");
+    e->tuned[nshots] = {shape[0], shape[1], shape[2], shape[3]};
+    release_graph(e->gfwd);
+    release_graph(e->gadj);
+    return IFOSB_OK;
+}

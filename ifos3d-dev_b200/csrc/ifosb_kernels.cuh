@@ -63,6 +63,19 @@ enum { PT_EXPLOSIVE = 1, PT_ADJOINT = 6, PT_RECEIVER = 7 };
 __constant__ float c_cpml[18][2 * MAXFW];
 
 __device__ __forceinline__ float CP(int row, int h) { return c_cpml[row][h - 1]; }
+
+// a / b rounded to nearest (IEEE), the same bits as the division operator. The
+// division's range check sends a zero dividend down its slow path (three times
+// the cost of a normal quotient), and a wavefield is zero ahead of its front, so
+// a zero dividend is handled here: q = 2^-24 / b has the sign of b, is finite for
+// every finite non-zero b (2^-24 / 2^-149 = 2^125), +-0 for b = +-inf or |b| near
+// FLT_MAX, inf for b = 0 and NaN for b = NaN; a * q is then exactly 0 / b
+// (+-0 with the sign of a xor b, NaN for b = 0 or NaN).
+__device__ __forceinline__ float div_rn(float a, float b) {
+    const bool z = a == 0.f;
+    const float q = __fdiv_rn(z ? 0x1p-24f : a, b);
+    return z ? __fmul_rn(a, q) : q;
+}
 // z-face slab indices differ between the lanes of a warp; the constant cache would
 // serialise them, L1 serves them in one pass
 __device__ __forceinline__ float CPG(const float *cpg, int row, int h) { return __ldg(cpg + row * 2 * MAXFW + h - 1); }

@@ -49,6 +49,18 @@ __host__ __device__ constexpr int a32(int x) { return (x + 31) & ~31; }
 constexpr int NSTAGE = IFOSB_NSTAGE;         // stage buffers (point-wise fields of NSTAGE planes in flight)
 static_assert(NSTAGE >= 2, "two stages at least");
 constexpr int NBAR = 2 * RING + 2 * NSTAGE;  // full/empty per ring slot, full/empty per stage
+// The velocity kernel holds less per plane than the stress kernel, so it can
+// afford a deeper ring and more stages (more loads in flight per CTA).
+#ifndef IFOSB_VRING
+#define IFOSB_VRING RING
+#endif
+#ifndef IFOSB_VNSTAGE
+#define IFOSB_VNSTAGE NSTAGE
+#endif
+constexpr int VRING = IFOSB_VRING;
+constexpr int VNSTAGE = IFOSB_VNSTAGE;
+static_assert(VRING >= 6 && VNSTAGE >= 2, "velocity ring: j-2..j+2 plus one in flight; two stages at least");
+constexpr int VNBAR = 2 * VRING + 2 * VNSTAGE;
 
 __device__ __forceinline__ uint32_t su32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -183,7 +195,7 @@ __device__ __forceinline__ void psi_load(PsiPre &q, const float *ps, const Slabs
 template <bool P2>
 __device__ __forceinline__ float ddiv(float a, float d, float inv) {
     if constexpr (P2) return a * inv;
-    else return a / d;
+    else return div_rn(a, d);
 }
 
 // The tile-height-dependent part, compiled for 8-row and 7-row tiles. The engine

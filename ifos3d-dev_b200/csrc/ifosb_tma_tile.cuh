@@ -15,7 +15,7 @@ static_assert(RSLOT % 32 == 0 && VS_PT % 32 == 0 && VS_MOD % 32 == 0 && VS_SP % 
 constexpr int NTHR = 32 * (TX + 1);          // TX consumer warps + 1 producer warp
 
 __host__ __device__ constexpr size_t vel_tma_smem() {
-    return sizeof(float) * ((size_t)RING * RSLOT + NSTAGE * (size_t)VS_SP) + 8 * NBAR;
+    return sizeof(float) * ((size_t)VRING * RSLOT + VNSTAGE * (size_t)VS_SP) + 8 * VNBAR;
 }
 // Stress stage: [sigma + memory variables: nsr][model: nm][DFT: ndf] boxes of PT
 // floats per field, each box start rounded up to 32 floats.
@@ -27,18 +27,20 @@ __host__ __device__ inline size_t str_tma_smem(int nsr, int nm, int ndf) {
 }
 
 // CTA start: returns false (for every thread) if an earlier CTA reported a timeout.
+// NR ring slots and NS stages: barriers [full ring | empty ring | full stage | empty stage].
+template <int NR, int NS>
 __device__ __forceinline__ bool pipeline_start(uint64_t *bar, const int *err) {
     __shared__ int s_go;
     if (threadIdx.x == 0 && threadIdx.y == TX) {
         s_go = *(volatile const int *)err == 0;
         if (s_go) {
-            for (int q = 0; q < RING; ++q) {
+            for (int q = 0; q < NR; ++q) {
                 mbar_init(&bar[q], 1);             // full ring slot
-                mbar_init(&bar[RING + q], TX);     // empty ring slot
+                mbar_init(&bar[NR + q], TX);       // empty ring slot
             }
-            for (int b = 0; b < NSTAGE; ++b) {
-                mbar_init(&bar[2 * RING + b], 1);            // full stage
-                mbar_init(&bar[2 * RING + NSTAGE + b], TX);  // empty stage
+            for (int b = 0; b < NS; ++b) {
+                mbar_init(&bar[2 * NR + b], 1);        // full stage
+                mbar_init(&bar[2 * NR + NS + b], TX);  // empty stage
             }
             asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         }
@@ -61,11 +63,12 @@ __device__ __forceinline__ bool consumer_wait(uint64_t *bar, int it, int j, int 
 }
 
 // Consumer hands back the ring plane j-2 and/or the stage of iteration `it`.
+template <int NR = RING, int NS = NSTAGE>
 __device__ __forceinline__ void consumer_release(uint64_t *bar, int it, bool ring_slot, bool stage) {
     __syncwarp();
     if (threadIdx.x == 0) {
-        if (ring_slot) mbar_arrive(&bar[RING + it % RING]);
-        if (stage) mbar_arrive(&bar[2 * RING + NSTAGE + it % NSTAGE]);
+        if (ring_slot) mbar_arrive(&bar[NR + it % NR]);
+        if (stage) mbar_arrive(&bar[2 * NR + NS + it % NS]);
     }
 }
 
@@ -106,15 +109,15 @@ __device__ __forceinline__ void vel_rows(const VelTma &T, int nt, const float *r
             for (int r = 0; r < 5; ++r) ok &= mbar_wait(&bar[r], 0);
         } else {
             ok &= mbar_wait(&bar[wslot], wpar);
-            if (++wslot == RING) { wslot = 0; wpar ^= 1; }
+            if (++wslot == VRING) { wslot = 0; wpar ^= 1; }
         }
-        ok &= mbar_wait(&bar[2 * RING + it % NSTAGE], (it / NSTAGE) & 1);
+        ok &= mbar_wait(&bar[2 * VRING + it % VNSTAGE], (it / VNSTAGE) & 1);
         if (!ok) { if (tz == 0) atomicExch(T.tma_err, 1); return; }
         // everything this row needs from the stage, so the stage can go back at once
         float sxx_x = 0.f, sxz_z = 0.f, szz_z = 0.f, sxz_x = 0.f;
         float vxo = 0.f, vyo = 0.f, vzo = 0.f, rip = 1.f, rjp = 1.f, rkp = 1.f;
         if (active) {
-            const float *stage = stg + (it % NSTAGE) * SP;
+            const float *stage = stg + (it % VNSTAGE) * SP;
             const float *Ip = stage + cx * RZ + cz;
             // stage in-plane fields: 0 sxx, 1 szz, 2 sxz
 #define IP(f, x, z) Ip[(f) * RPLANE + (x) * RZ + (z)]
@@ -127,7 +130,7 @@ __device__ __forceinline__ void vel_rows(const VelTma &T, int nt, const float *r
             vxo = pv[0]; vyo = pv[PT]; vzo = pv[2 * PT];
             rip = pm[0]; rjp = pm[PT]; rkp = pm[2 * PT];
         }
-        consumer_release(bar, it, false, true);
+        consumer_release<VRING, VNSTAGE>(bar, it, false, true);
         if (active) {
             // ring fields: 0 syy, 1 sxy, 2 syz
 #define RF(Rp, f, x, z) Rp[(f) * RPLANE + (x) * RZ + (z)]
@@ -142,24 +145,24 @@ __device__ __forceinline__ void vel_rows(const VelTma &T, int nt, const float *r
             if (XZ && hx) {
                 float *p = ps + sxi(g, j, hx, k);
                 const long long o = a.sl.sx;
-                float v0 = CP(BH_X, hx) * q.x[0] + CP(AH_X, hx) * sxx_x; p[0] = v0; sxx_x = sxx_x / CP(KH_X, hx) + v0;
-                float v1 = CP(B_X, hx) * q.x[1] + CP(A_X, hx) * sxy_x; p[o] = v1; sxy_x = sxy_x / CP(K_X, hx) + v1;
-                float v2 = CP(B_X, hx) * q.x[2] + CP(A_X, hx) * sxz_x; p[2 * o] = v2; sxz_x = sxz_x / CP(K_X, hx) + v2;
+                float v0 = CP(BH_X, hx) * q.x[0] + CP(AH_X, hx) * sxx_x; p[0] = v0; sxx_x = div_rn(sxx_x, CP(KH_X, hx)) + v0;
+                float v1 = CP(B_X, hx) * q.x[1] + CP(A_X, hx) * sxy_x; p[o] = v1; sxy_x = div_rn(sxy_x, CP(K_X, hx)) + v1;
+                float v2 = CP(B_X, hx) * q.x[2] + CP(A_X, hx) * sxz_x; p[2 * o] = v2; sxz_x = div_rn(sxz_x, CP(K_X, hx)) + v2;
             }
             if (hy) {
                 float *p = ps + 3 * a.sl.sx + syi(g, hy, i, k);
                 const long long o = a.sl.sy;
-                float v0 = CP(B_Y, hy) * q.y[0] + CP(A_Y, hy) * sxy_y; p[0] = v0; sxy_y = sxy_y / CP(K_Y, hy) + v0;
-                float v1 = CP(BH_Y, hy) * q.y[1] + CP(AH_Y, hy) * syy_y; p[o] = v1; syy_y = syy_y / CP(KH_Y, hy) + v1;
-                float v2 = CP(B_Y, hy) * q.y[2] + CP(A_Y, hy) * syz_y; p[2 * o] = v2; syz_y = syz_y / CP(K_Y, hy) + v2;
+                float v0 = CP(B_Y, hy) * q.y[0] + CP(A_Y, hy) * sxy_y; p[0] = v0; sxy_y = div_rn(sxy_y, CP(K_Y, hy)) + v0;
+                float v1 = CP(BH_Y, hy) * q.y[1] + CP(AH_Y, hy) * syy_y; p[o] = v1; syy_y = div_rn(syy_y, CP(KH_Y, hy)) + v1;
+                float v2 = CP(B_Y, hy) * q.y[2] + CP(A_Y, hy) * syz_y; p[2 * o] = v2; syz_y = div_rn(syz_y, CP(K_Y, hy)) + v2;
             }
             if (XZ && hz) {
                 float *p = ps + 3 * a.sl.sx + 3 * a.sl.sy + szi(g, j, i, hz);
                 const long long o = a.sl.sz;
                 const float *cg = a.cpg;
-                float v0 = CPG(cg, B_Z, hz) * q.z[0] + CPG(cg, A_Z, hz) * sxz_z; p[0] = v0; sxz_z = sxz_z / CPG(cg, K_Z, hz) + v0;
-                float v1 = CPG(cg, B_Z, hz) * q.z[1] + CPG(cg, A_Z, hz) * syz_z; p[o] = v1; syz_z = syz_z / CPG(cg, K_Z, hz) + v1;
-                float v2 = CPG(cg, BH_Z, hz) * q.z[2] + CPG(cg, AH_Z, hz) * szz_z; p[2 * o] = v2; szz_z = szz_z / CPG(cg, KH_Z, hz) + v2;
+                float v0 = CPG(cg, B_Z, hz) * q.z[0] + CPG(cg, A_Z, hz) * sxz_z; p[0] = v0; sxz_z = div_rn(sxz_z, CPG(cg, K_Z, hz)) + v0;
+                float v1 = CPG(cg, B_Z, hz) * q.z[1] + CPG(cg, A_Z, hz) * syz_z; p[o] = v1; syz_z = div_rn(syz_z, CPG(cg, K_Z, hz)) + v1;
+                float v2 = CPG(cg, BH_Z, hz) * q.z[2] + CPG(cg, AH_Z, hz) * szz_z; p[2 * o] = v2; szz_z = div_rn(szz_z, CPG(cg, KH_Z, hz)) + v2;
             }
             // the next plane's PML memory, a plane ahead of its use
             if (j < j1 && (hx || hz || face_y(g, j + 1))) psi_load(q, ps, a.sl, g, j + 1, i, k, hx, hz);
@@ -168,22 +171,22 @@ __device__ __forceinline__ void vel_rows(const VelTma &T, int nt, const float *r
                 const long long c = V - st;
                 V[VX * F] = vxo; V[VY * F] = vyo; V[VZ * F] = vzo;
                 if (frame) vel_points<BACK>(a, st, p0, p1, j, i, k, nt, c);
-                V[VX * F] = V[VX * F] + (sxx_x + sxy_y + sxz_z) / rip;
-                V[VY * F] = V[VY * F] + (syy_y + sxy_x + syz_z) / rjp;
-                V[VZ * F] = V[VZ * F] + (szz_z + sxz_x + syz_y) / rkp;
+                V[VX * F] = V[VX * F] + div_rn(sxx_x + sxy_y + sxz_z, rip);
+                V[VY * F] = V[VY * F] + div_rn(syy_y + sxy_x + syz_z, rjp);
+                V[VZ * F] = V[VZ * F] + div_rn(szz_z + sxz_x + syz_y, rkp);
                 const int passes = frame ? (BACK ? 1 : 0) : (BACK ? 2 : 1);
                 for (int pass = 0; pass < passes; ++pass) vel_points<BACK>(a, st, p0, p1, j, i, k, nt, c);
             } else {
-                V[VX * F] = vxo + (sxx_x + sxy_y + sxz_z) / rip;
-                V[VY * F] = vyo + (syy_y + sxy_x + syz_z) / rjp;
-                V[VZ * F] = vzo + (szz_z + sxz_x + syz_y) / rkp;
+                V[VX * F] = vxo + div_rn(sxx_x + sxy_y + sxz_z, rip);
+                V[VY * F] = vyo + div_rn(syy_y + sxy_x + syz_z, rjp);
+                V[VZ * F] = vzo + div_rn(szz_z + sxz_x + syz_y, rkp);
             }
             if (j == probe_j && isnan(V[VY * F])) atomicMin(a.err_step + s, nt);
         }
-        consumer_release(bar, it, true, false);
+        consumer_release<VRING, VNSTAGE>(bar, it, true, false);
         // planes move down one slot; the plane loaded into slot nslot becomes j+2
         Rm2 = Rm1; Rm1 = R0; R0 = Rp1; Rp1 = Rp2; Rp2 = Rb + nslot * RSLOT;
-        if (++nslot == RING) nslot = 0;
+        if (++nslot == VRING) nslot = 0;
     }
 }
 
@@ -201,22 +204,22 @@ __global__ void __launch_bounds__(NTHR, 3) k_velocity_tma(const __grid_constant_
     const int n = j1 - j0 + 1;
     float *ring = reinterpret_cast<float *>(smem);
     constexpr int SP = VS_SP;
-    float *stg = ring + RING * RSLOT;
-    uint64_t *bar = reinterpret_cast<uint64_t *>(stg + NSTAGE * SP);
+    float *stg = ring + VRING * RSLOT;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(stg + VNSTAGE * SP);
     const int rfirst = j0 - 2, rlast = j1 + 2;
-    if (!pipeline_start(bar, T.tma_err)) return;
+    if (!pipeline_start<VRING, VNSTAGE>(bar, T.tma_err)) return;
 
     if (tx == TX) {  // ---------------- producer warp
         if (tz != 0) return;
         auto ring_load = [&](int P) {
-            const int sl = (P - rfirst) % RING;
+            const int sl = (P - rfirst) % VRING;
             mbar_expect_tx(&bar[sl], 3 * RPLANE * 4);
             tma_load5(ring + sl * RSLOT, &T.m_halo, zc(k0) - HZ, xc(i0) - HX, yc_(P), SYY, s, &bar[sl]);
         };
         auto stage_load = [&](int it) {
-            const int j = j0 + it, b = it % NSTAGE;
+            const int j = j0 + it, b = it % VNSTAGE;
             float *d = stg + b * SP;
-            uint64_t *fb = &bar[2 * RING + b];
+            uint64_t *fb = &bar[2 * VRING + b];
             mbar_expect_tx(fb, (3 * RPLANE + 6 * PT) * 4);
             tma_load5(d, &T.m_halo, zc(k0) - HZ, xc(i0) - HX, yc_(j), SXX, s, fb);
             tma_load5(d + VS_PT, &T.m_pt, zc(k0), xc(i0), yc_(j), VX, s, fb);
@@ -229,25 +232,25 @@ __global__ void __launch_bounds__(NTHR, 3) k_velocity_tma(const __grid_constant_
             tma_prefetch4(&T.m_mod, zc(k0), xc(i0), yc_(j), MD_RIP);
         };
         auto ring_prefetch = [&](int P) { tma_prefetch5(&T.m_halo, zc(k0) - HZ, xc(i0) - HX, yc_(P), SYY, s); };
-        for (int P = rfirst; P <= min(rfirst + RING - 1, rlast); ++P) ring_load(P);
-        for (int it = 0; it < NSTAGE && it < n; ++it) stage_load(it);
+        for (int P = rfirst; P <= min(rfirst + VRING - 1, rlast); ++P) ring_load(P);
+        for (int it = 0; it < VNSTAGE && it < n; ++it) stage_load(it);
         for (int q = 0; q < T.l2ahead; ++q) {
-            if (NSTAGE + q < n) stage_prefetch(NSTAGE + q);
-            if (rfirst + RING + q <= rlast) ring_prefetch(rfirst + RING + q);
+            if (VNSTAGE + q < n) stage_prefetch(VNSTAGE + q);
+            if (rfirst + VRING + q <= rlast) ring_prefetch(rfirst + VRING + q);
         }
         for (int it = 0; it < n; ++it) {
-            if (rfirst + it + RING <= rlast) {
-                if (!mbar_wait(&bar[RING + it % RING], (it / RING) & 1)) { atomicExch(T.tma_err, 1); return; }
-                ring_load(rfirst + it + RING);
-                if (T.l2ahead > 0 && rfirst + it + RING + T.l2ahead <= rlast) ring_prefetch(rfirst + it + RING + T.l2ahead);
+            if (rfirst + it + VRING <= rlast) {
+                if (!mbar_wait(&bar[VRING + it % VRING], (it / VRING) & 1)) { atomicExch(T.tma_err, 1); return; }
+                ring_load(rfirst + it + VRING);
+                if (T.l2ahead > 0 && rfirst + it + VRING + T.l2ahead <= rlast) ring_prefetch(rfirst + it + VRING + T.l2ahead);
             }
-            if (it + NSTAGE < n) {
-                if (!mbar_wait(&bar[2 * RING + NSTAGE + it % NSTAGE], (it / NSTAGE) & 1)) {
+            if (it + VNSTAGE < n) {
+                if (!mbar_wait(&bar[2 * VRING + VNSTAGE + it % VNSTAGE], (it / VNSTAGE) & 1)) {
                     atomicExch(T.tma_err, 1);
                     return;
                 }
-                stage_load(it + NSTAGE);
-                if (T.l2ahead > 0 && it + NSTAGE + T.l2ahead < n) stage_prefetch(it + NSTAGE + T.l2ahead);
+                stage_load(it + VNSTAGE);
+                if (T.l2ahead > 0 && it + VNSTAGE + T.l2ahead < n) stage_prefetch(it + VNSTAGE + T.l2ahead);
             }
         }
         return;
@@ -286,7 +289,7 @@ __global__ void __maxnreg__(L == 0 ? STR_REGS_ELASTIC : STR_REGS_MECH) k_stress_
     float *stg = ring + RING * RSLOT;
     uint64_t *bar = reinterpret_cast<uint64_t *>(stg + NSTAGE * SP);
     const int rfirst = j0 - 2, rlast = j1 + 2;
-    if (!pipeline_start(bar, T.tma_err)) return;
+    if (!pipeline_start<RING, NSTAGE>(bar, T.tma_err)) return;
 
     if (tx == TX) {  // ---------------- producer warp
         if (tz != 0) return;
@@ -378,16 +381,16 @@ __global__ void __maxnreg__(L == 0 ? STR_REGS_ELASTIC : STR_REGS_MECH) k_stress_
             if (hx) {
                 float *p = ps + sxi(g, j, hx, k);
                 const long long o = a.sl.sx;
-                float v0 = CP(B_X, hx) * q.x[0] + CP(A_X, hx) * vxx; p[0] = v0; vxx = vxx / CP(K_X, hx) + v0;
-                float v1 = CP(BH_X, hx) * q.x[1] + CP(AH_X, hx) * vyx; p[o] = v1; vyx = vyx / CP(KH_X, hx) + v1;
-                float v2 = CP(BH_X, hx) * q.x[2] + CP(AH_X, hx) * vzx; p[2 * o] = v2; vzx = vzx / CP(KH_X, hx) + v2;
+                float v0 = CP(B_X, hx) * q.x[0] + CP(A_X, hx) * vxx; p[0] = v0; vxx = div_rn(vxx, CP(K_X, hx)) + v0;
+                float v1 = CP(BH_X, hx) * q.x[1] + CP(AH_X, hx) * vyx; p[o] = v1; vyx = div_rn(vyx, CP(KH_X, hx)) + v1;
+                float v2 = CP(BH_X, hx) * q.x[2] + CP(AH_X, hx) * vzx; p[2 * o] = v2; vzx = div_rn(vzx, CP(KH_X, hx)) + v2;
             }
             if (hy) {
                 float *p = ps + 3 * a.sl.sx + syi(g, hy, i, k);
                 const long long o = a.sl.sy;
-                float v0 = CP(BH_Y, hy) * q.y[0] + CP(AH_Y, hy) * vxy; p[0] = v0; vxy = vxy / CP(KH_Y, hy) + v0;
-                float v1 = CP(B_Y, hy) * q.y[1] + CP(A_Y, hy) * vyy; p[o] = v1; vyy = vyy / CP(K_Y, hy) + v1;
-                float v2 = CP(BH_Y, hy) * q.y[2] + CP(AH_Y, hy) * vzy; p[2 * o] = v2; vzy = vzy / CP(KH_Y, hy) + v2;
+                float v0 = CP(BH_Y, hy) * q.y[0] + CP(AH_Y, hy) * vxy; p[0] = v0; vxy = div_rn(vxy, CP(KH_Y, hy)) + v0;
+                float v1 = CP(B_Y, hy) * q.y[1] + CP(A_Y, hy) * vyy; p[o] = v1; vyy = div_rn(vyy, CP(K_Y, hy)) + v1;
+                float v2 = CP(BH_Y, hy) * q.y[2] + CP(AH_Y, hy) * vzy; p[2 * o] = v2; vzy = div_rn(vzy, CP(KH_Y, hy)) + v2;
             }
             if (hz) {
                 // the reference divides by K_y on the front z face (update_s_ssg_CPML_elastic.c:104-108)
@@ -396,9 +399,9 @@ __global__ void __maxnreg__(L == 0 ? STR_REGS_ELASTIC : STR_REGS_MECH) k_stress_
                 const float *cg = a.cpg;
                 const float kh = zfront ? CPG(cg, KH_Y, hz) : CPG(cg, KH_Z, hz);
                 const float kf = zfront ? CPG(cg, K_Y, hz) : CPG(cg, K_Z, hz);
-                float v0 = CPG(cg, BH_Z, hz) * q.z[0] + CPG(cg, AH_Z, hz) * vxz; p[0] = v0; vxz = vxz / kh + v0;
-                float v1 = CPG(cg, BH_Z, hz) * q.z[1] + CPG(cg, AH_Z, hz) * vyz; p[o] = v1; vyz = vyz / kh + v1;
-                float v2 = CPG(cg, B_Z, hz) * q.z[2] + CPG(cg, A_Z, hz) * vzz; p[2 * o] = v2; vzz = vzz / kf + v2;
+                float v0 = CPG(cg, BH_Z, hz) * q.z[0] + CPG(cg, AH_Z, hz) * vxz; p[0] = v0; vxz = div_rn(vxz, kh) + v0;
+                float v1 = CPG(cg, BH_Z, hz) * q.z[1] + CPG(cg, AH_Z, hz) * vyz; p[o] = v1; vyz = div_rn(vyz, kh) + v1;
+                float v2 = CPG(cg, B_Z, hz) * q.z[2] + CPG(cg, A_Z, hz) * vzz; p[2 * o] = v2; vzz = div_rn(vzz, kf) + v2;
             }
             // the next plane's PML memory, a plane ahead of its use
             if (j < j1 && (hx || hz || face_y(g, j + 1))) psi_load(q, ps, a.sl, g, j + 1, i, k, hx, hz);

@@ -94,6 +94,7 @@ def lib():
             "ifosb_kernel_times": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int)]),
             "ifosb_set_stream": (C.c_int, [vp, vp]),
             "ifosb_autotune": (C.c_int, [vp, C.c_int, C.POINTER(Shot), C.c_int, vp]),
+            "ifosb_set_launch_shape": (C.c_int, [vp, C.c_int, vp]),
             "ifosb_residual_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_float, vp, vp, vp, vp, vp]),
             "ifosb_optim_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(vp)]),
             "ifosb_optim_destroy": (None, [vp]),
@@ -125,7 +126,7 @@ def exported_symbols():
         "ifosb_adjoint", "ifosb_gradient", "ifosb_zero_gradient", "ifosb_get_gradient", "ifosb_shot_gradient",
         "ifosb_get_field", "ifosb_set_launch_mode", "ifosb_last_launch_count", "ifosb_graph_captures", "ifosb_cpml_coeff",
         "ifosb_wavelet", "ifosb_nsamples", "ifosb_moduli", "ifosb_set_profiling", "ifosb_kernel_times",
-        "ifosb_set_stream", "ifosb_autotune", "ifosb_residual_noalloc", "ifosb_optim_create", "ifosb_optim_destroy",
+        "ifosb_set_stream", "ifosb_autotune", "ifosb_set_launch_shape", "ifosb_residual_noalloc", "ifosb_optim_create", "ifosb_optim_destroy",
         "ifosb_optim_last_error", "ifosb_conjugate", "ifosb_lbfgs_savegrad", "ifosb_lbfgs", "ifosb_modelupdate",
         "ifosb_lbfgs_history", "ifosb_steplength", "ifosb_precon_grad", "ifosb_constant_boundary",
     ]
@@ -306,6 +307,14 @@ class Engine:
         self._c(lib().ifosb_autotune(self.h, len(shots), arr, steps, _p(shape)))
         return {"velocity": {"y_planes_per_cta": int(shape[0]), "l2_prefetch_planes": int(shape[1])},
                 "stress": {"y_planes_per_cta": int(shape[2]), "l2_prefetch_planes": int(shape[3])}}
+
+    def set_launch_shape(self, nshots, shape):
+        """shape: the dict autotune() returns, or [cy_vel, l2_vel, cy_str, l2_str]."""
+        if isinstance(shape, dict):
+            shape = [shape["velocity"]["y_planes_per_cta"], shape["velocity"]["l2_prefetch_planes"],
+                     shape["stress"]["y_planes_per_cta"], shape["stress"]["l2_prefetch_planes"]]
+        arr = np.ascontiguousarray(shape, np.int32)
+        self._c(lib().ifosb_set_launch_shape(self.h, nshots, _p(arr)))
 
     def residual(self, obs, want_l2_ref=False):
         obs = _f32(obs)

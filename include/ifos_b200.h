@@ -174,6 +174,10 @@ int ifosb_kernel_times(const ifosb_engine *e, double *vel_ms, double *str_ms, in
  * kernel planes per chunk and prefetch distance, then the stress kernel's. */
 int ifosb_autotune(ifosb_engine *e, int nshots, const ifosb_shot *shots, int steps, int *shape);
 
+/* Sets the launch shapes for batches of nshots shots directly (the int[4] that
+ * ifosb_autotune reports), e.g. a shape tuned in an earlier run. */
+int ifosb_set_launch_shape(ifosb_engine *e, int nshots, const int *shape);
+
 /* Run the engine's work on the caller's CUDA stream (a cudaStream_t passed as
  * void*; NULL = the engine's own stream). Calls stay synchronous at return. */
 int ifosb_set_stream(ifosb_engine *e, void *stream);

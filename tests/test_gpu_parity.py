@@ -210,6 +210,28 @@ def test_autotuned_launch_shape_gives_the_same_bits():
     assert np.array_equal(out[0][2], out[1][2])
 
 
+def test_set_launch_shape_reuses_a_tuned_shape():
+    """A shape set directly (as a caller that saved an autotuned shape would)
+    gives the same bits as the default shape, including odd chunk lengths and
+    prefetch off; out-of-range shapes are rejected with a message."""
+    import ifosb
+    c = synth.small_case(nx=37, ny=70, nz=45, nt=40, fw=6, nshots=3, seed=19)
+    e1, m, cp, shots = engine_for(c)
+    e2, _, _, _ = engine_for(c)
+    e2.set_launch_shape(len(shots), [5, 0, 7, 2])
+    out = []
+    for e in (e1, e2):
+        sec = e.forward(shots)
+        obs = (sec * np.float32(0.9)).astype(np.float32)
+        mis = e.shot_gradient(shots, obs)
+        out.append((sec, mis, e.get_gradient()))
+    for a, b in zip(out[0], out[1]):
+        assert np.array_equal(a, b)
+    for bad in ([0, 1, 4, 1], [4, 9, 4, 1], [4, 1, 71, 1], [4, 1, 4, -1]):
+        with pytest.raises(ifosb.IfosbError):
+            e2.set_launch_shape(len(shots), bad)
+
+
 @pytest.mark.parametrize("rows", [7, 8])
 @pytest.mark.parametrize("nmech", [0, 3])
 def test_tile_heights_match(rows, nmech, oracle, request, monkeypatch):
