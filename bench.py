@@ -378,6 +378,8 @@ def main():
     ach_step = b["total"] * ncell / ((tv + ts) / nsteps / 1000.0) / 1e9
     ach_str = b["stress"] * ncell / (ts / nsteps / 1000.0) / 1e9
     ach_vel = b["vel"] * ncell / (tv / nsteps / 1000.0) / 1e9
+    # DRAM bytes per launch from an ncu capture of the same kernels (committed
+    # summary); null when no capture of this workload exists
     traffic = None
     tf = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tf):
@@ -388,11 +390,14 @@ def main():
     roofline = {"bound": "hbm", "kernel": "time step = k_velocity + k_stress<L> (one launch each)",
                 "achieved": round(ach_step, 1), "peak": peak, "unit": "GB/s", "frac": round(ach_step / peak, 4),
                 "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
-                "traffic": traffic, "alg_bytes_per_cell_step": round(b["total"], 2),
+                "traffic": traffic["time_step"] if traffic else None,
+                "alg_bytes_per_step": round(b["total"] * ncell), "alg_bytes_per_cell_step": round(b["total"], 2),
                 "per_kernel": {"k_stress": {"alg_bytes_per_cell": round(b["stress"], 2), "ms": round(ts / nsteps, 4),
-                                            "achieved_gbs": round(ach_str, 1), "frac": round(ach_str / peak, 4)},
+                                            "achieved_gbs": round(ach_str, 1), "frac": round(ach_str / peak, 4),
+                                            "traffic": traffic["k_stress"] if traffic else None},
                                "k_velocity": {"alg_bytes_per_cell": round(b["vel"], 2), "ms": round(tv / nsteps, 4),
-                                              "achieved_gbs": round(ach_vel, 1), "frac": round(ach_vel / peak, 4)}}}
+                                              "achieved_gbs": round(ach_vel, 1), "frac": round(ach_vel / peak, 4),
+                                              "traffic": traffic["k_velocity"] if traffic else None}}}
 
     out = {
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
