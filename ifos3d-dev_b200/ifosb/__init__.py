@@ -18,9 +18,9 @@ import numpy as np
 PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LIB_PATH = os.path.join(PKG_DIR, "lib", "libifos_b200.so")
 
-OK, EARG, ECUDA, ENOMEM, EUNSTABLE, ESTATE, ENODEV, ETOOBIG = 0, 1, 2, 3, 4, 5, 6, 7
+OK, EARG, ECUDA, ENOMEM, EUNSTABLE, ESTATE, ENODEV, ETOOBIG, EIO = 0, 1, 2, 3, 4, 5, 6, 7, 8
 _NAMES = {EARG: "EARG", ECUDA: "ECUDA", ENOMEM: "ENOMEM", EUNSTABLE: "EUNSTABLE", ESTATE: "ESTATE", ENODEV: "ENODEV",
-          ETOOBIG: "ETOOBIG"}
+          ETOOBIG: "ETOOBIG", EIO: "EIO"}
 NOALLOC_MAX_TRACES = 65536
 
 F_VX, F_VY, F_VZ, F_SXX, F_SYY, F_SZZ, F_SXY, F_SYZ, F_SXZ = range(9)
@@ -109,6 +109,16 @@ def lib():
             "ifosb_constant_boundary": (C.c_int, [vp, vp, vp, vp, C.c_int]),
             "ifosb_precon_grad": (C.c_int, [vp, vp, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float,
                                             C.c_int, vp, C.c_int, vp]),
+            "ifosb_write_seis": (C.c_int, [C.c_char_p, C.c_int, vp, C.c_int, C.c_int, vp, vp, vp, C.c_float,
+                                           C.c_float, C.c_float, C.c_int, C.c_float, C.c_int, C.c_int]),
+            "ifosb_merge_seis": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(C.c_char_p), C.c_int,
+                                           C.POINTER(C.c_int)]),
+            "ifosb_read_seis": (C.c_int, [C.c_char_p, vp, C.c_int, C.c_int]),
+            "ifosb_read_seis_split": (C.c_int, [C.c_char_p, vp, C.c_int, vp, C.c_int]),
+            "ifosb_write_model": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp, vp, C.c_int,
+                                            C.c_int, C.c_int, C.c_int]),
+            "ifosb_write_gradient": (C.c_int, [C.c_char_p, C.c_float, C.c_int, C.c_int, C.c_int, C.c_int, vp,
+                                               C.c_int, C.c_int, C.c_int, C.c_int]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -129,6 +139,8 @@ def exported_symbols():
         "ifosb_set_stream", "ifosb_autotune", "ifosb_set_launch_shape", "ifosb_residual_noalloc", "ifosb_optim_create", "ifosb_optim_destroy",
         "ifosb_optim_last_error", "ifosb_conjugate", "ifosb_lbfgs_savegrad", "ifosb_lbfgs", "ifosb_modelupdate",
         "ifosb_lbfgs_history", "ifosb_steplength", "ifosb_precon_grad", "ifosb_constant_boundary",
+        "ifosb_write_seis", "ifosb_merge_seis", "ifosb_read_seis", "ifosb_read_seis_split",
+        "ifosb_write_model", "ifosb_write_gradient",
     ]
 
 

@@ -8,6 +8,10 @@ One iteration of src/ifos3d.c:669-1148, in its order:
   two test steps: modelupdate on a copy, forwards of NSHOTS_STEP
   shots, misfits                                                   :1021-1129
   steplength (parabola), modelupdate of the model                   :1133-1138
+With Settings.grad_file / mod_out_file set, the gradient and model files of
+:1000 (raw), :1006 (+1000, preconditioned), :1016 (+2000, search direction) and
+:1141 (model after the update; iteration 0 at :547) are written in the
+reference's format (ifosb.io).
 The differences are the ones the engine makes everywhere: shots run in batches,
 misfits are summed in FP64, and the optimiser's dot products and the step-length
 parabola are FP64. Models are the ghosted [NY+2][NX+2][NZ+2] rho, pi, u arrays of
@@ -20,6 +24,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import Engine, Optimizer, Params, steplength
+from . import io as fio
 
 
 @dataclass
@@ -42,6 +47,9 @@ class Settings:
     nshots_step: int = 1           # NSHOTS_STEP (shots of the step-length test forwards)
     tast: int = 100                # TAST (DFT sampling: ntast = 1 / (f_max TAST DT))
     max_batch: int = 4             # shots per engine launch
+    grad_file: str | None = None   # GRAD_FILE: gradients written per iteration (outgrad)
+    mod_out_file: str | None = None  # MOD_OUT_FILE: models written per iteration (outmod)
+    ids: tuple = (1, 1, 1)         # IDX, IDY, IDZ of the merged model/gradient files
 
 
 @dataclass
@@ -66,8 +74,19 @@ class Inversion:
         self.step = np.zeros(5, np.float64)    # step[0..4] (vector(0,4): zeros)
         self.stage_i, self.it_group, self.itmax, self.iteration = -1, 0, 0, 0
         self.hist = History()
+        if cfg.mod_out_file:
+            self._write_model(0)
 
     # -- helpers --------------------------------------------------------------
+    def _write_model(self, iteration):
+        i = self.cfg.ids
+        fio.write_model(self.cfg.mod_out_file, iteration, *self.model, ghosted=True, idx=i[0], idy=i[1], idz=i[2])
+
+    def _write_grad(self, g, iteration):
+        if self.cfg.grad_file:
+            i = self.cfg.ids
+            fio.write_gradient(self.cfg.grad_file, float(self.finv[0]), iteration, g, idx=i[0], idy=i[1], idz=i[2])
+
     def _set_model(self, m):
         self.eng.set_model(*(a[1:-1, 1:-1, 1:-1] for a in m), None, None, None)
 
@@ -112,7 +131,9 @@ class Inversion:
         L2 = np.zeros(4, np.float64)
         L2[0] = float(np.sum(mis[self._test_shots()]))
         g = self.eng.get_gradient()
+        self._write_grad(g, self.iteration)
         self.opt.precon_grad(g, cfg.damptype, p.free_surf, p.fw, (p.dx, p.dy, p.dz), self.srcpos_m, self.recpos)
+        self._write_grad(g, self.iteration + 1000)
         beta = None
         if cfg.lbfgs:
             if self.it_group > 1:
@@ -121,6 +142,7 @@ class Inversion:
                 self.opt.lbfgs_savegrad(g)
         else:
             beta = self.opt.conjugate(g, cdf)
+        self._write_grad(g, self.iteration + 2000)
         # step length: two test models
         for steptest in (1, 2):
             if cdf == 1:
@@ -135,6 +157,8 @@ class Inversion:
         steplength(L2, self.step, cfg.lbfgs, self.it_group, cfg.teststep)
         self.opt.modelupdate(g, *self.model, self.step[3], cfg.weight, cfg.vp0, cfg.vs0, cfg.rho0,
                              lbfgs=cfg.lbfgs, it_group=self.it_group)
+        if cfg.mod_out_file:
+            self._write_model(self.iteration)
         self.hist.misfit.append(L2[0])
         self.hist.step.append(float(self.step[3]))
         self.hist.beta.append(None if beta is None else beta.tolist())

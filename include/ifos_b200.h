@@ -296,6 +296,56 @@ int ifosb_steplength(double *L2, double *step, int lbfgs, int it_group, double t
 int ifosb_residual_noalloc(int nshots, int ntr, int ns, float dt, const float *d_syn, const float *d_obs,
                            float *d_diff, double *d_misfit, void *stream);
 
+/* ---- on-disk formats (host; the files IFOS3D writes and reads) ------------
+ * No engine and no GPU: plain C file IO in the host's byte order.
+ * Return IFOSB_OK, IFOSB_EARG or IFOSB_EIO (file cannot be opened or written). */
+#define IFOSB_EIO 8
+
+/* One component's seismograms in the reference's format, replacing outseis()
+ * (src/outseis.c:30-276; called from src/saveseis.c:76-81).
+ * section: [ntr][ns] float. rec: [ntr][3] global receiver grid indices (x, y, z),
+ * i.e. recpos[1..3][recpos_loc[4][t]]. trace_no: [ntr] trace numbers written to
+ * tracl (recpos_loc[4][t]); NULL = 1..ntr. src: the shot's source position in
+ * metres (x, y, z) or NULL = 0, as for nsrc != 1. comp is accepted for the
+ * reference's signature; it does not reach the file. fmt = SEIS_FORMAT: 0 or 1 SU
+ * (240-byte trace header + ns floats per trace), 2 ASCII (%e, one column per
+ * trace), 3 raw floats, byte-swapped when littlebig != 0 (LITTLEBIG). Header
+ * fields outseis() leaves unassigned (cdp, selev, swdep, trailing pad) are zero. */
+int ifosb_write_seis(const char *path, int comp, const float *section, int ntr, int ns, const int *rec,
+                     const int *trace_no, const float *src, float dx, float dy, float dz, int ndt, float dt, int fmt,
+                     int littlebig);
+
+/* Rank 0's merge of the ranks' SU files into one (src/saveseis.c:86-229): the
+ * whole traces (240 + 4 ns bytes each) of inputs[0..nin-1] in order; a missing
+ * input is skipped, an input whose size is not a whole number of traces
+ * contributes nothing. *ntr_out (may be NULL) = traces written. */
+int ifosb_merge_seis(const char *out, int nin, const char *const *inputs, int ns, int *ntr_out);
+
+/* Observed seismograms, replacing readseis() (src/readseis.c:25-69): ntr traces,
+ * each a 240-byte header (skipped) and ns floats, into section [ntr][ns]; samples
+ * past the end of the file read as 0. A missing file is IFOSB_EIO. */
+int ifosb_read_seis(const char *path, float *section, int ntr, int ns);
+
+/* readseis_split() (src/readseis_split.c:25-65): the traces t with keep[t] == 1
+ * (rnum_loc), packed in file order into section [count][ns]. */
+int ifosb_read_seis_split(const char *path, float *section, int ntr, const int *keep, int ns);
+
+/* Model files of outmod() + mergemod() for one rank (src/outmod.c:25-84,
+ * src/mergemod.c:25-80): "<base>.vp_it<iteration>", ".vs_it", ".rho_it", each
+ * [z][x][y] floats (y fastest), vp = sqrt(pi/rho), vs = sqrt(u/rho). rho, pi, u:
+ * [ny][nx][nz] (ghost = 0) or the reference's ghosted [ny+2][nx+2][nz+2]
+ * (ghost = 1). idx, idy, idz = IDX, IDY, IDZ: mergemod keeps the first
+ * ceil(NZ/IDZ)*ceil(NX/IDX)*ceil(NY/IDY) values of the full-resolution file,
+ * and so does this. */
+int ifosb_write_model(const char *base, int iteration, int nx, int ny, int nz, const float *rho, const float *pi,
+                      const float *u, int ghost, int idx, int idy, int idz);
+
+/* Gradient files of outgrad() + mergemod() (src/outgrad.c:25-85):
+ * "<base>.vp_<finv %4.2f>Hz_it<iteration>", ".vs_...", ".rho_..." from grad =
+ * [3][ny][nx][nz] (ghost = 0) or [3][ny+2][nx+2][nz+2] (ghost = 1). */
+int ifosb_write_gradient(const char *base, float finv, int iteration, int nx, int ny, int nz, const float *grad,
+                         int ghost, int idx, int idy, int idz);
+
 #ifdef __cplusplus
 }
 #endif

@@ -4,6 +4,7 @@ modelupdate) on a small elastic problem: with CG the FP64 misfit falls at every
 iteration (by 7 % over the first three updates). Over so few iterations the
 update is not yet aligned with the true anomaly, so no model-error claim is made."""
 import math
+import os
 
 import numpy as np
 import pytest
@@ -81,4 +82,33 @@ def test_free_surface_with_reference_damping_leaves_the_model():
     rho, pi, u = inv.model
     inner = (slice(2, NY - 1), slice(FW + 6, NX - FW - 4), slice(FW + 6, NZ - FW - 4))
     np.testing.assert_allclose(pi[inner], ghost[1][inner], rtol=1e-6, atol=0)
+    inv.close()
+
+
+def test_inversion_writes_reference_files(tmp_path):
+    """With GRAD_FILE and MOD_OUT_FILE set, an iteration writes the reference's
+    files: the model at iteration 0 and after the update, and the raw (it),
+    preconditioned (it+1000) and search-direction (it+2000) gradients, each
+    [z][x][y] float32. The written model is the driver's model."""
+    from ifosb import io as fio
+    p, cp, rec, shots, obs, srcpos_m, ghost, vp0, vpT = _problem(free_surf=0)
+    gf, mf = str(tmp_path / "grad"), str(tmp_path / "model")
+    cfg = Settings(teststep=0.02, damptype=2, nshots_step=4, max_batch=4, weight=(1.0, 0.0, 0.0),
+                   grad_file=gf, mod_out_file=mf)
+    inv = Inversion(p, cp, rec, shots, obs, srcpos_m, *ghost, [Stage([300.0, 450.0], 2)], cfg)
+    inv.run(1)
+    n = NX * NY * NZ * 4
+    for it in (1, 1001, 2001):
+        for q in ("vp", "vs", "rho"):
+            assert os.path.getsize(f"{gf}.{q}_300.00Hz_it{it}") == n
+    for it in (0, 1):
+        for q in ("vp", "vs", "rho"):
+            assert os.path.getsize(f"{mf}.{q}_it{it}") == n
+    again = str(tmp_path / "again")
+    fio.write_model(again, 1, *inv.model, ghosted=True)
+    assert open(f"{mf}.vp_it1", "rb").read() == open(f"{again}.vp_it1", "rb").read()
+    vp = np.fromfile(f"{mf}.vp_it0", np.float32).reshape(NZ, NX, NY).transpose(2, 1, 0)
+    assert np.allclose(vp, vp0, rtol=1e-6, atol=0)
+    g1 = np.fromfile(f"{gf}.vp_300.00Hz_it1", np.float32)
+    assert np.isfinite(g1).all() and np.any(g1 != 0)
     inv.close()
