@@ -119,6 +119,7 @@ def lib():
                                             C.c_int, C.c_int, C.c_int]),
             "ifosb_write_gradient": (C.c_int, [C.c_char_p, C.c_float, C.c_int, C.c_int, C.c_int, C.c_int, vp,
                                                C.c_int, C.c_int, C.c_int, C.c_int]),
+            "ifosb_filt_seis": (C.c_int, [vp, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int, C.c_int]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -140,7 +141,7 @@ def exported_symbols():
         "ifosb_optim_last_error", "ifosb_conjugate", "ifosb_lbfgs_savegrad", "ifosb_lbfgs", "ifosb_modelupdate",
         "ifosb_lbfgs_history", "ifosb_steplength", "ifosb_precon_grad", "ifosb_constant_boundary",
         "ifosb_write_seis", "ifosb_merge_seis", "ifosb_read_seis", "ifosb_read_seis_split",
-        "ifosb_write_model", "ifosb_write_gradient",
+        "ifosb_write_model", "ifosb_write_gradient", "ifosb_filt_seis",
     ]
 
 

@@ -25,6 +25,7 @@ import numpy as np
 
 from . import Engine, Optimizer, Params, steplength
 from . import io as fio
+from . import stages as fstages
 
 
 @dataclass
@@ -50,6 +51,8 @@ class Settings:
     grad_file: str | None = None   # GRAD_FILE: gradients written per iteration (outgrad)
     mod_out_file: str | None = None  # MOD_OUT_FILE: models written per iteration (outmod)
     ids: tuple = (1, 1, 1)         # IDX, IDY, IDZ of the merged model/gradient files
+    filt: bool = False             # FILT = 1: low-pass source signals and observed data at each
+                                   # stage's highest frequency (ifos3d.c:731, :840-855)
 
 
 @dataclass
@@ -59,10 +62,16 @@ class History:
     beta: list = field(default_factory=list)
 
 
+def stages_from_workflow(path: str, nstages: int) -> list:
+    """Stages of a workflow file (INV_FILE) read as readinv() reads them."""
+    return [Stage(list(w.finv), w.itmax) for w in fstages.read_workflow(path, nstages)]
+
+
 class Inversion:
     def __init__(self, p: Params, cpml, recpos, shots, obs, srcpos_m, rho, pi, u, stages, cfg: Settings):
         self.p, self.cfg, self.stages = p, cfg, list(stages)
-        self.shots, self.obs = list(shots), np.ascontiguousarray(obs, np.float32)
+        self.shots_raw, self.obs_raw = list(shots), np.ascontiguousarray(obs, np.float32)
+        self.shots, self.obs = self.shots_raw, self.obs_raw
         self.recpos = np.ascontiguousarray(recpos, np.int32)
         self.srcpos_m = np.ascontiguousarray(srcpos_m, np.float32)
         self.model = [np.ascontiguousarray(a, np.float32).copy() for a in (rho, pi, u)]
@@ -81,6 +90,13 @@ class Inversion:
     def _write_model(self, iteration):
         i = self.cfg.ids
         fio.write_model(self.cfg.mod_out_file, iteration, *self.model, ghosted=True, idx=i[0], idy=i[1], idz=i[2])
+
+    def _filter_stage(self, fc):
+        """FILT: the raw source signals and observed data low-passed at fc."""
+        dt = self.p.dt
+        self.shots = [(sp, fstages.filt_seis(sig, fc, dt)) for sp, sig in self.shots_raw]
+        o = self.obs_raw
+        self.obs = fstages.filt_seis(o.reshape(-1, o.shape[-1]), fc, dt).reshape(o.shape)
 
     def _write_grad(self, g, iteration):
         if self.cfg.grad_file:
@@ -118,6 +134,8 @@ class Inversion:
             self.finv = np.asarray(st.finv, np.float32)
             ntast = int(1.0 / (float(self.finv[-1]) * cfg.tast * p.dt)) or 1
             self.eng.set_frequencies(self.finv, ntast)
+            if cfg.filt:
+                self._filter_stage(float(self.finv[-1]))
             cdf, self.itmax, self.it_group = 1, st.itmax, 1
         else:
             cdf = 0

@@ -346,6 +346,16 @@ int ifosb_write_model(const char *base, int iteration, int nx, int ny, int nz, c
 int ifosb_write_gradient(const char *base, float finv, int iteration, int nx, int ny, int nz, const float *grad,
                          int ghost, int idx, int idy, int idz);
 
+/* ---- multiscale stages (host) ---------------------------------------------
+ * Time-domain Butterworth filter of FILT = 1, replacing filt_seis()
+ * (src/filt_seis.c:27-77, which calls libcseife's seife_lpb / seife_hpb): each of
+ * the ntr traces of data [ntr][ns] is filtered in place in double precision,
+ * corner frequency finv (the stage's highest frequency), sample interval dt,
+ * order `order` (the reference uses 4), low-pass (highpass = 0, the reference's
+ * method 1) or high-pass. As in the reference, the last sample of each trace
+ * is left unfiltered. */
+int ifosb_filt_seis(float *data, int ntr, int ns, float finv, float dt, int order, int highpass);
+
 #ifdef __cplusplus
 }
 #endif

@@ -167,3 +167,26 @@ int ifo_ref_outgrad(const char *base, float finv, int iteration, int nx, int ny,
     for (int c = 0; c < 3; ++c) free_f3tensor(G[c], 1, ny, 1, nx, 1, nz);
     return 0;
 }
+
+/* filt_seis (src/filt_seis.c) on data [ntr][ns] in place: FILT's Butterworth
+ * low-pass of order 4 through libcseife's seife_lpb. */
+extern float DT;
+int ifo_ref_filt_seis(float *data, int ntr, int ns, float finv, float dt) {
+    quiet();
+    DT = dt;
+    float **S = sec_mat(ntr, ns, data);
+    filt_seis(S, ntr, ns, finv);
+    for (int t = 1; t <= ntr; ++t) memcpy(data + (size_t)(t - 1) * ns, &S[t][1], sizeof(float) * ns);
+    free_matrix(S, 1, ntr > 0 ? ntr : 1, 1, ns);
+    return 0;
+}
+
+/* readinv (src/readinv.c) for stage `groupnum`: finv[nfmax], *nf, it[2]. */
+extern char INV_FILE[STRING_SIZE];
+int ifo_ref_readinv(const char *path, int groupnum, float *finv, int *nf, int *it, int nfmax) {
+    quiet();
+    snprintf(INV_FILE, STRING_SIZE, "%s", path);
+    int g = groupnum - 1;
+    readinv(finv, nf, &g, it, nfmax);
+    return g;
+}

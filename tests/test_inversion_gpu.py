@@ -112,3 +112,27 @@ def test_inversion_writes_reference_files(tmp_path):
     g1 = np.fromfile(f"{gf}.vp_300.00Hz_it1", np.float32)
     assert np.isfinite(g1).all() and np.any(g1 != 0)
     inv.close()
+
+
+def test_multiscale_workflow_with_filter(tmp_path):
+    """Two workflow stages (readinv format) with FILT: each stage low-passes the
+    raw source signals and observed data at its highest frequency, and the
+    driver moves to stage 2 after stage 1's itmax iterations."""
+    from ifosb import stages as fst
+    from ifosb.inversion import stages_from_workflow
+    p, cp, rec, shots, obs, srcpos_m, ghost, vp0, vpT = _problem(free_surf=0)
+    wf = tmp_path / "workflow.txt"
+    wf.write_text("1 1 0.01 0 0 0 0 0 1 250.0\n1 2 0.01 0 0 0 0 0 2 250.0 400.0\n")
+    st = stages_from_workflow(str(wf), 2)
+    assert [s.itmax for s in st] == [1, 2] and st[1].finv == [250.0, 400.0]
+    cfg = Settings(teststep=0.02, damptype=2, nshots_step=4, max_batch=4, weight=(1.0, 0.0, 0.0), filt=True)
+    inv = Inversion(p, cp, rec, shots, obs, srcpos_m, *ghost, st, cfg)
+    inv.iterate()
+    assert inv.stage_i == 0
+    assert np.array_equal(inv.obs, fst.filt_seis(obs.reshape(-1, obs.shape[-1]), 250.0, p.dt).reshape(obs.shape))
+    assert np.array_equal(inv.shots[0][1], fst.filt_seis(shots[0][1], 250.0, p.dt))
+    inv.iterate()
+    assert inv.stage_i == 1
+    assert np.array_equal(inv.obs, fst.filt_seis(obs.reshape(-1, obs.shape[-1]), 400.0, p.dt).reshape(obs.shape))
+    assert all(np.isfinite(inv.hist.misfit)) and all(s > 0 for s in inv.hist.step)
+    inv.close()
