@@ -91,6 +91,11 @@ struct ifosb_engine {
     int nt_limit = 0;
     long long captures = 0;  // time-loop graphs captured (a replay reuses one)
     float *d_mstage = nullptr;  // ifosb_set_model's staging of the raw model (5 ghosted fields)
+    // approximate Hessian: receivers' Green's-function DFT fields and the accumulated diagonal
+    float *d_green = nullptr; int ngreen = 0, cap_green = 0;
+    float *d_gsig = nullptr;   // [max_shots][3][NT] injection traces of a Green's-function batch
+    float *d_hess = nullptr;   // [3][NY][NX][NZ]
+    bool hess_fwd = false;     // d_dftf holds a forward batch not yet added to the Hessian
     // TMA staging (default) and its wait-timeout flag
     int use_tma = 1;
     int *d_tma_err = nullptr;
@@ -309,7 +314,7 @@ extern "C" void ifosb_destroy(ifosb_engine *e) {
     void *bufs[] = {e->d_state, e->d_psi, e->d_model, e->d_rho_w, e->d_dftf, e->d_dftb, e->d_grad, e->d_grad64,
                     e->d_err, e->d_sec, e->d_diff, e->d_obs, e->d_part, e->d_misfit, e->d_l2, e->d_trig_f,
                     e->d_trig_b, e->d_voff, e->d_soff, e->d_vpts, e->d_spts, e->d_amp, e->d_tma_err, e->d_cpg,
-                    e->d_mstage};
+                    e->d_mstage, e->d_green, e->d_gsig, e->d_hess};
     for (void *b : bufs)
         if (b) cudaFree(b);
     for (cudaEvent_t ev : e->events) cudaEventDestroy(ev);
@@ -375,6 +380,7 @@ extern "C" int ifosb_set_model(ifosb_engine *e, const float *rho, const float *p
     if (!e || !rho || !pi || !u) return IFOSB_EARG;
     const ifosb_params &p = e->p;
     if (p.nmech > 0 && (!taus || !taup || !eta)) return fail(e, IFOSB_EARG, "viscoelastic model needs taus, taup, eta");
+    e->ngreen = 0;  // Green's functions belong to a model
     const size_t ng = (size_t)(p.nx + 2) * (p.ny + 2) * (p.nz + 2);
     for (size_t q = 0; q < ng; ++q)
         if (!(rho[q] > 0.f) || !(u[q] > 0.f) || !(pi[q] > 0.f) || !std::isfinite(rho[q]) || !std::isfinite(u[q]) ||
@@ -427,6 +433,7 @@ extern "C" int ifosb_set_model(ifosb_engine *e, const float *rho, const float *p
 
 extern "C" int ifosb_set_receivers(ifosb_engine *e, int ntr, const int *recpos) {
     if (!e || ntr < 0 || (ntr > 0 && !recpos)) return IFOSB_EARG;
+    e->ngreen = 0;
     const ifosb_params &p = e->p;
     for (int t = 0; t < ntr; ++t) {
         const int i = recpos[3 * t], j = recpos[3 * t + 1], k = recpos[3 * t + 2];
@@ -474,6 +481,8 @@ static void trig_table(const ifosb_params &p, int nf, const float *finv, int nta
 
 extern "C" int ifosb_set_frequencies(ifosb_engine *e, int nf, const float *finv, int ntast) {
     if (!e || nf < 0 || nf > e->max_nf || (nf > 0 && (!finv || ntast < 1))) return IFOSB_EARG;
+    e->ngreen = 0;
+    e->hess_fwd = false;
     for (int l = 0; l < nf; ++l)
         if (!(finv[l] > 0.f)) return fail(e, IFOSB_EARG, "frequency must be positive");
     const ifosb_params &p = e->p;
@@ -949,6 +958,7 @@ extern "C" int ifosb_forward(ifosb_engine *e, int nshots, const ifosb_shot *shot
     if ((rc = run_loop(e, L))) return rc;
     e->nshots = nshots;
     e->fwd_ok = true;
+    e->hess_fwd = e->nf > 0;
     e->res_ok = e->adj_ok = false;
     if ((rc = check_unstable(e, nshots))) return rc;
     if (sections && e->ntr > 0)
@@ -1046,6 +1056,133 @@ extern "C" int ifosb_gradient(ifosb_engine *e) {
     if (rc) return rc;
     CU(cudaStreamSynchronize(e->stream));
     e->adj_ok = false;  // one gradient contribution per adjoint batch
+    return IFOSB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Approximate Hessian (hess_F.c, and the Hessian wavefields of ifos3d.c:882-938).
+// The Green's function of receiver r is the wavefield of a y-directed velocity
+// injection of `signal` at the receiver, propagated like an adjoint wavefield
+// (update_v with back = 1, elastic stress update) with the backward DFT. Each
+// is computed once per model and frequency set and kept on the device; a
+// batch of them runs as one multi-shot adjoint launch.
+extern "C" int ifosb_hessian_green(ifosb_engine *e, int nrec, const int *rec_ids, const float *signals) {
+    if (!e || nrec < 1 || !rec_ids || !signals) return IFOSB_EARG;
+    const ifosb_params &p = e->p;
+    if (!e->have_model || !e->have_cpml) return fail(e, IFOSB_ESTATE, "Green's functions need a model and CPML");
+    if (p.nmech != 0) return fail(e, IFOSB_EARG, "the Hessian wavefields are elastic (ifos3d.c:929): nmech must be 0");
+    if (e->nf == 0) return fail(e, IFOSB_ESTATE, "Green's functions need DFT frequencies");
+    if (p.ndt != 1 || p.ndtshift != 0)
+        return fail(e, IFOSB_EARG, "the injection indexes its trace by time step: NDT=1, NDTSHIFT=0");
+    for (int q = 0; q < nrec; ++q)
+        if (rec_ids[q] < 0 || rec_ids[q] >= e->ntr) return fail(e, IFOSB_EARG, "receiver index out of range");
+    int rc;
+    if (nrec > e->cap_green) {
+        dfree(e, &e->d_green, (size_t)e->dft_shot * e->cap_green);
+        e->cap_green = 0;
+        if ((rc = dalloc(e, &e->d_green, (size_t)e->dft_shot * nrec))) return rc;
+        e->cap_green = nrec;
+    }
+    e->ngreen = 0;
+    const int NT = p.nt, B0 = e->max_shots;
+    if (!e->d_gsig && (rc = dalloc(e, &e->d_gsig, (size_t)B0 * 3 * NT))) return rc;
+    std::vector<float> sig((size_t)B0 * 3 * NT, 0.0f);
+    for (int q0 = 0; q0 < nrec; q0 += B0) {
+        const int B = std::min(B0, nrec - q0);
+        for (int b = 0; b < B; ++b)  // vx and vz stay 0, vy is the receiver's signal
+            std::memcpy(&sig[((size_t)b * 3 + 1) * NT], signals + (size_t)(q0 + b) * NT, sizeof(float) * NT);
+        CU(cudaMemcpyAsync(e->d_gsig, sig.data(), sizeof(float) * (size_t)B * 3 * NT, cudaMemcpyHostToDevice, e->stream));
+        CU(cudaStreamSynchronize(e->stream));  // sig is reused by the next batch
+        std::vector<HostPt> vp;
+        for (int b = 0; b < B; ++b) {
+            const int t = rec_ids[q0 + b];
+            vp.push_back({b, e->rec[3 * t + 1], e->rec[3 * t], e->rec[3 * t + 2], PT_ADJOINT, b * 3});
+        }
+        float *dft = e->d_green + (long long)q0 * e->dft_shot;
+        Loop L;
+        std::memset(static_cast<void *>(&L), 0, sizeof(L));  // the graph cache compares Loops bytewise
+        L.nshots = B;
+        L.back = true;
+        L.lg = launch_geo(e, B, false);
+        L.lgv = launch_geo(e, B, true);
+        if ((rc = upload_points(e, L.lgv, B, vp, &e->d_voff, &e->cap_voff, &e->d_vpts, &e->cap_vpts))) return rc;
+        if ((rc = reset_state(e, B, dft))) return rc;
+        fill_common(e, L);
+        L.va.pt_off = e->d_voff;
+        L.va.pts = e->d_vpts;
+        L.va.val = e->d_gsig;  // entry b: vx, vy, vz traces at b*3*NT
+        L.va.val_row = NT;
+        L.va.val_comp = NT;
+        L.sa.pt_off = nullptr;
+        L.sa.pts = nullptr;
+        L.sa.dft = dft;
+        L.sa.trig = e->d_trig_b;
+        L.tma = e->use_tma && setup_tma(e, L, dft);
+        if ((rc = run_loop(e, L))) return rc;
+        if ((rc = check_unstable(e, B))) return rc;
+    }
+    e->ngreen = nrec;
+    e->fwd_ok = e->res_ok = e->adj_ok = false;  // the wavefield state now holds the last Green's function
+    return check_launch(e, "hessian_green");
+}
+
+// hess_F for the shots of the last forward batch against every stored Green's function.
+extern "C" int ifosb_hessian(ifosb_engine *e) {
+    if (!e) return IFOSB_EARG;
+    if (e->ngreen == 0) return fail(e, IFOSB_ESTATE, "hessian needs ifosb_hessian_green first");
+    if (e->nshots < 1 || e->nf == 0 || !e->hess_fwd) return fail(e, IFOSB_ESTATE, "hessian needs a forward batch with DFT");
+    const ifosb_params &p = e->p;
+    int rc;
+    if (!e->d_hess) {
+        if ((rc = dalloc(e, &e->d_hess, (size_t)3 * p.nx * p.ny * p.nz))) return rc;
+        CU(cudaMemsetAsync(e->d_hess, 0, sizeof(float) * 3 * p.nx * p.ny * p.nz, e->stream));
+    }
+    HessArgs a{};
+    a.g = e->g;
+    a.dftf = e->d_dftf;
+    a.dft_shot = e->dft_shot;
+    a.green = e->d_green;
+    a.nshots = e->nshots;
+    a.nrec = e->ngreen;
+    a.nf = e->nf;
+    a.md = e->d_model;
+    a.rho = e->d_rho_w;
+    for (int l = 0; l < e->nf; ++l) {
+        float fdummy = 0.0;
+        fdummy = e->finv[l] * M_PI * 2;  // hess_F.c:72-74
+        fdummy = 1 / fdummy;
+        a.fdummy[l] = fdummy;
+    }
+    a.b1 = e->b1; a.b2 = e->b2;
+    a.rdx = p.dx; a.rdy = p.dy; a.rdz = p.dz;
+    a.hess = e->d_hess;
+    dim3 blk(BX, BY), grd(e->g.ntk, e->g.nti, e->g.nyc);
+    k_hessian<<<grd, blk, 0, e->stream>>>(a);
+    if ((rc = check_launch(e, "hessian"))) return rc;
+    CU(cudaStreamSynchronize(e->stream));
+    e->hess_fwd = false;  // one contribution per forward batch
+    return IFOSB_OK;
+}
+
+extern "C" int ifosb_zero_hessian(ifosb_engine *e) {
+    if (!e) return IFOSB_EARG;
+    const size_t n = (size_t)3 * e->p.nx * e->p.ny * e->p.nz;
+    int rc;
+    if (!e->d_hess && (rc = dalloc(e, &e->d_hess, n))) return rc;
+    CU(cudaMemsetAsync(e->d_hess, 0, n * sizeof(float), e->stream));
+    CU(cudaStreamSynchronize(e->stream));
+    return IFOSB_OK;
+}
+
+extern "C" int ifosb_get_hessian(ifosb_engine *e, float *hess) {
+    if (!e || !hess) return IFOSB_EARG;
+    const size_t n = (size_t)3 * e->p.nx * e->p.ny * e->p.nz;
+    if (!e->d_hess) {
+        std::memset(hess, 0, n * sizeof(float));
+        return IFOSB_OK;
+    }
+    CU(cudaMemcpyAsync(hess, e->d_hess, n * sizeof(float), cudaMemcpyDeviceToHost, e->stream));
+    CU(cudaStreamSynchronize(e->stream));
     return IFOSB_OK;
 }
 

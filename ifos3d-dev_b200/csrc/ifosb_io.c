@@ -241,3 +241,29 @@ int ifosb_write_gradient(const char *base, float finv, int iteration, int nx, in
     }
     return IFOSB_OK;
 }
+
+/* readhess.c:25-95 on one rank: the three "<base>.{vp,vs,rho}_<finv %4.2f>Hz_it<n>"
+ * files, [z][x][y] floats, into hess [3][ny][nx][nz] scaled by VP0^2, VS0^2, RHO0^2
+ * (float value times the double power, rounded to float). */
+int ifosb_read_hessian(const char *base, float finv, int iteration, int nx, int ny, int nz, float vp0, float vs0,
+                       float rho0, float *hess) {
+    if (!base || !hess || nx < 1 || ny < 1 || nz < 1) return IFOSB_EARG;
+    static const char *name[3] = {"vp", "vs", "rho"};
+    const double sc[3] = {pow(vp0, 2), pow(vs0, 2), pow(rho0, 2)};
+    const size_t n = (size_t)nx * ny * nz;
+    char path[4096];
+    for (int c = 0; c < 3; ++c) {
+        snprintf(path, sizeof path, "%s.%s_%4.2fHz_it%d", base, name[c], finv, iteration);
+        FILE *f = fopen(path, "rb");
+        if (!f) return IFOSB_EIO;
+        for (int k = 1; k <= nz; ++k)
+            for (int i = 1; i <= nx; ++i)
+                for (int j = 1; j <= ny; ++j) {
+                    float v = 0.0f;
+                    if (fread(&v, sizeof(float), 1, f) != 1) { fclose(f); return IFOSB_EIO; }
+                    hess[c * n + ((size_t)(j - 1) * nx + (i - 1)) * nz + (k - 1)] = (float)(v * sc[c]);
+                }
+        fclose(f);
+    }
+    return IFOSB_OK;
+}

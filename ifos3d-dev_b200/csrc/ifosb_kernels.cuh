@@ -586,6 +586,88 @@ __global__ void __launch_bounds__(BX *BY) k_gradient(GradArgs a) {
 }
 
 // ---------------------------------------------------------------------------
+// hess_F (hess_F.c:67-155): the diagonal approximate Hessian from the forward DFT
+// fields of every shot of the batch (in order) and the DFT fields of the
+// receivers' Green's functions (wavefields of a y-force at each receiver), for
+// every frequency. hess is compact [3][NY][NX][NZ] FP32, accumulated in the
+// reference's order: shots, then receivers, then frequencies.
+struct HessArgs {
+    Geo g;
+    const float *dftf;         // [shot][nf][6][field]
+    long long dft_shot;
+    const float *green;        // [receiver][nf][6][field] (same per-entry stride)
+    int nshots, nrec, nf;
+    const float *md;           // model: pi, u slots
+    const float *rho;          // rho in field layout
+    float fdummy[MAXNF];       // 1/(2 pi f) in float as hess_F.c:72-74
+    float b1, b2, rdx, rdy, rdz;
+    float *hess;
+};
+
+__global__ void __launch_bounds__(BX *BY) k_hessian(HessArgs a) {
+    const Geo &g = a.g;
+    const int k = blockIdx.x * BX + threadIdx.x + 1;
+    const int i = blockIdx.y * BY + threadIdx.y + 1;
+    const int yc = blockIdx.z;
+    if (k > g.nz || i > g.nx) return;
+    const int j0 = yc * g.cy + 1;
+    const int j1 = min(j0 + g.cy - 1, g.ny);
+    const long long F = g.field, dI = g.pz, dJ = g.plane;
+    const long long n = (long long)g.nx * g.ny * g.nz;
+    for (int j = j0; j <= j1; ++j) {
+        const long long c = widx(g, j, i, k);
+        const long long m = ((long long)(j - 1) * g.nx + (i - 1)) * g.nz + (k - 1);
+        float h1 = a.hess[m], h2 = a.hess[n + m], h3 = a.hess[2 * n + m];
+        const float r = a.rho[c], pp = a.md[MD_PI * F + c], uu = a.md[MD_U * F + c];
+        for (int s = 0; s < a.nshots; ++s) {
+            for (int q = 0; q < a.nrec; ++q) {
+                for (int l = 0; l < a.nf; ++l) {
+                    const float *Fb = a.dftf + (long long)s * a.dft_shot + (long long)l * 6 * F;
+                    const float *Bb = a.green + (long long)q * a.dft_shot + (long long)l * 6 * F;
+                    float fv[9], bv[9], fi[9], bi[9];
+                    dft_derivs(Fb, Fb + F, Fb + 2 * F, c, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, fv);
+                    dft_derivs(Bb, Bb + F, Bb + 2 * F, c, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, bv);
+                    dft_derivs(Fb + 3 * F, Fb + 4 * F, Fb + 5 * F, c, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, fi);
+                    dft_derivs(Bb + 3 * F, Bb + 4 * F, Bb + 5 * F, c, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, bi);
+                    const float fd = a.fdummy[l];
+                    const float fdiv = fv[0] + fv[4] + fv[8], fidiv = fi[0] + fi[4] + fi[8];
+                    const float bdiv = bv[0] + bv[4] + bv[8], bidiv = bi[0] + bi[4] + bi[8];
+                    float relam = fidiv * bdiv + fdiv * bidiv;
+                    relam = fd * relam;
+                    float imlam = fidiv * bidiv - fdiv * bdiv;
+                    imlam = fd * imlam;
+                    float remu = 2.0f * fi[0] * bv[0] + 2.0f * fi[4] * bv[4] + 2.0f * fi[8] * bv[8] +
+                                 2.0f * fv[0] * bi[0] + 2.0f * fv[4] * bi[4] + 2.0f * fv[8] * bi[8] +
+                                 (fi[1] + fi[3]) * (bv[1] + bv[3]) + (fv[1] + fv[3]) * (bi[1] + bi[3]) +
+                                 (fi[2] + fi[6]) * (bv[2] + bv[6]) + (fv[2] + fv[6]) * (bi[2] + bi[6]) +
+                                 (fi[5] + fi[7]) * (bv[5] + bv[7]) + (fv[5] + fv[7]) * (bi[5] + bi[7]);
+                    remu = fd * remu;
+                    float immu = 2.0f * fi[0] * bi[0] + 2.0f * fi[4] * bi[4] + 2.0f * fi[8] * bi[8] -
+                                 2.0f * fv[0] * bv[0] - 2.0f * fv[4] * bv[4] - 2.0f * fv[8] * bv[8] +
+                                 (fi[1] + fi[3]) * (bi[1] + bi[3]) - (fv[1] + fv[3]) * (bv[1] + bv[3]) +
+                                 (fi[2] + fi[6]) * (bi[2] + bi[6]) - (fv[2] + fv[6]) * (bv[2] + bv[6]) +
+                                 (fi[5] + fi[7]) * (bi[5] + bi[7]) - (fv[5] + fv[7]) * (bv[5] + bv[7]);
+                    immu = fd * immu;
+                    const float rerho = (Fb[c] * Bb[c] + Fb[F + c] * Bb[F + c] + Fb[2 * F + c] * Bb[2 * F + c]) -
+                                        (Fb[3 * F + c] * Bb[3 * F + c] + Fb[4 * F + c] * Bb[4 * F + c] +
+                                         Fb[5 * F + c] * Bb[5 * F + c]);
+                    const float imrho = (Fb[c] * Bb[3 * F + c] + Fb[F + c] * Bb[4 * F + c] + Fb[2 * F + c] * Bb[5 * F + c]) +
+                                        (Fb[3 * F + c] * Bb[c] + Fb[4 * F + c] * Bb[F + c] + Fb[5 * F + c] * Bb[2 * F + c]);
+                    const float revs = -2.0f * relam + remu;
+                    const float imvs = -2.0f * imlam + immu;
+                    const float rerho1 = rerho + relam * (pp - 2.0f * uu) / r + remu * uu / r;
+                    const float imrho1 = imrho + imlam * (pp - 2.0f * uu) / r + immu * uu / r;
+                    h1 += (relam * relam + imlam * imlam) * r * pp * 4.0f;
+                    h2 += (revs * revs + imvs * imvs) * 4.0f * r * uu;
+                    h3 += rerho1 * rerho1 + imrho1 * imrho1;
+                }
+            }
+        }
+        a.hess[m] = h1; a.hess[n + m] = h2; a.hess[2 * n + m] = h3;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // av_mat (av_mat.c:45-69) from the ghosted model [NY+2][NX+2][NZ+2] into the
 // model slots, plus the per-cell pi, u, taus, taup.
 struct AvArgs {

@@ -670,3 +670,46 @@ extern "C" int ifosb_constant_boundary(ifosb_optim *o, float *rho, float *pi, fl
     OCU(cudaMemcpyAsync(u, du, sizeof(float) * mg, cudaMemcpyDefault, o->stream));
     return finish(o);
 }
+
+// ---------------------------------------------------------------------------
+// hess_apply (hess_apply.c:25-79): with L-BFGS the gradients are first scaled by
+// VP0, VS0, RHO0; then grad_c /= (hess_c + WATER_HESS[c]). The water level the
+// reference derives from the Hessian's log-average is printed there and never
+// used, so it is not formed here.
+__global__ void k_hess_apply(float *g, const float *h, long long n, float w0, float w1, float w2, int lbfgs, float vp0,
+                             float vs0, float rho0) {
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
+        float g1 = g[m], g2 = g[n + m], g3 = g[2 * n + m];
+        if (lbfgs) {
+            g1 = g1 * vp0;
+            g2 = g2 * vs0;
+            g3 = g3 * rho0;
+        }
+        g[m] = g1 / (h[m] + w0);
+        g[n + m] = g2 / (h[n + m] + w1);
+        g[2 * n + m] = g3 / (h[2 * n + m] + w2);
+    }
+}
+
+extern "C" int ifosb_hess_apply(ifosb_optim *o, float *grad, const float *hess, const float *water, int lbfgs,
+                                float vp0, float vs0, float rho0) {
+    if (!o || !grad || !hess || !water) return IFOSB_EARG;
+    const long long n = o->n;
+    float *dh = nullptr;
+    OCU(cudaMalloc(&dh, sizeof(float) * 3 * n));
+    cudaError_t ce = cudaMemcpyAsync(dh, hess, sizeof(float) * 3 * n, cudaMemcpyDefault, o->stream);
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(o->d_grad, grad, sizeof(float) * 3 * n, cudaMemcpyDefault, o->stream);
+    if (ce == cudaSuccess) {
+        k_hess_apply<<<RBLK, RTHR, 0, o->stream>>>(o->d_grad, dh, n, water[0], water[1], water[2], lbfgs ? 1 : 0, vp0,
+                                                   vs0, rho0);
+        ce = cudaGetLastError();
+    }
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(grad, o->d_grad, sizeof(float) * 3 * n, cudaMemcpyDefault, o->stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(o->stream);
+    cudaFree(dh);
+    if (ce != cudaSuccess) {
+        o->err = std::string("hess_apply: ") + cudaGetErrorString(ce);
+        return IFOSB_ECUDA;
+    }
+    return IFOSB_OK;
+}

@@ -120,6 +120,13 @@ def lib():
             "ifosb_write_gradient": (C.c_int, [C.c_char_p, C.c_float, C.c_int, C.c_int, C.c_int, C.c_int, vp,
                                                C.c_int, C.c_int, C.c_int, C.c_int]),
             "ifosb_filt_seis": (C.c_int, [vp, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int, C.c_int]),
+            "ifosb_hessian_green": (C.c_int, [vp, C.c_int, vp, vp]),
+            "ifosb_hessian": (C.c_int, [vp]),
+            "ifosb_zero_hessian": (C.c_int, [vp]),
+            "ifosb_get_hessian": (C.c_int, [vp, vp]),
+            "ifosb_read_hessian": (C.c_int, [C.c_char_p, C.c_float, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float,
+                                             C.c_float, C.c_float, vp]),
+            "ifosb_hess_apply": (C.c_int, [vp, vp, vp, vp, C.c_int, C.c_float, C.c_float, C.c_float]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -141,7 +148,8 @@ def exported_symbols():
         "ifosb_optim_last_error", "ifosb_conjugate", "ifosb_lbfgs_savegrad", "ifosb_lbfgs", "ifosb_modelupdate",
         "ifosb_lbfgs_history", "ifosb_steplength", "ifosb_precon_grad", "ifosb_constant_boundary",
         "ifosb_write_seis", "ifosb_merge_seis", "ifosb_read_seis", "ifosb_read_seis_split",
-        "ifosb_write_model", "ifosb_write_gradient", "ifosb_filt_seis",
+        "ifosb_write_model", "ifosb_write_gradient", "ifosb_filt_seis", "ifosb_hessian_green", "ifosb_hessian",
+        "ifosb_zero_hessian", "ifosb_get_hessian", "ifosb_read_hessian", "ifosb_hess_apply",
     ]
 
 
@@ -347,6 +355,31 @@ class Engine:
     def zero_gradient(self):
         self._c(lib().ifosb_zero_gradient(self.h))
 
+    # -- approximate Hessian (hess_F) -----------------------------------------
+    def hessian_green(self, rec_ids, signals):
+        """Green's functions of receivers rec_ids: a y-force signals[q] ([NT]; one
+        row shared by all when 1-D) at receiver rec_ids[q]."""
+        r = np.ascontiguousarray(rec_ids, np.int32)
+        sig = np.asarray(signals, np.float32)
+        if sig.ndim == 1:
+            sig = np.broadcast_to(sig, (len(r), sig.size))
+        sig = np.ascontiguousarray(sig)
+        if sig.shape != (len(r), self.p.nt):
+            raise IfosbError(EARG, f"signals of shape {sig.shape}, expected ({len(r)}, NT={self.p.nt})")
+        self._c(lib().ifosb_hessian_green(self.h, len(r), _p(r), _p(sig)))
+
+    def hessian(self):
+        """Add the last forward batch's hess_F contributions to the device Hessian."""
+        self._c(lib().ifosb_hessian(self.h))
+
+    def zero_hessian(self):
+        self._c(lib().ifosb_zero_hessian(self.h))
+
+    def get_hessian(self):
+        h = np.zeros((3, self.p.ny, self.p.nx, self.p.nz), np.float32)
+        self._c(lib().ifosb_get_hessian(self.h, _p(h)))
+        return h
+
     def get_gradient(self, fp64=False):
         g = np.zeros((3, self.p.ny, self.p.nx, self.p.nz), np.float64 if fp64 else np.float32)
         if fp64:
@@ -441,6 +474,13 @@ class Optimizer:
         self._c(lib().ifosb_precon_grad(self.h, _p(self._grad(grad)), damptype, int(bool(free_surf)), fw, dh[0], dh[1],
                                         dh[2], 0 if src is None else src.shape[0], _p(src),
                                         0 if rec is None else rec.shape[0], _p(rec)))
+
+    def hess_apply(self, grad, hess, water, lbfgs=False, vp0=0.0, vs0=0.0, rho0=0.0):
+        """hess_apply: grad [3][NY][NX][NZ] in place divided by hess + water[c]
+        (scaled first by VP0, VS0, RHO0 with L-BFGS)."""
+        h = self._grad(np.ascontiguousarray(hess, np.float32))
+        w = np.ascontiguousarray(water, np.float32)
+        self._c(lib().ifosb_hess_apply(self.h, _p(self._grad(grad)), _p(h), _p(w), int(bool(lbfgs)), vp0, vs0, rho0))
 
     def constant_boundary(self, rho, pi, u, fw):
         """constant_boundary on the ghosted model arrays in place."""

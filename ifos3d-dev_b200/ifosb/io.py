@@ -144,3 +144,11 @@ def write_gradient(base, finv, iteration, grad, idx=1, idy=1, idz=1):
     _, ny, nx, nz = g.shape
     _check(lib().ifosb_write_gradient(os.fsencode(base), finv, iteration, nx, ny, nz, _p(g), 0, idx, idy, idz),
            f"write_gradient {base}")
+
+
+def read_hessian(base, finv, iteration, ny, nx, nz, vp0, vs0, rho0):
+    """readhess(): "<base>.{vp,vs,rho}_<f>Hz_it<n>" into [3][ny][nx][nz], scaled by VP0^2 etc."""
+    out = np.zeros((3, ny, nx, nz), np.float32)
+    _check(lib().ifosb_read_hessian(os.fsencode(base), finv, iteration, nx, ny, nz, vp0, vs0, rho0, _p(out)),
+           f"read_hessian {base}")
+    return out

@@ -182,6 +182,28 @@ int ifosb_set_launch_shape(ifosb_engine *e, int nshots, const int *shape);
  * void*; NULL = the engine's own stream). Calls stay synchronous at return. */
 int ifosb_set_stream(ifosb_engine *e, void *stream);
 
+/* ---- approximate Hessian (HESS; src/hess_F.c, src/ifos3d.c:882-986) --------
+ * Elastic models only (the reference propagates its Hessian wavefields with
+ * update_s_elastic), NDT = 1, NDTSHIFT = 0, frequencies set.
+ *
+ * ifosb_hessian_green: the Hessian wavefields of the reference's pshot loop
+ * (ifos3d.c:887-938) for receivers rec_ids[0..nrec-1] (indices into the
+ * receiver list): each is a y-velocity injection of its row of signals
+ * [nrec][NT] at the receiver, propagated in adjoint mode with the backward DFT
+ * (discfourier, back = 1). The reference's row is wavelet(..., 5, ...) of the
+ * receiver's recpos_loc column with amplitude 1 (a step at t = row 4), low-passed
+ * when FILT. They are kept on the
+ * device until the model, receivers or frequencies change. Destroys the current
+ * wavefield state (call before a batch's forward).
+ * ifosb_hessian: replaces hess_F (hess_F.c:25-160) for the shots of the last
+ * forward batch, adding to the device Hessian in the reference's order (shots,
+ * receivers, frequencies), FP32, the same bits.
+ * ifosb_zero_hessian / ifosb_get_hessian: hess [3][NY][NX][NZ] (vp, vs, rho). */
+int ifosb_hessian_green(ifosb_engine *e, int nrec, const int *rec_ids, const float *signals);
+int ifosb_hessian(ifosb_engine *e);
+int ifosb_zero_hessian(ifosb_engine *e);
+int ifosb_get_hessian(ifosb_engine *e, float *hess);
+
 /* ---- host utilities (restated reference host code) ---------------------- */
 
 /* CPML_coeff (src/CPML_coeff.c:87-324) with VPPML, FPML into coeff[18][2*FW]. */
@@ -265,6 +287,12 @@ int ifosb_lbfgs_history(const ifosb_optim *o, double *s, double *y, double *scal
  * on the host in FP64. */
 int ifosb_steplength(double *L2, double *step, int lbfgs, int it_group, double teststep, double *abc);
 
+/* hess_apply (src/hess_apply.c:25-79, called at src/ifos3d.c:1002): grad [3][ny][nx][nz]
+ * (host or device pointer) divided by hess + water[c] (WATER_HESS), after scaling by
+ * VP0, VS0, RHO0 when lbfgs; the same bits as the reference. */
+int ifosb_hess_apply(ifosb_optim *o, float *grad, const float *hess, const float *water, int lbfgs, float vp0,
+                     float vs0, float rho0);
+
 /* ---- residual without allocation ---------------------------------------- */
 
 /* No counterpart in the reference (its residual() works on host arrays).
@@ -345,6 +373,11 @@ int ifosb_write_model(const char *base, int iteration, int nx, int ny, int nz, c
  * [3][ny][nx][nz] (ghost = 0) or [3][ny+2][nx+2][nz+2] (ghost = 1). */
 int ifosb_write_gradient(const char *base, float finv, int iteration, int nx, int ny, int nz, const float *grad,
                          int ghost, int idx, int idy, int idz);
+
+/* Hessian files written by outgrad (HESS_FILE) read back as readhess() does
+ * (src/readhess.c:25-95): hess [3][ny][nx][nz] = file value * VP0^2, VS0^2, RHO0^2. */
+int ifosb_read_hessian(const char *base, float finv, int iteration, int nx, int ny, int nz, float vp0, float vs0,
+                       float rho0, float *hess);
 
 /* ---- multiscale stages (host) ---------------------------------------------
  * Time-domain Butterworth filter of FILT = 1, replacing filt_seis()

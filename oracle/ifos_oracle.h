@@ -97,6 +97,9 @@ int ifo_adjoint(const ifo_params *p, const float *rho, const float *pi, const fl
 /* gradient_F (src/gradient_F.c:30-171): grad[3][NY][NX][NZ] += contribution. */
 int ifo_gradient(const ifo_params *p, const float *rho, const float *pi, const float *u,
                  int nf, const float *finv, const float *dft_fwd, const float *dft_back, float *grad);
+/* hess_F for one shot against ngreen receivers' DFT fields (reference build only). */
+int ifo_hessian(const ifo_params *p, const float *rho, const float *pi, const float *u, int nf, const float *finv,
+                const float *dft_fwd, int ngreen, const float *dft_green, float *hess);
 
 #ifdef __cplusplus
 }

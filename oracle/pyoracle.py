@@ -149,6 +149,17 @@ class Oracle:
             raise RuntimeError(f"ifo_adjoint rc={rc}")
         return dict(dft=dft, state=st)
 
+    def hessian(self, p: IfoParams, m, finv, dft_f, greens, hess=None):
+        """hess_F of one shot (dft_f [6][nf][W]) against receivers' DFT fields
+        greens [ngreen][6][nf][W], added to hess [3][ny][nx][nz] (reference build)."""
+        h = np.zeros((3, p.ny, p.nx, p.nz), np.float32) if hess is None else np.ascontiguousarray(hess, np.float32).copy()
+        finv = _f32(finv)
+        greens = _f32(greens)
+        rc = self.lib.ifo_hessian(C.byref(p), _ptr(_f32(m["rho"])), _ptr(_f32(m["pi"])), _ptr(_f32(m["u"])),
+                                  len(finv), _ptr(finv), _ptr(_f32(dft_f)), greens.shape[0], _ptr(greens), _ptr(h))
+        assert rc == 0
+        return h
+
     def gradient(self, p: IfoParams, m, finv, dft_f, dft_b, grad=None):
         g = np.zeros((3, p.ny, p.nx, p.nz), np.float32) if grad is None else np.ascontiguousarray(grad, np.float32).copy()
         finv = _f32(finv)

@@ -562,3 +562,40 @@ int ifo_gradient(const ifo_params *p, const float *rho, const float *pi, const f
     model_free(p, &m);
     return 0;
 }
+
+/* hess_F (src/hess_F.c) for one shot: forward DFT [6][nf][W] against ngreen
+ * receivers' DFT fields [ngreen][6][nf][W], added to hess [3][ny][nx][nz].
+ * Receiver n (1-based) sits at the reference's backward index n*nf + l. */
+int ifo_hessian(const ifo_params *p, const float *rho, const float *pi, const float *u, int nf, const float *finv,
+                const float *dft_fwd, int ngreen, const float *dft_green, float *hess) {
+    ifo_params q = *p;
+    q.nmech = 0;
+    p = &q;
+    set_globals(p);
+    refmodel m; model_setup(p, &m, rho, pi, u, NULL, NULL, NULL);
+    size_t n = wsize(p);
+    const int nb = nf * (ngreen + 1);
+    float ****F[6], ****B[6];
+    for (int c = 0; c < 6; c++) {
+        F[c] = alloc_f(p, nf); B[c] = alloc_f(p, nb);
+        for (int l = 1; l <= nf; l++)
+            memcpy(&F[c][l][-2][-1][-1], dft_fwd + ((size_t)c * nf + l - 1) * n, sizeof(float) * n);
+        for (int r = 1; r <= ngreen; r++)
+            for (int l = 1; l <= nf; l++)
+                memcpy(&B[c][r * nf + l][-2][-1][-1], dft_green + (((size_t)(r - 1) * 6 + c) * nf + l - 1) * n,
+                       sizeof(float) * n);
+    }
+    float *fv = vector(0, nf - 1);
+    for (int l = 0; l < nf; l++) fv[l] = finv[l];
+    size_t g = (size_t)p->nx * p->ny * p->nz;
+    float ***h1 = alloc_g(p), ***h2 = alloc_g(p), ***h3 = alloc_g(p);
+    g_in(p, h1, hess); g_in(p, h2, hess + g); g_in(p, h3, hess + 2 * g);
+    hess_F(NX, NY, NZ, F[0], F[1], F[2], F[3], F[4], F[5], B[0], B[1], B[2], B[3], B[4], B[5],
+           h1, h2, h3, NT, m.rho, m.pi, m.u, fv, nf, ngreen);
+    g_out(p, h1, hess); g_out(p, h2, hess + g); g_out(p, h3, hess + 2 * g);
+    free_g(p, h1); free_g(p, h2); free_g(p, h3);
+    free_vector(fv, 0, nf - 1);
+    for (int c = 0; c < 6; c++) { free_f(p, F[c], nf); free_f(p, B[c], nb); }
+    model_free(p, &m);
+    return 0;
+}

@@ -190,3 +190,46 @@ int ifo_ref_readinv(const char *path, int groupnum, float *finv, int *nf, int *i
     readinv(finv, nf, &g, it, nfmax);
     return g;
 }
+
+/* hess_apply (src/hess_apply.c) on grad, hess [3][ny][nx][nz] (grad in place). */
+extern float WATER_HESS[3], VP0, VS0, RHO0;
+extern int LBFGS, NXG, NYG, NZG, FW;
+int ifo_ref_hess_apply(int nx, int ny, int nz, float *grad, const float *hess, const float *water, int lbfgs,
+                       float vp0, float vs0, float rho0) {
+    quiet();
+    NX = NXG = nx; NY = NYG = ny; NZ = NZG = nz; FW = 1;
+    for (int c = 0; c < 3; ++c) WATER_HESS[c] = water[c];
+    LBFGS = lbfgs; VP0 = vp0; VS0 = vs0; RHO0 = rho0;
+    const size_t n = (size_t)nx * ny * nz;
+    float ***G[3], ***H[3];
+    for (int c = 0; c < 3; ++c) {
+        G[c] = f3tensor(1, ny, 1, nx, 1, nz); memcpy(&G[c][1][1][1], grad + c * n, sizeof(float) * n);
+        H[c] = f3tensor(1, ny, 1, nx, 1, nz); memcpy(&H[c][1][1][1], hess + c * n, sizeof(float) * n);
+    }
+    hess_apply(1, nx, 1, ny, 1, nz, G[0], G[1], G[2], H[0], H[1], H[2], 0.0f, 1);
+    for (int c = 0; c < 3; ++c) {
+        memcpy(grad + c * n, &G[c][1][1][1], sizeof(float) * n);
+        free_f3tensor(G[c], 1, ny, 1, nx, 1, nz);
+        free_f3tensor(H[c], 1, ny, 1, nx, 1, nz);
+    }
+    return 0;
+}
+
+/* readhess (src/readhess.c) into hess [3][ny][nx][nz]. */
+extern char HESS_FILE[STRING_SIZE];
+int ifo_ref_readhess(const char *base, float finv, int iteration, int nx, int ny, int nz, float vp0, float vs0,
+                     float rho0, float *hess) {
+    quiet();
+    NX = NXG = nx; NY = NYG = ny; NZ = NZG = nz;
+    VP0 = vp0; VS0 = vs0; RHO0 = rho0;
+    snprintf(HESS_FILE, STRING_SIZE, "%s", base);
+    const size_t n = (size_t)nx * ny * nz;
+    float ***H[3];
+    for (int c = 0; c < 3; ++c) H[c] = f3tensor(1, ny, 1, nx, 1, nz);
+    readhess(nx, ny, nz, H[0], H[1], H[2], finv, iteration);
+    for (int c = 0; c < 3; ++c) {
+        memcpy(hess + c * n, &H[c][1][1][1], sizeof(float) * n);
+        free_f3tensor(H[c], 1, ny, 1, nx, 1, nz);
+    }
+    return 0;
+}

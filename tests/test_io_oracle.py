@@ -30,7 +30,7 @@ def ref(ref_oracle):
     from pyoracle import REF_LIB
     lib = C.CDLL(REF_LIB)
     for n in ("ifo_ref_outseis", "ifo_ref_saveseis", "ifo_ref_readseis", "ifo_ref_readseis_split",
-              "ifo_ref_outmod", "ifo_ref_outgrad"):
+              "ifo_ref_outmod", "ifo_ref_outgrad", "ifo_ref_readhess"):
         getattr(lib, n).restype = C.c_int
     return lib
 
@@ -228,3 +228,19 @@ def test_io_errors(wd):
     with pytest.raises(ifosb.IfosbError):
         fio.write_seis(str(wd / "no_dir" / "x.su"), sec, rec, **GEOM)
     assert fio.merge_seis(str(wd / "m.su"), [str(wd / "none")], 5) == 0
+
+
+def test_read_hessian_matches_readhess(ref, wd):
+    """Hessian files as outgrad writes them (HESS_FILE), read back as readhess
+    does: scaled by VP0^2, VS0^2, RHO0^2."""
+    ny, nx, nz = 5, 6, 4
+    rng = np.random.default_rng(9)
+    h = (rng.uniform(0.0, 1.0, (3, ny, nx, nz)) * 1e-12).astype(np.float32)
+    fio.write_gradient("hess", 7.25, 1, h)
+    out_ref = np.zeros_like(h)
+    assert ref.ifo_ref_readhess(b"hess", f(7.25), 1, nx, ny, nz, f(3100.0), f(1790.0), f(2250.0), P(out_ref)) == 0
+    ours = fio.read_hessian("hess", 7.25, 1, ny, nx, nz, 3100.0, 1790.0, 2250.0)
+    assert np.array_equal(out_ref.view(np.uint32), ours.view(np.uint32))
+    assert np.allclose(ours[0], h[0] * 3100.0 ** 2, rtol=1e-6)
+    with pytest.raises(ifosb.IfosbError):
+        fio.read_hessian("nohess", 7.25, 1, ny, nx, nz, 1.0, 1.0, 1.0)
