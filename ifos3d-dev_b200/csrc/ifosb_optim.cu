@@ -713,3 +713,80 @@ extern "C" int ifosb_hess_apply(ifosb_optim *o, float *grad, const float *hess, 
     }
     return IFOSB_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Model resampling between the grids of a multiscale run (coarse to fine, e.g.
+// 256x256x160 at 2 m to 512x512x320 at 1 m). The reference has no such step, so
+// the rule is our own and plain: cell (i, j, k) of a grid sits at (i dx, j dy,
+// k dz), as source and receiver positions do in the reference (index x spacing).
+// A destination cell takes the trilinear interpolation of the source grid at its
+// position, clamped to the source's first/last cell outside it (constant
+// extrapolation), computed in double and rounded once to float.
+struct ResampleArgs {
+    const float *src;
+    float *dst;
+    int nx, ny, nz, mx, my, mz;
+    double rx, ry, rz;  // destination spacing / source spacing, per axis
+};
+
+__device__ __forceinline__ void axis_weights(int i, double r, int n, int &i0, int &i1, double &w) {
+    const double u = (double)i * r;  // position in source index units (1-based)
+    if (u <= 1.0) { i0 = i1 = 1; w = 0.0; return; }
+    if (u >= (double)n) { i0 = i1 = n; w = 0.0; return; }
+    i0 = (int)floor(u);
+    i1 = i0 + 1;
+    w = u - (double)i0;
+}
+
+__global__ void k_resample(ResampleArgs a) {
+    const long long total = (long long)a.mx * a.my * a.mz;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
+         q += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(q % a.mz) + 1, i = (int)((q / a.mz) % a.mx) + 1, j = (int)(q / ((long long)a.mz * a.mx)) + 1;
+        int x0, x1, y0, y1, z0, z1;
+        double wx, wy, wz;
+        axis_weights(i, a.rx, a.nx, x0, x1, wx);
+        axis_weights(j, a.ry, a.ny, y0, y1, wy);
+        axis_weights(k, a.rz, a.nz, z0, z1, wz);
+        auto S = [&](int jj, int ii, int kk) {
+            return (double)a.src[((long long)(jj - 1) * a.nx + (ii - 1)) * a.nz + (kk - 1)];
+        };
+        const double c00 = S(y0, x0, z0) * (1.0 - wz) + S(y0, x0, z1) * wz;
+        const double c01 = S(y0, x1, z0) * (1.0 - wz) + S(y0, x1, z1) * wz;
+        const double c10 = S(y1, x0, z0) * (1.0 - wz) + S(y1, x0, z1) * wz;
+        const double c11 = S(y1, x1, z0) * (1.0 - wz) + S(y1, x1, z1) * wz;
+        const double c0 = c00 * (1.0 - wx) + c01 * wx;
+        const double c1 = c10 * (1.0 - wx) + c11 * wx;
+        a.dst[q] = (float)(c0 * (1.0 - wy) + c1 * wy);
+    }
+}
+
+extern "C" int ifosb_resample(const float *src, int nx, int ny, int nz, float dx, float dy, float dz, float *dst,
+                              int mx, int my, int mz, float ex, float ey, float ez) {
+    if (!src || !dst || nx < 1 || ny < 1 || nz < 1 || mx < 1 || my < 1 || mz < 1) return IFOSB_EARG;
+    if (!(dx > 0.f && dy > 0.f && dz > 0.f && ex > 0.f && ey > 0.f && ez > 0.f)) return IFOSB_EARG;
+    int dev = 0;
+    if (cudaGetDeviceCount(&dev) != cudaSuccess || dev == 0) {
+        cudaGetLastError();
+        return IFOSB_ENODEV;
+    }
+    const size_t ns = (size_t)nx * ny * nz, nd = (size_t)mx * my * mz;
+    float *ds = nullptr, *dd = nullptr;
+    cudaError_t ce = cudaMalloc(&ds, ns * sizeof(float));
+    if (ce == cudaSuccess) ce = cudaMalloc(&dd, nd * sizeof(float));
+    if (ce == cudaSuccess) ce = cudaMemcpy(ds, src, ns * sizeof(float), cudaMemcpyDefault);
+    if (ce == cudaSuccess) {
+        ResampleArgs a{ds, dd, nx, ny, nz, mx, my, mz, (double)ex / (double)dx, (double)ey / (double)dy,
+                       (double)ez / (double)dz};
+        k_resample<<<RBLK, RTHR>>>(a);
+        ce = cudaGetLastError();
+    }
+    if (ce == cudaSuccess) ce = cudaMemcpy(dst, dd, nd * sizeof(float), cudaMemcpyDefault);
+    if (ds) cudaFree(ds);
+    if (dd) cudaFree(dd);
+    if (ce != cudaSuccess) {
+        cudaGetLastError();
+        return ce == cudaErrorMemoryAllocation ? IFOSB_ENOMEM : IFOSB_ECUDA;
+    }
+    return IFOSB_OK;
+}

@@ -127,6 +127,8 @@ def lib():
             "ifosb_read_hessian": (C.c_int, [C.c_char_p, C.c_float, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float,
                                              C.c_float, C.c_float, vp]),
             "ifosb_hess_apply": (C.c_int, [vp, vp, vp, vp, C.c_int, C.c_float, C.c_float, C.c_float]),
+            "ifosb_resample": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float, vp,
+                                         C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -149,7 +151,7 @@ def exported_symbols():
         "ifosb_lbfgs_history", "ifosb_steplength", "ifosb_precon_grad", "ifosb_constant_boundary",
         "ifosb_write_seis", "ifosb_merge_seis", "ifosb_read_seis", "ifosb_read_seis_split",
         "ifosb_write_model", "ifosb_write_gradient", "ifosb_filt_seis", "ifosb_hessian_green", "ifosb_hessian",
-        "ifosb_zero_hessian", "ifosb_get_hessian", "ifosb_read_hessian", "ifosb_hess_apply",
+        "ifosb_zero_hessian", "ifosb_get_hessian", "ifosb_read_hessian", "ifosb_hess_apply", "ifosb_resample",
     ]
 
 

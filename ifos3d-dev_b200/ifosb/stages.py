@@ -81,3 +81,24 @@ def filt_seis(data, finv, dt, order=4, highpass=False):
     if rc != 0:
         raise IfosbError(rc, "filt_seis")
     return a
+
+
+def resample(field, spacing, shape, new_spacing):
+    """A [ny][nx][nz] field on a grid of spacing (dx, dy, dz) resampled onto a
+    grid of `shape` (ny, nx, nz) and spacing new_spacing (ifosb_resample:
+    trilinear at the cell positions, constant outside)."""
+    a = np.ascontiguousarray(field, np.float32)
+    ny, nx, nz = a.shape
+    my, mx, mz = shape
+    out = np.zeros((my, mx, mz), np.float32)
+    rc = lib().ifosb_resample(a.ctypes.data_as(C.c_void_p), nx, ny, nz, *[float(v) for v in spacing],
+                              out.ctypes.data_as(C.c_void_p), mx, my, mz, *[float(v) for v in new_spacing])
+    if rc != 0:
+        raise IfosbError(rc, "resample")
+    return out
+
+
+def resample_model(vp, vs, rho, spacing, shape, new_spacing):
+    """vp, vs, rho of one multiscale grid carried to the next (velocities and
+    density are interpolated, not the moduli)."""
+    return tuple(resample(f, spacing, shape, new_spacing) for f in (vp, vs, rho))

@@ -389,6 +389,14 @@ int ifosb_read_hessian(const char *base, float finv, int iteration, int nx, int 
  * is left unfiltered. */
 int ifosb_filt_seis(float *data, int ntr, int ns, float finv, float dt, int order, int highpass);
 
+/* Model resampling between multiscale grids (the reference has none): src
+ * [ny][nx][nz] with spacing dx, dy, dz onto dst [my][mx][mz] with spacing ex, ey,
+ * ez, by trilinear interpolation at the cell positions (i*dx etc.), constant
+ * outside the source grid, in double, rounded once. Host or device pointers; runs
+ * on the current CUDA device. */
+int ifosb_resample(const float *src, int nx, int ny, int nz, float dx, float dy, float dz, float *dst, int mx, int my,
+                   int mz, float ex, float ey, float ez);
+
 #ifdef __cplusplus
 }
 #endif
