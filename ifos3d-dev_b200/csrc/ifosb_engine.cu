@@ -58,6 +58,8 @@ struct ifosb_engine {
     int ntr = 0, ns = 0;
     std::vector<int> rec;
     float *d_sec = nullptr, *d_diff = nullptr, *d_obs = nullptr;
+    int seismo = 1;            // SEISMO: 1 vx, vy, vz; 2 p; 3 div, curl; 4 all six
+    float *d_sec2 = nullptr;   // [max_shots][3][ntr][ns]: p, div, curl (SEISMO 2-4)
     double *d_part = nullptr, *d_misfit = nullptr;
     float *d_l2 = nullptr;
     // frequencies
@@ -314,12 +316,25 @@ extern "C" void ifosb_destroy(ifosb_engine *e) {
     void *bufs[] = {e->d_state, e->d_psi, e->d_model, e->d_rho_w, e->d_dftf, e->d_dftb, e->d_grad, e->d_grad64,
                     e->d_err, e->d_sec, e->d_diff, e->d_obs, e->d_part, e->d_misfit, e->d_l2, e->d_trig_f,
                     e->d_trig_b, e->d_voff, e->d_soff, e->d_vpts, e->d_spts, e->d_amp, e->d_tma_err, e->d_cpg,
-                    e->d_mstage, e->d_green, e->d_gsig, e->d_hess};
+                    e->d_mstage, e->d_green, e->d_gsig, e->d_hess, e->d_sec2};
     for (void *b : bufs)
         if (b) cudaFree(b);
     for (cudaEvent_t ev : e->events) cudaEventDestroy(ev);
     if (e->own_stream) cudaStreamDestroy(e->own_stream);
     delete e;
+}
+
+extern "C" int ifosb_set_seismo(ifosb_engine *e, int seismo) {
+    if (!e || seismo < 1 || seismo > 4) return IFOSB_EARG;
+    if (seismo >= 2 && !e->d_sec2 && e->ntr > 0) {
+        const size_t secn = (size_t)e->max_shots * 3 * e->ntr * e->ns;
+        int rc;
+        if ((rc = dalloc(e, &e->d_sec2, secn))) return rc;
+        CU(cudaMemsetAsync(e->d_sec2, 0, secn * sizeof(float), e->stream));
+        CU(cudaStreamSynchronize(e->stream));
+    }
+    e->seismo = seismo;
+    return IFOSB_OK;
 }
 
 extern "C" int ifosb_set_profiling(ifosb_engine *e, int profile) {
@@ -443,6 +458,7 @@ extern "C" int ifosb_set_receivers(ifosb_engine *e, int ntr, const int *recpos) 
     const int ns = nsamples(&p);
     const size_t secn = (size_t)e->max_shots * 3 * std::max(ntr, 1) * std::max(ns, 1);
     dfree(e, &e->d_sec, e->ntr ? (size_t)e->max_shots * 3 * e->ntr * e->ns : 0);
+    dfree(e, &e->d_sec2, e->ntr ? (size_t)e->max_shots * 3 * e->ntr * e->ns : 0);
     dfree(e, &e->d_diff, e->ntr ? (size_t)e->max_shots * 3 * e->ntr * e->ns : 0);
     dfree(e, &e->d_obs, e->ntr ? (size_t)e->max_shots * 3 * e->ntr * e->ns : 0);
     dfree(e, &e->d_part, e->ntr ? (size_t)e->max_shots * 3 * e->ntr : 0);
@@ -455,6 +471,10 @@ extern "C" int ifosb_set_receivers(ifosb_engine *e, int ntr, const int *recpos) 
         (rc = dalloc(e, &e->d_misfit, (size_t)e->max_shots)) || (rc = dalloc(e, &e->d_l2, (size_t)e->max_shots)))
         return rc;
     CU(cudaMemsetAsync(e->d_sec, 0, secn * sizeof(float), e->stream));
+    if (e->seismo >= 2) {
+        if ((rc = dalloc(e, &e->d_sec2, secn))) return rc;
+        CU(cudaMemsetAsync(e->d_sec2, 0, secn * sizeof(float), e->stream));
+    }
     e->ntr = ntr;
     e->ns = ns;
     e->rec.assign(recpos, recpos + 3 * ntr);
@@ -594,6 +614,11 @@ static void fill_common(ifosb_engine *e, Loop &L) {
         sa.msb[l] = eta / (1.0 + (eta * 0.5));     // surface_ssg.c:152
     }
     sa.sec = e->d_sec;
+    sa.seismo = e->seismo;
+    sa.sec2 = e->d_sec2;
+    sa.hrx = (float)(1.0 / (double)e->p.dx);  // seismo_ssg.c:38-40
+    sa.hry = (float)(1.0 / (double)e->p.dy);
+    sa.hrz = (float)(1.0 / (double)e->p.dz);
     sa.sec_tr = e->ns;
     sa.sec_comp = (long long)e->ntr * e->ns;
     sa.sec_shot = 3 * sa.sec_comp;
@@ -961,8 +986,20 @@ extern "C" int ifosb_forward(ifosb_engine *e, int nshots, const ifosb_shot *shot
     e->hess_fwd = e->nf > 0;
     e->res_ok = e->adj_ok = false;
     if ((rc = check_unstable(e, nshots))) return rc;
-    if (sections && e->ntr > 0)
-        CU(cudaMemcpy(sections, e->d_sec, sizeof(float) * (size_t)nshots * 3 * e->ntr * e->ns, cudaMemcpyDeviceToHost));
+    if (sections && e->ntr > 0) {
+        // [shot][component][ntr][ns] in saveseis's order: vx vy vz (1), p (2), div curl (3), all six (4)
+        const size_t tr = (size_t)e->ntr * e->ns;
+        static const int comps[5][7] = {{0}, {3, 0, 1, 2}, {1, 3}, {2, 4, 5}, {6, 0, 1, 2, 3, 4, 5}};
+        const int *cl = comps[e->seismo];
+        for (int sh = 0; sh < nshots; ++sh)
+            for (int q = 0; q < cl[0]; ++q) {
+                const int c = cl[q + 1];
+                const float *src = c < 3 ? e->d_sec + ((size_t)sh * 3 + c) * tr : e->d_sec2 + ((size_t)sh * 3 + c - 3) * tr;
+                CU(cudaMemcpyAsync(sections + ((size_t)sh * cl[0] + q) * tr, src, sizeof(float) * tr,
+                                   cudaMemcpyDeviceToHost, e->stream));
+            }
+        CU(cudaStreamSynchronize(e->stream));
+    }
     return check_launch(e, "forward");
 }
 

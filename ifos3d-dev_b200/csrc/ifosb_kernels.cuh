@@ -149,7 +149,30 @@ struct StrArgs {
     float b1, b2;
     float eta[MAXMECH], mb[MAXMECH], mc[MAXMECH], msb[MAXMECH];
     const float *cpg;     // global copy of the CPML rows, for lane-divergent (z-face) reads
+    int seismo;           // SEISMO: 1 particle velocities; 2, 3, 4 add p / div, curl (sec2)
+    float *sec2;          // [shot][3][ntr][ns]: p, div, curl
+    float hrx, hry, hrz;  // 1.0/DX etc. in float (seismo_ssg.c:38-40)
 };
+
+// seismo (seismo_ssg.c:48-125), SEISMO 2-4: pressure from the cell's new
+// stresses; divergence and curl from one-sided velocity differences at the cell.
+// The curl's squares are formed in double as the reference's fabs() promotes them.
+__device__ __forceinline__ void seismo_pdc(float vx, float vx_im, float vx_jp, float vx_kp, float vy, float vy_jm,
+                                           float vy_ip, float vy_kp, float vz, float vz_km, float vz_ip, float vz_jp,
+                                           float sxx, float syy, float szz, float pi, float u, float hx, float hy,
+                                           float hz, float &p, float &dv, float &cu) {
+    p = -sxx - syy - szz;
+    const float vxy = (vx_jp - vx) * hy, vxz = (vx_kp - vx) * hz;
+    const float vyx = (vy_ip - vy) * hx, vyz = (vy_kp - vy) * hz;
+    const float vzx = (vz_ip - vz) * hx, vzy = (vz_jp - vz) * hy;
+    const double t1 = (double)(vyz - vzy) * fabs((double)(vyz - vzy));
+    const double t2 = (double)(vzx - vxz) * fabs((double)(vzx - vxz));
+    const double t3 = (double)(vxy - vyx) * fabs((double)(vxy - vyx));
+    const float amp = (float)((double)u * (t1 + t2 + t3));
+    cu = (float)((amp < 0.0 ? -1 : 1) * sqrt(fabs((double)amp)));
+    const float vxx = (vx - vx_im) * hx, vyy = (vy - vy_jm) * hy, vzz = (vz - vz_km) * hz;
+    dv = (float)((double)(vxx + vyy + vzz) * sqrt((double)pi));
+}
 
 __device__ __forceinline__ void block_points(const int *pt_off, const Geo &g, int s, int yc, int &p0, int &p1) {
     p0 = p1 = 0;
@@ -495,6 +518,17 @@ __global__ void __launch_bounds__(BX *BY) k_stress(StrArgs a, int nt, int do_dft
                     o[0] = vx0;
                     o[a.sec_comp] = vy0;
                     o[2 * a.sec_comp] = vz0;
+                    if (a.seismo >= 2) {
+                        float pr, dv, cu;
+                        seismo_pdc(vx0, __ldg(vx + c - dI), __ldg(vx + c + dJ), __ldg(vx + c + 1), vy0, __ldg(vy + c - dJ),
+                                   __ldg(vy + c + dI), __ldg(vy + c + 1), vz0, __ldg(vz + c - 1), __ldg(vz + c + dI),
+                                   __ldg(vz + c + dJ), sxx, syy, szz, a.md[MD_PI * F + c], a.md[MD_U * F + c], a.hrx,
+                                   a.hry, a.hrz, pr, dv, cu);
+                        float *o2 = a.sec2 + (long long)s * a.sec_shot + (long long)pt.row * a.sec_tr + sample;
+                        o2[0] = pr;
+                        o2[a.sec_comp] = dv;
+                        o2[2 * a.sec_comp] = cu;
+                    }
                 }
             }
         }

@@ -574,6 +574,20 @@ __global__ void __maxnreg__(L == 0 ? STR_REGS_ELASTIC : STR_REGS_MECH) k_stress_
                         o[0] = vx0;
                         o[a.sec_comp] = vy0;
                         o[2 * a.sec_comp] = vz0;
+                        if (a.seismo >= 2) {
+#define RV(Rp, f, x, z) Rp[(f) * RPLANE + (x) * RZ + (z)]
+                            const long long c = widx(g, j, i, k);
+                            float pr, dv, cu;
+                            seismo_pdc(vx0, RV(R0, 0, -1, 0), RV(Rp1, 0, 0, 0), RV(R0, 0, 0, 1), vy0, RV(Rm1, 1, 0, 0),
+                                       RV(R0, 1, 1, 0), RV(R0, 1, 0, 1), vz0, RV(R0, 2, 0, -1), RV(R0, 2, 1, 0),
+                                       RV(Rp1, 2, 0, 0), sxx, syy, szz, a.md[MD_PI * F + c], a.md[MD_U * F + c], a.hrx,
+                                       a.hry, a.hrz, pr, dv, cu);
+#undef RV
+                            float *o2 = a.sec2 + (long long)s * a.sec_shot + (long long)pt.row * a.sec_tr + sample;
+                            o2[0] = pr;
+                            o2[a.sec_comp] = dv;
+                            o2[2 * a.sec_comp] = cu;
+                        }
                     }
                 }
             }

@@ -129,6 +129,7 @@ def lib():
             "ifosb_hess_apply": (C.c_int, [vp, vp, vp, vp, C.c_int, C.c_float, C.c_float, C.c_float]),
             "ifosb_resample": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float, vp,
                                          C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float]),
+            "ifosb_set_seismo": (C.c_int, [vp, C.c_int]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -152,6 +153,7 @@ def exported_symbols():
         "ifosb_write_seis", "ifosb_merge_seis", "ifosb_read_seis", "ifosb_read_seis_split",
         "ifosb_write_model", "ifosb_write_gradient", "ifosb_filt_seis", "ifosb_hessian_green", "ifosb_hessian",
         "ifosb_zero_hessian", "ifosb_get_hessian", "ifosb_read_hessian", "ifosb_hess_apply", "ifosb_resample",
+        "ifosb_set_seismo",
     ]
 
 
@@ -315,10 +317,19 @@ class Engine:
             arr[s] = Shot(sp.shape[0], _p(sp), _p(sg))
         return arr, keep
 
+    SEISMO_COMPONENTS = {1: ("vx", "vy", "vz"), 2: ("p",), 3: ("div", "curl"), 4: ("vx", "vy", "vz", "p", "div", "curl")}
+
+    def set_seismo(self, seismo):
+        """SEISMO 1-4: which components forward() records (SEISMO_COMPONENTS)."""
+        self._c(lib().ifosb_set_seismo(self.h, seismo))
+        self.seismo = seismo
+
     def forward(self, shots, want_sections=True):
-        """shots: list of (srcpos[nsrc][7], signals[nsrc][NT]). Returns [nshots][3][ntr][ns] or None."""
+        """shots: list of (srcpos[nsrc][7], signals[nsrc][NT]). Returns
+        [nshots][ncomp][ntr][ns] (ncomp = 3 for SEISMO 1) or None."""
         arr, keep = self._shots(shots)
-        out = np.zeros((len(shots), 3, self.ntr, self.ns), np.float32) if (want_sections and self.ntr) else None
+        ncomp = len(self.SEISMO_COMPONENTS[getattr(self, "seismo", 1)])
+        out = np.zeros((len(shots), ncomp, self.ntr, self.ns), np.float32) if (want_sections and self.ntr) else None
         self._c(lib().ifosb_forward(self.h, len(shots), arr, _p(out)))
         return out
 

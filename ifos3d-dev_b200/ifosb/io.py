@@ -96,19 +96,27 @@ def read_seis_split(path, keep, ns):
     return out
 
 
+# file-name tag of each SEISMO component (saveseis.c:48-63; the curl is "rot")
+SEISMO_FILES = {1: ("vx", "vy", "vz"), 2: ("p",), 3: ("div", "rot"), 4: ("vx", "vy", "vz", "p", "div", "rot")}
+
+
 def save_seis(seisfile, sections, rec, src, *, ishot, iteration, dx, dy, dz, ndt, dt, fmt=1, obs=False,
-              method=True, multiple_shots=True, trace_no=None, rank=0, nranks=1, barrier=None):
-    """saveseis() with SEISMO = 1 (particle velocities): each rank writes its
-    vx, vy, vz files, rank 0 merges the ranks' files, and the rank files are
-    removed after an inversion iteration (iteration > 0, METHOD, not observed data).
-    sections: [3][ntr][ns] of this rank. `barrier` (callable) separates the
+              method=True, multiple_shots=True, trace_no=None, rank=0, nranks=1, barrier=None, seismo=1):
+    """saveseis(): each rank writes its files of the SEISMO components (sections
+    [ncomp][ntr][ns] in Engine.forward's order), rank 0 merges the ranks' vx, vy,
+    vz files, and those rank files are removed after an inversion iteration
+    (iteration > 0, METHOD, not observed data). `barrier` (callable) separates the
     writes from the merge when several ranks share the files."""
     sections = np.asarray(sections)
     ntr, ns = sections.shape[1], sections.shape[2]
+    names = SEISMO_FILES[seismo]
+    if sections.shape[0] != len(names):
+        raise IfosbError(EARG, f"SEISMO {seismo} has {len(names)} components, got {sections.shape[0]}")
     if ntr > 0:
-        for c, name in enumerate(COMPONENTS):
+        for c, name in enumerate(names):
+            comp = {"vx": 1, "vy": 2, "vz": 3}.get(name, 0)
             write_seis(seis_rank_file(seisfile, name, iteration, fmt, ishot, rank, multiple_shots), sections[c], rec,
-                       comp=c + 1, trace_no=trace_no, src=src, dx=dx, dy=dy, dz=dz, ndt=ndt, dt=dt, fmt=fmt)
+                       comp=comp, trace_no=trace_no, src=src, dx=dx, dy=dy, dz=dz, ndt=ndt, dt=dt, fmt=fmt)
     if barrier:
         barrier()
     if rank == 0:

@@ -109,7 +109,8 @@ int ifosb_set_frequencies(ifosb_engine *e, int nf, const float *finv, int ntast)
 /* Forward propagation of nshots shots in one batch (src/ifos3d.c:738-814 per shot):
  * zeroes the wavefield, runs NT steps of update_v/_CPML, update_s(_elastic)/_CPML,
  * psource, discfourier (if nf>0), surface, seismo. sections (optional, host):
- * [nshots][3][ntr][ns] vx, vy, vz traces. DFT fields stay on the device. */
+ * [nshots][3][ntr][ns] vx, vy, vz traces, or the SEISMO components set by
+ * ifosb_set_seismo. DFT fields stay on the device. */
 int ifosb_forward(ifosb_engine *e, int nshots, const ifosb_shot *shots, float *sections);
 
 /* residual() for every shot of the last forward batch (src/ifos3d.c:837-858):
@@ -181,6 +182,13 @@ int ifosb_set_launch_shape(ifosb_engine *e, int nshots, const int *shape);
 /* Run the engine's work on the caller's CUDA stream (a cudaStream_t passed as
  * void*; NULL = the engine's own stream). Calls stay synchronous at return. */
 int ifosb_set_stream(ifosb_engine *e, void *stream);
+
+/* SEISMO (seismo_ssg.c:27-129): 1 (default) records vx, vy, vz; 2 the pressure
+ * p = -(sxx+syy+szz); 3 the divergence and curl (one-sided velocity differences,
+ * scaled by sqrt(pi) and sqrt(u) as the reference does); 4 all six. ifosb_forward's
+ * sections are then [nshots][ncomp][ntr][ns] with ncomp = 3, 1, 2, 6 in saveseis's
+ * order (vx vy vz p div curl). The residual and adjoint use vx, vy, vz. */
+int ifosb_set_seismo(ifosb_engine *e, int seismo);
 
 /* ---- approximate Hessian (HESS; src/hess_F.c, src/ifos3d.c:882-986) --------
  * Elastic models only (the reference propagates its Hessian wavefields with

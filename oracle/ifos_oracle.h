@@ -100,6 +100,12 @@ int ifo_gradient(const ifo_params *p, const float *rho, const float *pi, const f
 /* hess_F for one shot against ngreen receivers' DFT fields (reference build only). */
 int ifo_hessian(const ifo_params *p, const float *rho, const float *pi, const float *u, int nf, const float *finv,
                 const float *dft_fwd, int ngreen, const float *dft_green, float *hess);
+/* The forward with SEISMO 1-4 (reference build only): sections [3][ntr][ns],
+ * pdc [3][ntr][ns] = p, div, curl. */
+int ifo_forward_seismo(const ifo_params *p, const float *rho, const float *pi, const float *u,
+                       const float *taus, const float *taup, const float *eta, const float *cpml,
+                       int nsrc, const float *srcpos, const float *signals, int ntr, const int *recpos,
+                       int seismo, float *sections, float *pdc);
 
 #ifdef __cplusplus
 }

@@ -127,6 +127,21 @@ class Oracle:
             raise RuntimeError(f"ifo_forward rc={rc}")
         return dict(sections=sec, dft=dft, state=st)
 
+    def forward_seismo(self, p: IfoParams, m, cpml, srcpos, signals, recpos, seismo):
+        """The forward with SEISMO 1-4 (reference build): (v [3][ntr][ns], pdc [3][ntr][ns])."""
+        ns = self.nsamples(p)
+        recpos = np.ascontiguousarray(recpos, dtype=np.int32)
+        srcpos, signals = _f32(srcpos), _f32(signals)
+        sec = np.zeros((3, recpos.shape[0], ns), np.float32)
+        pdc = np.zeros((3, recpos.shape[0], ns), np.float32)
+        keep = [_f32(m["rho"]), _f32(m["pi"]), _f32(m["u"]), _f32(m.get("taus")), _f32(m.get("taup")),
+                _f32(m.get("eta")), _f32(cpml)]
+        rc = self.lib.ifo_forward_seismo(C.byref(p), *[_ptr(a) for a in keep], srcpos.shape[0], _ptr(srcpos),
+                                         _ptr(signals), recpos.shape[0], _ptr(recpos), seismo, _ptr(sec), _ptr(pdc))
+        if rc:
+            raise RuntimeError(f"ifo_forward_seismo rc={rc}")
+        return sec, pdc
+
     def residual(self, p: IfoParams, obs, syn):
         obs, syn = _f32(obs), _f32(syn)
         diff = np.zeros_like(syn)

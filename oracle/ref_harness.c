@@ -331,7 +331,8 @@ static void time_step(const ifo_params *p, refstate *s, refmodel *m, refcpml *c,
                       float **srcpos, float **sigx, float **sigy, float **sigz, int nsrc, int back,
                       float **psrc_signals, int npsrc,
                       float ****F[6], float *finv, int nf, int ntast,
-                      int ntr, int **recpos, float **sx, float **sy, float **sz, float **sdum, int *lsamp, int *nlsamp) {
+                      int ntr, int **recpos, float **sx, float **sy, float **sz, float **sdum, int *lsamp, int *nlsamp,
+                      float **sdiv, float **scurl, float **sp) {
     float **v = c->v;
     if (isnan(s->vy[NY / 2][NX / 2][NZ / 2])) err(" Simulation is unstable !");
     update_v(s->xb[0], s->xb[1], s->yb[0], s->yb[1], s->zb[0], s->zb[1], nt, s->vx, s->vy, s->vz,
@@ -372,7 +373,8 @@ static void time_step(const ifo_params *p, refstate *s, refmodel *m, refcpml *c,
                      s->rxx, s->ryy, s->rzz, s->vx, s->vy, s->vz);
     }
     if (ntr > 0 && nt == *lsamp) {
-        seismo(*nlsamp, ntr, recpos, sx, sy, sz, sdum, sdum, sdum, s->vx, s->vy, s->vz, s->sxx, s->syy, s->szz, m->pi, m->u);
+        seismo(*nlsamp, ntr, recpos, sx, sy, sz, sdiv ? sdiv : sdum, scurl ? scurl : sdum, sp ? sp : sdum, s->vx, s->vy,
+               s->vz, s->sxx, s->syy, s->szz, m->pi, m->u);
         (*nlsamp)++;
         *lsamp += NDT;
     }
@@ -410,14 +412,41 @@ static int check_params(const ifo_params *p) {
     return 0;
 }
 
+static int forward_impl(const ifo_params *p, const float *rho, const float *pi, const float *u,
+                        const float *taus, const float *taup, const float *eta, const float *cpml,
+                        int nsrc, const float *srcpos, const float *signals,
+                        int ntr, const int *recpos, int nf, const float *finv, int ntast,
+                        float *sections, float *dft, float *state9, int seismo, float *pdc);
+
 int ifo_forward(const ifo_params *p, const float *rho, const float *pi, const float *u,
                 const float *taus, const float *taup, const float *eta, const float *cpml,
                 int nsrc, const float *srcpos, const float *signals,
                 int ntr, const int *recpos, int nf, const float *finv, int ntast,
                 float *sections, float *dft, float *state9) {
+    return forward_impl(p, rho, pi, u, taus, taup, eta, cpml, nsrc, srcpos, signals, ntr, recpos, nf, finv, ntast,
+                        sections, dft, state9, 1, NULL);
+}
+
+/* The forward with SEISMO = seismo (1-4): sections [3][ntr][ns] vx, vy, vz (zero
+ * unless SEISMO is 1 or 4, as seismo() leaves them) and pdc [3][ntr][ns] p, div,
+ * curl (reference build only). */
+int ifo_forward_seismo(const ifo_params *p, const float *rho, const float *pi, const float *u,
+                       const float *taus, const float *taup, const float *eta, const float *cpml,
+                       int nsrc, const float *srcpos, const float *signals, int ntr, const int *recpos,
+                       int seismo, float *sections, float *pdc) {
+    return forward_impl(p, rho, pi, u, taus, taup, eta, cpml, nsrc, srcpos, signals, ntr, recpos, 0, NULL, 1,
+                        sections, NULL, NULL, seismo, pdc);
+}
+
+static int forward_impl(const ifo_params *p, const float *rho, const float *pi, const float *u,
+                        const float *taus, const float *taup, const float *eta, const float *cpml,
+                        int nsrc, const float *srcpos, const float *signals,
+                        int ntr, const int *recpos, int nf, const float *finv, int ntast,
+                        float *sections, float *dft, float *state9, int seismo, float *pdc) {
     int rc = check_params(p);
     if (rc) return rc;
     set_globals(p);
+    SEISMO = seismo;
     int ns = ifo_nsamples(p);
     refmodel m; model_setup(p, &m, rho, pi, u, taus, taup, eta);
     refcpml c; cpml_alloc(p, &c); cpml_load(p, &c, cpml);
@@ -438,10 +467,14 @@ int ifo_forward(const ifo_params *p, const float *rho, const float *pi, const fl
     }
     zero_state(&s);
     int lsamp = NDTSHIFT + 1, nlsamp = 1;
+    float **xd = fmatrix(1, ntr1, 1, ns1), **xc = fmatrix(1, ntr1, 1, ns1), **xp = fmatrix(1, ntr1, 1, ns1);
     for (int nt = 1; nt <= NT; nt++)
         time_step(p, &s, &m, &c, nt, sp, sig, sig, sig, nsrc, 0, sig, nsrc, F, fv, nf, ntast,
-                  ntr, rp, sx, sy, sz, sdum, &lsamp, &nlsamp);
+                  ntr, rp, sx, sy, sz, sdum, &lsamp, &nlsamp, xd, xc, xp);
+    SEISMO = 1;
     if (sections && ntr > 0) sections_out(ntr, ns, sx, sy, sz, sections);
+    if (pdc && ntr > 0) sections_out(ntr, ns, xp, xd, xc, pdc);
+    free_matrix(xd, 1, ntr1, 1, ns1); free_matrix(xc, 1, ntr1, 1, ns1); free_matrix(xp, 1, ntr1, 1, ns1);
     if (dft && nf > 0) dft_out(p, F, nf, dft);
     state_out(p, &s, state9);
     if (nf > 0) {
@@ -516,7 +549,7 @@ int ifo_adjoint(const ifo_params *p, const float *rho, const float *pi, const fl
     int lsamp = NDTSHIFT + 1, nlsamp = 1;
     for (int nt = 1; nt <= NT; nt++)
         time_step(p, &s, &m, &c, nt, back, dx, dy, dz, ntr, 1, NULL, 0, F, fv, nf, ntast,
-                  ntr, rp, sx, sy, sz, sdum, &lsamp, &nlsamp);
+                  ntr, rp, sx, sy, sz, sdum, &lsamp, &nlsamp, NULL, NULL, NULL);
     if (dft_back && nf > 0) dft_out(p, F, nf, dft_back);
     state_out(p, &s, state9);
     if (nf > 0) {
