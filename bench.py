@@ -178,9 +178,15 @@ def setup_dist(args):
     local = int(os.environ.get("LOCAL_RANK", "0"))
     dist = None
     if world > 1:
-        import torch.distributed as dist
         import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+        import torch
+        import torch.distributed as dist
+        # bind this rank's GPU before the communicator exists (barriers and
+        # collectives then run on it); the timeout bounds a rank waiting on a dead peer
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
     return world, rank, local, dist
 
 
