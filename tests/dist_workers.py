@@ -73,3 +73,29 @@ def worker(rank, world, port, mode, q):
                 dist.destroy_process_group()
             except Exception:
                 pass
+
+
+def seis_worker(rank, world, port, wdir, q):
+    """Two ranks write their receivers' SU files through ifosb.io.save_seis with a
+    gloo barrier between the writes and rank 0's merge."""
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    import torch.distributed as dist
+
+    from ifosb import io as fio
+
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=20))
+    try:
+        os.chdir(wdir)
+        ntr, ns = 3 + rank, 17
+        rng = np.random.default_rng(100 + rank)
+        secs = rng.standard_normal((3, ntr, ns)).astype(np.float32)
+        rec = np.stack([np.arange(ntr) + 5 * rank + 1, np.ones(ntr, int), np.full(ntr, 4)], 1).astype(np.int32)
+        tn = (np.arange(ntr) + 1 + 3 * rank).astype(np.int32)  # global trace numbers
+        fio.save_seis("seis", secs, rec, np.array([10.0, 2.0, 5.0], np.float32), ishot=1, iteration=0, dx=1.0,
+                      dy=1.0, dz=1.0, ndt=1, dt=1e-4, trace_no=tn, rank=rank, nranks=world, barrier=dist.barrier)
+        q.put((rank, "ok", secs))
+    except Exception as e:
+        q.put((rank, "error", repr(e)))
+    finally:
+        dist.destroy_process_group()

@@ -82,3 +82,33 @@ def test_single_rank_failure_raises():
     shots, obs = dw.make_inputs()
     with pytest.raises(ShotGradientError):
         distributed_shot_gradient(dw.FakeEngine(fail_shot=2), shots, obs, max_batch=2)
+
+
+def test_two_ranks_save_and_merge_seismograms(tmp_path):
+    """saveseis across two ranks: each rank's SU file, then rank 0's merged file
+    holding rank 0's traces followed by rank 1's (saveseis.c:86-229)."""
+    from ifosb import io as fio
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _port()
+    procs = [ctx.Process(target=dw.seis_worker, args=(r, 2, port, str(tmp_path), q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    out = {}
+    try:
+        for _ in range(2):
+            r = q.get(timeout=90)
+            out[r[0]] = r[1:]
+    finally:
+        for p in procs:
+            p.join(timeout=30)
+            if p.is_alive():
+                p.kill()
+    assert out[0][0] == "ok" and out[1][0] == "ok", out
+    for c, name in enumerate(fio.COMPONENTS):
+        merged = fio.read_seis(str(tmp_path / fio.seis_merged_file("seis", name, 0, 1, 1)), 7, 17)
+        want = np.concatenate([out[0][1][c], out[1][1][c]])
+        assert np.array_equal(merged, want)
+        raw = open(tmp_path / fio.seis_merged_file("seis", name, 0, 1, 1), "rb").read()
+        tracl = [int.from_bytes(raw[t * (240 + 68):t * (240 + 68) + 4], "little") for t in range(7)]
+        assert tracl == [1, 2, 3, 4, 5, 6, 7]
