@@ -94,7 +94,7 @@ int ifosb_filt_seis(float *data, int ntr, int ns, float finv, float dt, int orde
     if (ntr < 0 || ns < 1 || order < 1 || !(finv > 0.0f) || !(dt > 0.0f) || (ntr > 0 && !data))
         return IFOSB_EARG;
     double *s = (double *)malloc(sizeof(double) * (size_t)(ns + 1));
-    if (!s) return IFOSB_EARG;
+    if (!s) return IFOSB_ENOMEM;
     const double T0 = 1.0 / finv;
     const double t0 = T0 / (double)dt;
     for (int t = 0; t < ntr; ++t) {

@@ -29,6 +29,9 @@
 
 static int iround_d(double x) { return (int)floor(x + 0.5); }
 
+/* snprintf into a path buffer; 0 when the name did not fit. */
+#define PATH_FMT(buf, ...) (snprintf(buf, sizeof buf, __VA_ARGS__) < (int)sizeof buf)
+
 static void put32(unsigned char *h, int off, int32_t v) { memcpy(h + off, &v, 4); }
 static void put16(unsigned char *h, int off, int16_t v) { memcpy(h + off, &v, 2); }
 
@@ -112,7 +115,7 @@ int ifosb_merge_seis(const char *out, int nin, const char *const *inputs, int ns
     if (!fo) return IFOSB_EIO;
     const size_t rec = SU_HDR + 4 * (size_t)ns;
     unsigned char *buf = (unsigned char *)malloc(rec);
-    int rc = buf ? IFOSB_OK : IFOSB_EARG, total = 0;
+    int rc = buf ? IFOSB_OK : IFOSB_ENOMEM, total = 0;
     for (int r = 0; r < nin && rc == IFOSB_OK; ++r) {
         FILE *fi = inputs[r] ? fopen(inputs[r], "rb") : NULL;
         if (!fi) continue; /* saveseis.c:97: a rank without traces wrote no file */
@@ -218,11 +221,11 @@ int ifosb_write_model(const char *base, int iteration, int nx, int ny, int nz, c
     const float *r[1] = {rho};
     char path[4096];
     int rc;
-    snprintf(path, sizeof path, "%s.vp_it%d", base, iteration);
+    if (!PATH_FMT(path, "%s.vp_it%d", base, iteration)) return IFOSB_EARG;
     if ((rc = write_zxy(path, cell_vp, m, ghost, nx, ny, nz, cnt)) != IFOSB_OK) return rc;
-    snprintf(path, sizeof path, "%s.vs_it%d", base, iteration);
+    if (!PATH_FMT(path, "%s.vs_it%d", base, iteration)) return IFOSB_EARG;
     if ((rc = write_zxy(path, cell_vs, m, ghost, nx, ny, nz, cnt)) != IFOSB_OK) return rc;
-    snprintf(path, sizeof path, "%s.rho_it%d", base, iteration);
+    if (!PATH_FMT(path, "%s.rho_it%d", base, iteration)) return IFOSB_EARG;
     return write_zxy(path, cell_0, r, ghost, nx, ny, nz, cnt);
 }
 
@@ -235,7 +238,7 @@ int ifosb_write_gradient(const char *base, float finv, int iteration, int nx, in
     char path[4096];
     for (int c = 0; c < 3; ++c) {
         const float *a[1] = {grad + c * n};
-        snprintf(path, sizeof path, "%s.%s_%4.2fHz_it%d", base, name[c], finv, iteration);
+        if (!PATH_FMT(path, "%s.%s_%4.2fHz_it%d", base, name[c], finv, iteration)) return IFOSB_EARG;
         const int rc = write_zxy(path, cell_0, a, ghost, nx, ny, nz, cnt);
         if (rc != IFOSB_OK) return rc;
     }
@@ -253,7 +256,7 @@ int ifosb_read_hessian(const char *base, float finv, int iteration, int nx, int 
     const size_t n = (size_t)nx * ny * nz;
     char path[4096];
     for (int c = 0; c < 3; ++c) {
-        snprintf(path, sizeof path, "%s.%s_%4.2fHz_it%d", base, name[c], finv, iteration);
+        if (!PATH_FMT(path, "%s.%s_%4.2fHz_it%d", base, name[c], finv, iteration)) return IFOSB_EARG;
         FILE *f = fopen(path, "rb");
         if (!f) return IFOSB_EIO;
         for (int k = 1; k <= nz; ++k)

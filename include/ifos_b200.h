@@ -334,7 +334,9 @@ int ifosb_residual_noalloc(int nshots, int ntr, int ns, float dt, const float *d
 
 /* ---- on-disk formats (host; the files IFOS3D writes and reads) ------------
  * No engine and no GPU: plain C file IO in the host's byte order.
- * Return IFOSB_OK, IFOSB_EARG or IFOSB_EIO (file cannot be opened or written). */
+ * Return IFOSB_OK, IFOSB_EARG (bad argument, or a file name longer than 4095
+ * bytes), IFOSB_ENOMEM (host allocation) or IFOSB_EIO (file cannot be opened,
+ * read or written). */
 #define IFOSB_EIO 8
 
 /* One component's seismograms in the reference's format, replacing outseis()
