@@ -8,6 +8,8 @@ One iteration of src/ifos3d.c:669-1148, in its order:
   two test steps: modelupdate on a copy, forwards of NSHOTS_STEP
   shots, misfits                                                   :1021-1129
   steplength (parabola), modelupdate of the model                   :1133-1138
+With Settings.hess, the approximate Hessian of ifos3d.c:882-1002 is formed at
+iteration 1 (or read, READ_HESS) and divides the raw gradient every iteration.
 With Settings.grad_file / mod_out_file set, the gradient and model files of
 :1000 (raw), :1006 (+1000, preconditioned), :1016 (+2000, search direction) and
 :1141 (model after the update; iteration 0 at :547) are written in the
@@ -23,7 +25,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import Engine, Optimizer, Params, steplength
+from . import Engine, Optimizer, Params, steplength, wavelet
 from . import io as fio
 from . import stages as fstages
 
@@ -53,6 +55,13 @@ class Settings:
     ids: tuple = (1, 1, 1)         # IDX, IDY, IDZ of the merged model/gradient files
     filt: bool = False             # FILT = 1: low-pass source signals and observed data at each
                                    # stage's highest frequency (ifos3d.c:731, :840-855)
+    hess: bool = False             # HESS: approximate Hessian at iteration 1, applied every iteration
+    read_hess: bool = False        # READ_HESS: take it from hess_file instead (readhess)
+    read_hess_at: tuple = (0.0, 1)  # (finv, iteration) in the names of the files read
+    rec_hess: int = 1              # REC_HESS: Green's functions of the first ntr // rec_hess receivers
+    water_hess: tuple = (0.0, 0.0, 0.0)  # WATER_HESS_VP, _VS, _RHO
+    hess_file: str | None = None   # HESS_FILE
+    hess_signal: object = None     # [NT] y-force of the Hessian wavefields; None = the reference's rows
 
 
 @dataclass
@@ -83,6 +92,10 @@ class Inversion:
         self.step = np.zeros(5, np.float64)    # step[0..4] (vector(0,4): zeros)
         self.stage_i, self.it_group, self.itmax, self.iteration = -1, 0, 0, 0
         self.hist = History()
+        self.hess = None
+        if cfg.hess and cfg.read_hess:  # ifos3d.c:658
+            f, it = cfg.read_hess_at
+            self.hess = fio.read_hessian(cfg.hess_file, f, it, p.ny, p.nx, p.nz, cfg.vp0, cfg.vs0, cfg.rho0)
         if cfg.mod_out_file:
             self._write_model(0)
 
@@ -90,6 +103,23 @@ class Inversion:
     def _write_model(self, iteration):
         i = self.cfg.ids
         fio.write_model(self.cfg.mod_out_file, iteration, *self.model, ghosted=True, idx=i[0], idy=i[1], idz=i[2])
+
+    def _hess_signals(self, ntr_hess):
+        """The Hessian wavefields' y-force per receiver: wavelet(..., 5, ...) of the
+        receiver's recpos_loc column with amplitude 1 (a step at t = its trace
+        number, ifos3d.c:893-895), low-passed with FILT; or cfg.hess_signal."""
+        p, cfg = self.p, self.cfg
+        if cfg.hess_signal is not None:
+            sig = np.broadcast_to(np.asarray(cfg.hess_signal, np.float32), (ntr_hess, p.nt)).copy()
+        else:
+            rows = np.zeros((ntr_hess, 7), np.float32)
+            rows[:, :3] = self.recpos[:ntr_hess]
+            rows[:, 3] = np.arange(1, ntr_hess + 1)  # recpos_loc[4]: the trace number
+            rows[:, 5] = 1.0
+            sig = wavelet(p, 5, rows)
+        if cfg.filt:
+            sig = fstages.filt_seis(sig, float(self.finv[-1]), p.dt)
+        return sig
 
     def _filter_stage(self, fc):
         """FILT: the raw source signals and observed data low-passed at fc."""
@@ -143,13 +173,28 @@ class Inversion:
         # shot gradients and misfit[0] over the NSHOTS_STEP shots
         self._set_model(self.model)
         self.eng.zero_gradient()
+        new_hess = cfg.hess and not cfg.read_hess and self.iteration == 1
+        if new_hess:  # Hessian wavefields of ifos3d.c:882-938, once for all shots
+            ntr_hess = len(self.recpos) // cfg.rec_hess
+            self.eng.hessian_green(list(range(ntr_hess)), self._hess_signals(ntr_hess))
+            self.eng.zero_hessian()
         mis = np.zeros(len(self.shots))
         for chunk in self._batches(list(range(len(self.shots)))):
             mis[chunk] = self.eng.shot_gradient([self.shots[i] for i in chunk], self.obs[chunk])
+            if new_hess:
+                self.eng.hessian()  # hess_F of these shots (ifos3d.c:983)
         L2 = np.zeros(4, np.float64)
         L2[0] = float(np.sum(mis[self._test_shots()]))
+        if new_hess:
+            self.hess = self.eng.get_hessian()
+            if cfg.hess_file:  # ifos3d.c:996
+                fio.write_gradient(cfg.hess_file, float(self.finv[0]), self.iteration, self.hess,
+                                   idx=cfg.ids[0], idy=cfg.ids[1], idz=cfg.ids[2])
         g = self.eng.get_gradient()
         self._write_grad(g, self.iteration)
+        if cfg.hess and self.hess is not None:  # ifos3d.c:1002
+            self.opt.hess_apply(g, self.hess, np.asarray(cfg.water_hess, np.float32), lbfgs=cfg.lbfgs,
+                                vp0=cfg.vp0, vs0=cfg.vs0, rho0=cfg.rho0)
         self.opt.precon_grad(g, cfg.damptype, p.free_surf, p.fw, (p.dx, p.dy, p.dz), self.srcpos_m, self.recpos)
         self._write_grad(g, self.iteration + 1000)
         beta = None
