@@ -98,6 +98,15 @@ struct ifosb_engine {
     float *d_gsig = nullptr;   // [max_shots][3][NT] injection traces of a Green's-function batch
     float *d_hess = nullptr;   // [3][NY][NX][NZ]
     bool hess_fwd = false;     // d_dftf holds a forward batch not yet added to the Hessian
+    // time-domain gradient mode: the last forward batch's point lists (host) and
+    // device copies of its own, so the recomputation never shares the adjoint's
+    std::vector<HostPt> td_vp, td_sp;
+    std::vector<float> td_amp;
+    int *d_voff_t = nullptr, *d_soff_t = nullptr, *d_voff_a = nullptr;
+    size_t cap_voff_t = 0, cap_soff_t = 0, cap_voff_a = 0;
+    Pt *d_vpts_t = nullptr, *d_spts_t = nullptr, *d_vpts_a = nullptr;
+    size_t cap_vpts_t = 0, cap_spts_t = 0, cap_vpts_a = 0;
+    float *d_amp_t = nullptr; size_t cap_amp_t = 0;
     // TMA staging (default) and its wait-timeout flag
     int use_tma = 1;
     int *d_tma_err = nullptr;
@@ -316,7 +325,8 @@ extern "C" void ifosb_destroy(ifosb_engine *e) {
     void *bufs[] = {e->d_state, e->d_psi, e->d_model, e->d_rho_w, e->d_dftf, e->d_dftb, e->d_grad, e->d_grad64,
                     e->d_err, e->d_sec, e->d_diff, e->d_obs, e->d_part, e->d_misfit, e->d_l2, e->d_trig_f,
                     e->d_trig_b, e->d_voff, e->d_soff, e->d_vpts, e->d_spts, e->d_amp, e->d_tma_err, e->d_cpg,
-                    e->d_mstage, e->d_green, e->d_gsig, e->d_hess, e->d_sec2};
+                    e->d_mstage, e->d_green, e->d_gsig, e->d_hess, e->d_sec2, e->d_voff_t, e->d_soff_t,
+                    e->d_voff_a, e->d_vpts_t, e->d_spts_t, e->d_vpts_a, e->d_amp_t};
     for (void *b : bufs)
         if (b) cudaFree(b);
     for (cudaEvent_t ev : e->events) cudaEventDestroy(ev);
@@ -964,6 +974,9 @@ extern "C" int ifosb_forward(ifosb_engine *e, int nshots, const ifosb_shot *shot
         (rc = dgrow(e, &e->d_amp, &e->cap_amp, amp.size())))
         return rc;
     if (!amp.empty()) CU(cudaMemcpyAsync(e->d_amp, amp.data(), amp.size() * sizeof(float), cudaMemcpyHostToDevice, e->stream));
+    e->td_vp = vp;
+    e->td_sp = sp;
+    e->td_amp = amp;
     if ((rc = reset_state(e, nshots, e->d_dftf))) return rc;
     fill_common(e, L);
     VelArgs &va = L.va;
@@ -1094,6 +1107,196 @@ extern "C" int ifosb_gradient(ifosb_engine *e) {
     CU(cudaStreamSynchronize(e->stream));
     e->adj_ok = false;  // one gradient contribution per adjoint batch
     return IFOSB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Time-domain gradient kernels with checkpointing: the forward batch is run again
+// with its state saved every `interval` steps; the adjoint then runs forward in
+// its own time, and for each adjoint step the forward step it pairs with is
+// recomputed segment by segment from the nearest checkpoint (segments taken in
+// reverse). Memory: one state per checkpoint plus one segment of velocities,
+// instead of the whole time history. Plain launches, no DFT, no traces.
+static void td_step(ifosb_engine *e, const Loop &L, int nt) {
+    const dim3 grd(L.lg.ntk, L.lg.nti, L.lg.nyc * L.nshots), grdv(L.lgv.ntk, L.lgv.nti, L.lgv.nyc * L.nshots);
+    launch_vel(L, grdv, e->stream, nt);
+    launch_str(e->p.nmech, L, grd, e->stream, nt, 0, -1);
+}
+
+extern "C" int ifosb_gradient_td(ifosb_engine *e, int interval, double *kernels) {
+    if (!e || !kernels || interval < 1) return IFOSB_EARG;
+    const ifosb_params &p = e->p;
+    if (!e->fwd_ok || !e->res_ok) return fail(e, IFOSB_ESTATE, "the time-domain gradient needs a forward batch and its residual");
+    if (p.nmech != 0) return fail(e, IFOSB_EARG, "the time-domain gradient is elastic (nmech 0)");
+    if (p.ndt != 1 || p.ndtshift != 0) return fail(e, IFOSB_EARG, "the adjoint indexes the residual by step: NDT=1, NDTSHIFT=0");
+    // The adjoint's step m stands at time TIME - m DT (discfourier's backward phase), so
+    // forward step n meets it at zero lag when n + m = P = TIME / DT (nearest whole step).
+    const int NT = p.nt, P = (int)std::lround((double)p.time / (double)p.dt);
+    if (P < 2 || P > NT + 1) return fail(e, IFOSB_EARG, "TIME / DT must lie between 2 and NT + 1 steps");
+    const int nshots = e->nshots, K = std::min(interval, P - 1);
+    const long long F = e->g.field, n = (long long)p.nx * p.ny * p.nz;
+    auto al = [](size_t v) { return (v + 63) & ~(size_t)63; };  // 256-byte sub-buffers
+    const size_t ssz = (size_t)e->st_shot * nshots, psz = (size_t)e->psi_shot * nshots;  // the batch's words
+    const size_t ss = al(ssz), ps = al(psz), us = al((size_t)3 * F * nshots);
+    const int last = P - 1;                   // forward steps that pair with an adjoint step: 1..P-1
+    const int nseg = (last + K - 1) / K;      // segment q covers steps q*K+1 .. min((q+1)*K, last)
+    const size_t ck = ss + ps + us;           // one checkpoint: state, PML memory, running sums
+    const size_t seg_shot = (size_t)6 * F;    // one step of a segment: v and running sums
+    // one device block: state2 | psi2 | Uf | Ub | Uf(NT) | checkpoints 1..nseg-1 | segment
+    const size_t total = ss + ps + 3 * us + (size_t)(nseg - 1) * ck + (size_t)K * seg_shot * nshots;
+    float *blk = nullptr;
+    double *dk = nullptr;
+    CU(cudaMalloc(&blk, total * sizeof(float)));
+    cudaError_t ce = cudaMalloc(&dk, (size_t)4 * n * sizeof(double));
+    if (ce != cudaSuccess) {
+        cudaFree(blk);
+        CU(ce);
+    }
+    float *st2 = blk, *psi2 = st2 + ss, *uf = psi2 + ps, *ub = uf + us, *uf_end = ub + us, *ckp = uf_end + us;
+    float *segb = ckp + (size_t)(nseg - 1) * ck;
+    int rc = IFOSB_OK;
+    auto run = [&]() -> int {
+        CU(cudaMemsetAsync(dk, 0, (size_t)4 * n * sizeof(double), e->stream));
+        // the recomputation loop: the last forward's sources on its own state
+        Loop Lf;
+        std::memset(static_cast<void *>(&Lf), 0, sizeof(Lf));
+        Lf.nshots = nshots;
+        Lf.lg = launch_geo(e, nshots, false);
+        Lf.lgv = launch_geo(e, nshots, true);
+        int r;
+        if ((r = upload_points(e, Lf.lgv, nshots, e->td_vp, &e->d_voff_t, &e->cap_voff_t, &e->d_vpts_t, &e->cap_vpts_t)) ||
+            (r = upload_points(e, Lf.lg, nshots, e->td_sp, &e->d_soff_t, &e->cap_soff_t, &e->d_spts_t, &e->cap_spts_t)) ||
+            (r = dgrow(e, &e->d_amp_t, &e->cap_amp_t, e->td_amp.size())))
+            return r;
+        if (!e->td_amp.empty())
+            CU(cudaMemcpyAsync(e->d_amp_t, e->td_amp.data(), e->td_amp.size() * sizeof(float), cudaMemcpyHostToDevice,
+                               e->stream));
+        std::swap(e->d_state, st2);  // fill_common and the tensor maps take the engine's state pointers
+        std::swap(e->d_psi, psi2);
+        fill_common(e, Lf);
+        Lf.va.pt_off = e->td_vp.empty() ? nullptr : e->d_voff_t;
+        Lf.va.pts = e->d_vpts_t;
+        Lf.va.val = e->d_amp_t;
+        Lf.va.val_row = NT;
+        Lf.sa.pt_off = e->td_sp.empty() ? nullptr : e->d_soff_t;
+        Lf.sa.pts = e->d_spts_t;
+        Lf.sa.amp = e->d_amp_t;
+        Lf.sa.amp_row = NT;
+        {
+            const int ms = e->max_shots;  // the tensor maps cover this batch's shots only
+            e->max_shots = nshots;
+            Lf.tma = e->use_tma && setup_tma(e, Lf, nullptr);
+            e->max_shots = ms;
+        }
+        std::swap(e->d_state, st2);
+        std::swap(e->d_psi, psi2);
+        // the adjoint loop: the residual injected at the receivers, on the engine's state
+        Loop La;
+        std::memset(static_cast<void *>(&La), 0, sizeof(La));
+        La.nshots = nshots;
+        La.back = true;
+        La.lg = launch_geo(e, nshots, false);
+        La.lgv = launch_geo(e, nshots, true);
+        std::vector<HostPt> va;
+        for (int sh = 0; sh < nshots; ++sh)
+            for (int t = 0; t < e->ntr; ++t)
+                va.push_back({sh, e->rec[3 * t + 1], e->rec[3 * t], e->rec[3 * t + 2], PT_ADJOINT, sh * 3 * e->ntr + t});
+        if ((r = upload_points(e, La.lgv, nshots, va, &e->d_voff_a, &e->cap_voff_a, &e->d_vpts_a, &e->cap_vpts_a))) return r;
+        fill_common(e, La);
+        La.va.pt_off = va.empty() ? nullptr : e->d_voff_a;
+        La.va.pts = e->d_vpts_a;
+        La.va.val = e->d_diff;
+        La.va.val_row = e->ns;
+        La.va.val_comp = (long long)e->ntr * e->ns;
+        La.tma = e->use_tma && setup_tma(e, La, nullptr);
+        const int nb = 2 * 148, tb = 256;
+        auto integrate = [&](float *u, const float *st) {
+            k_td_integrate<<<nb, tb, 0, e->stream>>>(u, st, e->st_shot, F, nshots, p.dt);
+        };
+        // 1. the forward again, saving a checkpoint after steps K, 2K, ... and the sums at NT
+        CU(cudaMemsetAsync(st2, 0, ss * sizeof(float), e->stream));
+        CU(cudaMemsetAsync(psi2, 0, ps * sizeof(float), e->stream));
+        CU(cudaMemsetAsync(uf, 0, us * sizeof(float), e->stream));
+        {
+            std::vector<int> init(nshots, INT_MAX);
+            CU(cudaMemcpyAsync(e->d_err, init.data(), sizeof(int) * nshots, cudaMemcpyHostToDevice, e->stream));
+            CU(cudaMemsetAsync(e->d_tma_err, 0, sizeof(int), e->stream));
+            CU(cudaStreamSynchronize(e->stream));  // init lives on the host stack
+        }
+        for (int nt = 1; nt <= NT; ++nt) {
+            td_step(e, Lf, nt);
+            integrate(uf, st2);
+            if (nt % K == 0 && nt / K < nseg) {
+                float *c = ckp + (size_t)(nt / K - 1) * ck;
+                CU(cudaMemcpyAsync(c, st2, ss * sizeof(float), cudaMemcpyDeviceToDevice, e->stream));
+                CU(cudaMemcpyAsync(c + ss, psi2, ps * sizeof(float), cudaMemcpyDeviceToDevice, e->stream));
+                CU(cudaMemcpyAsync(c + ss + ps, uf, us * sizeof(float), cudaMemcpyDeviceToDevice, e->stream));
+            }
+        }
+        CU(cudaMemcpyAsync(uf_end, uf, us * sizeof(float), cudaMemcpyDeviceToDevice, e->stream));
+        if ((r = check_launch(e, "time-domain forward"))) return r;
+        // 2. the adjoint, with each segment of forward steps recomputed as it is reached
+        CU(cudaMemsetAsync(e->d_state, 0, ssz * sizeof(float), e->stream));
+        CU(cudaMemsetAsync(e->d_psi, 0, psz * sizeof(float), e->stream));
+        CU(cudaMemsetAsync(ub, 0, us * sizeof(float), e->stream));
+        TdArgs ta{};
+        ta.g = e->g;
+        ta.st = e->d_state;
+        ta.st_shot = e->st_shot;
+        ta.ub = ub;
+        ta.seg_shot = (long long)seg_shot;
+        ta.nshots = nshots;
+        ta.b1 = e->b1; ta.b2 = e->b2;
+        ta.rdx = p.dx; ta.rdy = p.dy; ta.rdz = p.dz;
+        ta.k = dk;
+        int ntb = 1;  // next adjoint step
+        for (int q = nseg - 1; q >= 0; --q) {
+            const int a0 = q * K + 1, a1 = std::min((q + 1) * K, last);
+            if (q == 0) {
+                CU(cudaMemsetAsync(st2, 0, ss * sizeof(float), e->stream));
+                CU(cudaMemsetAsync(psi2, 0, ps * sizeof(float), e->stream));
+                CU(cudaMemsetAsync(uf, 0, us * sizeof(float), e->stream));
+            } else {
+                const float *c = ckp + (size_t)(q - 1) * ck;
+                CU(cudaMemcpyAsync(st2, c, ss * sizeof(float), cudaMemcpyDeviceToDevice, e->stream));
+                CU(cudaMemcpyAsync(psi2, c + ss, ps * sizeof(float), cudaMemcpyDeviceToDevice, e->stream));
+                CU(cudaMemcpyAsync(uf, c + ss + ps, us * sizeof(float), cudaMemcpyDeviceToDevice, e->stream));
+            }
+            for (int m = a0; m <= a1; ++m) {
+                td_step(e, Lf, m);
+                integrate(uf, st2);
+                float *slot = segb + (size_t)(m - a0) * seg_shot * nshots;
+                for (int sh = 0; sh < nshots; ++sh) {
+                    float *d = slot + (size_t)sh * seg_shot;
+                    CU(cudaMemcpyAsync(d, st2 + (size_t)sh * e->st_shot, 3 * F * sizeof(float), cudaMemcpyDeviceToDevice,
+                                       e->stream));
+                    CU(cudaMemcpyAsync(d + 3 * F, uf + (size_t)sh * 3 * F, 3 * F * sizeof(float),
+                                       cudaMemcpyDeviceToDevice, e->stream));
+                }
+            }
+            for (int m = a1; m >= a0; --m, ++ntb) {  // adjoint steps P-a1 .. P-a0, in order
+                td_step(e, La, ntb);
+                integrate(ub, e->d_state);
+                ta.seg = segb + (size_t)(m - a0) * seg_shot * nshots;
+                k_td_corr<<<nb, tb, 0, e->stream>>>(ta);
+            }
+            if ((r = check_launch(e, "time-domain adjoint"))) return r;
+        }
+        for (; ntb <= NT; ++ntb) {  // adjoint steps past P-1 meet forward steps before the first (zero)
+            td_step(e, La, ntb);
+            integrate(ub, e->d_state);
+        }
+        k_td_dc<<<nb, tb, 0, e->stream>>>(ta, uf_end);
+        if ((r = check_launch(e, "time-domain kernels"))) return r;
+        if ((r = check_unstable(e, nshots))) return r;
+        CU(cudaMemcpyAsync(kernels, dk, (size_t)4 * n * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+        CU(cudaStreamSynchronize(e->stream));
+        return IFOSB_OK;
+    };
+    rc = run();
+    cudaStreamSynchronize(e->stream);
+    cudaFree(blk);
+    cudaFree(dk);
+    return rc;
 }
 
 // ---------------------------------------------------------------------------

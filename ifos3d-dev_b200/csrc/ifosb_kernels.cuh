@@ -620,6 +620,77 @@ __global__ void __launch_bounds__(BX *BY) k_gradient(GradArgs a) {
 }
 
 // ---------------------------------------------------------------------------
+// Time-domain gradient kernels (the optional checkpoint/recompute mode). For a
+// forward step n and the adjoint step m = P - n, P = TIME / DT (TIME = (NT-1) DT
+// after ifos3d.c:177), the pair whose discfourier phases agree (t_f - t_b =
+// n DT - (TIME - m DT) = 0), they add
+//   rho: sum_c v_f,c v_b,c                      (gradient_F's gradrho term)
+//   lambda: div U_f . div U_b                   (U = running time sum of v times DT)
+//   mu: 2 sum_i e_ii,f e_ii,b + sum_i<j (e_ij+e_ji)_f (e_ij+e_ji)_b
+// in FP64 over the interior cells, summed over the batch's shots.
+struct TdArgs {
+    Geo g;
+    const float *st;       // adjoint state [shot][slot][field] (v at slots 0..2)
+    long long st_shot;
+    const float *ub;       // adjoint running sums [shot][3][field]
+    const float *seg;      // forward v and running sums of one step [shot][6][field]
+    long long seg_shot;
+    int nshots;
+    float b1, b2, rdx, rdy, rdz;
+    double *k;             // [4][NY][NX][NZ]: rho, lambda, mu, dc
+};
+
+__global__ void k_td_corr(TdArgs a) {
+    const Geo &g = a.g;
+    const long long n = (long long)g.nx * g.ny * g.nz, F = g.field, dI = g.pz, dJ = g.plane;
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(m % g.nz) + 1, i = (int)((m / g.nz) % g.nx) + 1, j = (int)(m / ((long long)g.nz * g.nx)) + 1;
+        const long long c = widx(g, j, i, k);
+        double kr = 0.0, kl = 0.0, km = 0.0;
+        for (int s = 0; s < a.nshots; ++s) {
+            const float *vb = a.st + (long long)s * a.st_shot, *ub = a.ub + (long long)s * 3 * F;
+            const float *vf = a.seg + (long long)s * a.seg_shot, *uf = vf + 3 * F;
+            kr += (double)vf[c] * vb[c] + (double)vf[F + c] * vb[F + c] + (double)vf[2 * F + c] * vb[2 * F + c];
+            float fu[9], bu[9];
+            dft_derivs(uf, uf + F, uf + 2 * F, c, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, fu);
+            dft_derivs(ub, ub + F, ub + 2 * F, c, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, bu);
+            kl += ((double)fu[0] + fu[4] + fu[8]) * ((double)bu[0] + bu[4] + bu[8]);
+            km += 2.0 * ((double)fu[0] * bu[0] + (double)fu[4] * bu[4] + (double)fu[8] * bu[8]) +
+                  ((double)fu[1] + fu[3]) * ((double)bu[1] + bu[3]) + ((double)fu[2] + fu[6]) * ((double)bu[2] + bu[6]) +
+                  ((double)fu[5] + fu[7]) * ((double)bu[5] + bu[7]);
+        }
+        a.k[m] += kr;
+        a.k[n + m] += kl;
+        a.k[2 * n + m] += km;
+    }
+}
+
+// The zero-frequency product of the two runs: sum_c U_f,c(NT) U_b,c(NT).
+__global__ void k_td_dc(TdArgs a, const float *uf_end) {
+    const Geo &g = a.g;
+    const long long n = (long long)g.nx * g.ny * g.nz, F = g.field;
+    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(m % g.nz) + 1, i = (int)((m / g.nz) % g.nx) + 1, j = (int)(m / ((long long)g.nz * g.nx)) + 1;
+        const long long c = widx(g, j, i, k);
+        double d = 0.0;
+        for (int s = 0; s < a.nshots; ++s) {
+            const float *uf = uf_end + (long long)s * 3 * F, *ub = a.ub + (long long)s * 3 * F;
+            d += (double)uf[c] * ub[c] + (double)uf[F + c] * ub[F + c] + (double)uf[2 * F + c] * ub[2 * F + c];
+        }
+        a.k[3 * n + m] += d;
+    }
+}
+
+// U += v * DT over every shot's three velocity fields (whole padded fields).
+__global__ void k_td_integrate(float *u, const float *st, long long st_shot, long long F, int nshots, float dt) {
+    const long long per = 3 * F, total = per * nshots;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total; q += (long long)gridDim.x * blockDim.x) {
+        const long long s = q / per, r = q % per;
+        u[q] += st[s * st_shot + r] * dt;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // hess_F (hess_F.c:67-155): the diagonal approximate Hessian from the forward DFT
 // fields of every shot of the batch (in order) and the DFT fields of the
 // receivers' Green's functions (wavefields of a y-force at each receiver), for

@@ -79,6 +79,7 @@ def lib():
             "ifosb_residual": (C.c_int, [vp, vp, vp, vp]),
             "ifosb_adjoint": (C.c_int, [vp, vp]),
             "ifosb_gradient": (C.c_int, [vp]),
+            "ifosb_gradient_td": (C.c_int, [vp, C.c_int, vp]),
             "ifosb_zero_gradient": (C.c_int, [vp]),
             "ifosb_get_gradient": (C.c_int, [vp, vp, vp]),
             "ifosb_shot_gradient": (C.c_int, [vp, C.c_int, C.POINTER(Shot), vp, vp]),
@@ -153,7 +154,7 @@ def exported_symbols():
         "ifosb_write_seis", "ifosb_merge_seis", "ifosb_read_seis", "ifosb_read_seis_split",
         "ifosb_write_model", "ifosb_write_gradient", "ifosb_filt_seis", "ifosb_hessian_green", "ifosb_hessian",
         "ifosb_zero_hessian", "ifosb_get_hessian", "ifosb_read_hessian", "ifosb_hess_apply", "ifosb_resample",
-        "ifosb_set_seismo",
+        "ifosb_set_seismo", "ifosb_gradient_td",
     ]
 
 
@@ -367,6 +368,14 @@ class Engine:
 
     def zero_gradient(self):
         self._c(lib().ifosb_zero_gradient(self.h))
+
+    def gradient_td(self, interval):
+        """Time-domain kernels of the last forward batch and its residual with a
+        checkpoint every `interval` steps: float64 [4, NY, NX, NZ] = rho, lambda,
+        mu and the zero-frequency product (sums over the batch's shots)."""
+        k = np.zeros((4, self.p.ny, self.p.nx, self.p.nz), np.float64)
+        self._c(lib().ifosb_gradient_td(self.h, int(interval), _p(k)))
+        return k
 
     # -- approximate Hessian (hess_F) -----------------------------------------
     def hessian_green(self, rec_ids, signals):

@@ -131,6 +131,23 @@ int ifosb_adjoint(ifosb_engine *e, const float *diff);
  * loop): FP32 exactly as the reference, and a parallel FP64 accumulation. */
 int ifosb_gradient(ifosb_engine *e);
 
+/* Time-domain gradient kernels of the last forward batch and its residual, with
+ * checkpointing instead of the DFT: the forward is run again saving its state
+ * every `interval` steps, the residual is back-propagated, and each forward step
+ * is recomputed from the nearest checkpoint, one segment at a time, when its
+ * zero-lag adjoint step (n + m = TIME/DT, the pairing of discfourier's phases,
+ * src/disc_fourier.c:36-37) is reached. kernels[4][NY][NX][NZ] (FP64, summed over
+ * the batch's shots): rho  sum_t v_f . v_b;  lambda  sum_t div U_f div U_b;
+ * mu  sum_t (2 sum_i e_ii,f e_ii,b + sum_i<j (e_ij+e_ji)_f (e_ij+e_ji)_b), with U
+ * the running sum of v DT and e the gradient_F stencils of U; dc  U_f(NT) . U_b(NT).
+ * With frequencies f_l = l / (2 NT DT) the rho kernel equals (by Parseval)
+ * (dc + 2 sum_{l=1}^{NT-1} gradrho_l + gradrho_NT) / (2 NT DT^2), gradrho_l being
+ * gradient_F's rho term. Elastic (NMECH 0), NDT 1, NDTSHIFT 0. Device memory:
+ * ceil((TIME/DT - 1)/interval) checkpoints of the batch state plus `interval` steps
+ * of six fields per shot. The DFT fields, traces and residual stay as they were;
+ * the wavefield state (ifosb_get_field) is the time-domain adjoint's last step. */
+int ifosb_gradient_td(ifosb_engine *e, int interval, double *kernels);
+
 /* Zero the accumulated gradients (zero_grad, src/zero_grad.c). */
 int ifosb_zero_gradient(ifosb_engine *e);
 
