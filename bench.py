@@ -1,7 +1,7 @@
 #!/usr/bin/env python
 """Benchmark of the B200 IFOS3D wavefield engine.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload visco256|elastic128]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload visco256|elastic128|visco384]
                     [--impl ours|reference]
 
 A step is one pass of the hot path over one batch of synthetic input:
@@ -11,6 +11,11 @@ A step is one pass of the hot path over one batch of synthetic input:
              across ranks, no data-path collective: weak scaling).
   elastic128 one shot-gradient (forward + residual + adjoint + DFT gradient),
              128^3, NT=2000, 2 frequencies.
+  visco384   the batched multi-shot gradient: 32 viscoelastic (L=3) shot-gradients
+             (4 frequencies, 1024 receivers) on 384 x 256 x 384 cells, in
+             HBM-sized batches of shots that share one launch; NT=200 by default
+             (the configuration names no NT). Shots shard across ranks; one FP64
+             all-reduce of gradient and misfits per step.
 metric: cell-updates per second over all ranks (all NX*NY*NZ cells of every
 shot and time step, CPML frame included; forward and adjoint both count).
 
@@ -221,7 +226,14 @@ def reference_arm(args, world, rank, dist):
     }), flush=True)
 
 
-def workload_config(wl, world):
+def workload_config(wl, world, nt=None):
+    if wl == "visco384":
+        return {"workload": "visco384: batched viscoelastic L=3 (Q=50, 20-200 Hz) shot-gradients (forward+residual+"
+                            f"adjoint+DFT gradient), 384x256x384 cells, NT={nt or 200}, 4 frequencies, 32 shots on an "
+                            "8x4 surface grid, 1024 receivers, 3 Gaussian blobs in a depth gradient",
+                "grid": [384, 256, 384], "nt": nt or 200, "nmech": 3, "nf": 4, "shots": 32, "receivers": 1024,
+                "parallelism": f"shot-sharded x{world}, FP64 gradient all-reduce per step",
+                "l2_flush": "state+DFT about 11 GB per shot > 126 MB L2"}
     if wl == "visco256":
         return {"workload": "visco256: viscoelastic L=3 (Q=50, 20-200 Hz) forward modelling, 256^3 cells, "
                             "NT=3000, 8 layers, sin^3 fc=80 Hz, 400 receivers, 1 shot per GPU",
@@ -239,7 +251,7 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="visco256", choices=["visco256", "elastic128"])
+    ap.add_argument("--workload", default="visco256", choices=["visco256", "elastic128", "visco384"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nt", type=int, default=None, help="override NT (testing only)")
     ap.add_argument("--no-cpu", action="store_true")
@@ -253,6 +265,13 @@ def main():
     world, rank, local, dist = setup_dist(args)
     if args.impl == "reference":
         reference_arm(args, world, rank, dist)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    if args.workload == "visco384":
+        batched_gradient_workload(args, world, rank, local, dist)
         if dist:
             dist.barrier()
             dist.destroy_process_group()
@@ -436,6 +455,147 @@ def main():
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def batched_gradient_workload(args, world, rank, local, dist):
+    """visco384: every rank takes its share of the 32 shots in batches as large as
+    its HBM holds (one launch per kernel and time step for a whole batch, the time
+    loop replayed from a CUDA graph); a step is the gradient of all 32 shots,
+    host observed traces in and the summed FP64 gradient out on every rank."""
+    import torch
+    import ifosb
+    from ifosb import synth
+    from ifosb.dist import batches, distributed_shot_gradient, shard
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    nt = args.nt or 200
+    c = synth.case("visco384", nt=nt)
+    p = c["params"]
+    m, cp, shots = synth.build_inputs(c)
+    nf, nshots = len(c["finv"]), len(shots)
+    mine = shard(nshots, world, rank)
+
+    def engine(nb, mode=0):
+        e = ifosb.Engine(p, max_shots=nb, max_nf=nf)
+        e.set_stream(stream.cuda_stream)
+        e.set_launch_mode(mode)
+        e.set_cpml(cp)
+        e.set_model(m["rho"], m["pi"], m["u"], m["taus"], m["taup"], m["eta"])
+        e.set_receivers(c["recpos"])
+        e.set_frequencies(c["finv"], c["ntast"])
+        return e
+
+    # batch size: the shots this GPU's free memory holds next to a 6 GB margin
+    e = engine(1)
+    b1 = e.device_bytes
+    e.close()
+    e = engine(2)
+    per_shot = e.device_bytes - b1
+    e.close()
+    free, _ = torch.cuda.mem_get_info(dev)
+    cap = max(1, int((free - 6e9 - (b1 - per_shot)) // per_shot))
+    nbatch = -(-len(mine) // min(cap, len(mine)))
+    B = -(-len(mine) // nbatch)
+    eng = engine(B)
+    tuned = eng.autotune([shots[i] for i in mine[:B]], steps=min(40, p.nt))
+    last = len(mine) - (nbatch - 1) * B
+    if last != B:  # a shorter last batch gets its own launch shape
+        eng.autotune([shots[i] for i in mine[-last:]], steps=min(40, p.nt))
+    # observed data: this rank's shots modelled in the same (true = start) model and
+    # scaled, so that the residual is not zero; other ranks' entries are placeholders
+    obs = np.zeros((nshots, 3, eng.ntr, eng.ns), np.float32)
+    for chunk in batches(mine, B):
+        obs[chunk] = eng.forward([shots[i] for i in chunk]) * np.float32(0.9)
+
+    def step():
+        return distributed_shot_gradient(eng, shots, obs, max_batch=B, dist=dist)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            grad, mis = step()
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+        if dist:
+            dist.barrier()
+    clocks = clk.summary()
+    ms = ev0.elapsed_time(ev1)
+    if dist:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ncell = p.nx * p.ny * p.nz
+    cells = 2 * ncell * p.nt * nshots * args.steps
+    value = cells / (ms / 1000.0) / 1e9
+    launches = args.steps * nbatch * (4 * p.nt + 3)
+
+    # roofline: per-kernel CUDA events over one profiled batched forward (with DFT)
+    eng.set_profiling(True)
+    eng.forward([shots[i] for i in mine[:B]], want_sections=False)
+    tv, ts, nsteps = eng.kernel_times()
+    eng.shot_gradient([shots[i] for i in mine[:B]], obs[mine[:B]])
+    atv, ats, ansteps = eng.kernel_times()  # the adjoint loop of that shot-gradient
+    eng.set_profiling(False)
+    b = alg_bytes_per_cell_step(p, nf, c["ntast"])
+    peak, peak_kind = load_peaks()
+    cb = ncell * B
+    ach = b["total"] * cb / ((tv + ts) / nsteps / 1000.0) / 1e9
+    ach_s = b["stress"] * cb / (ts / nsteps / 1000.0) / 1e9
+    ach_v = b["vel"] * cb / (tv / nsteps / 1000.0) / 1e9
+    roofline = {"bound": "hbm", "kernel": f"time step of a {B}-shot batch = k_velocity + k_stress<3> with DFT",
+                "achieved": round(ach, 1), "peak": peak, "unit": "GB/s", "frac": round(ach / peak, 4),
+                "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
+                "traffic": None, "alg_bytes_per_cell_step": round(b["total"], 2),
+                "per_kernel": {"k_stress": {"alg_bytes_per_cell": round(b["stress"], 2), "ms": round(ts / nsteps, 4),
+                                            "achieved_gbs": round(ach_s, 1), "frac": round(ach_s / peak, 4)},
+                               "k_velocity": {"alg_bytes_per_cell": round(b["vel"], 2), "ms": round(tv / nsteps, 4),
+                                              "achieved_gbs": round(ach_v, 1), "frac": round(ach_v / peak, 4)}},
+                "adjoint_ms_per_step": {"k_stress": round(ats / ansteps, 4), "k_velocity": round(atv / ansteps, 4)}}
+    out = {
+        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 2), "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": dict(workload_config("visco384", world, p.nt), shots_per_batch=B, batches_per_gpu=nbatch,
+                       launch_shape=dict(tuned, picked_by="ifosb_autotune")),
+        "clocks": clocks,
+        "e2e": {"value": round(value, 3), "unit": UNIT, "note": "the step itself is end to end: host observed "
+                "traces in, the summed FP64 gradient out", "h2d_bytes_per_step": int(obs[mine].nbytes),
+                "d2h_bytes_per_step": int(grad.nbytes + mis.nbytes)},
+        "gpu_launches": int(launches), "roofline": roofline,
+        "shot_gradients_per_s": round(nshots * args.steps / (ms / 1000.0), 4),
+    }
+    eng.close()
+    # one shot per launch sequence (plain launches) on the same GPU, two shots timed
+    if rank == 0 and world == 1 and not args.no_extras:
+        e1 = engine(1, 1)
+        e1.shot_gradient(shots[:1], obs[:1])
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        for s in range(2):
+            e1.shot_gradient(shots[s:s + 1], obs[s:s + 1])
+        torch.cuda.synchronize(dev)
+        t1 = (time.perf_counter() - t0) / 2
+        e1.close()
+        out["per_shot_path"] = {"shot_gradients_per_s": round(1.0 / t1, 4),
+                                "batched_speedup": round(t1 * nshots * args.steps / (ms / 1000.0), 3),
+                                "timing": "host wall clock around 2 synchronised one-shot gradients"}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        code, kind = cpu_kind(p.nmech)
+        grid, cnt = (64, 64, 64), args.cpu_nt
+        v1, _, _ = cpu_run(code, p.nmech, 1, grid, cnt)
+        out["cpu_baseline"] = {"value": round(v1, 5), "unit": UNIT, "cores": 1, "kind": kind,
+                               "sample": f"one core, {grid[0]}x{grid[1]}x{grid[2]} grid x {cnt} steps of the "
+                                         f"same forward step (L={p.nmech}, FW=10 CPML, free surface)"}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
 
 
 def shot_gradient_comparison(torch, ifosb, synth, dev, stream, nt_override, nshots=4):

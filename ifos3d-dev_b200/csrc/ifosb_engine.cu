@@ -557,27 +557,42 @@ struct Loop {
     size_t vel_smem = 0, str_smem = 0;
 };
 
-// y planes per CTA: long chunks amortise the ring prologue; enough chunks keep
-// about four CTAs per SM in flight over the whole batch.
+// The launch shape for a batch of nshots: the autotuner's for that batch size,
+// else the one tuned for the nearest batch size (the larger on a tie), else null.
+static const ifosb_engine::Shape *shape_for(const ifosb_engine *e, int nshots) {
+    if (e->tuned.empty()) return nullptr;
+    auto hi = e->tuned.lower_bound(nshots);
+    if (hi != e->tuned.end() && hi->first == nshots) return &hi->second;
+    if (hi == e->tuned.begin()) return &hi->second;
+    auto lo = std::prev(hi);
+    if (hi == e->tuned.end() || nshots - lo->first < hi->first - nshots) return &lo->second;
+    return &hi->second;
+}
+
+// y planes per CTA. Untuned, with no other batch size tuned either: enough chunks
+// for about four CTAs per SM over the whole batch, 8 to 16 planes each (the
+// autotuner picked 3 to 32 on 128^3 to 384x256x384 grids; chunks of 64 planes ran
+// a 10-shot 384x256x384 batch 60 % slower than its tuned shape).
 static Geo launch_geo(const ifosb_engine *e, int nshots, bool vel) {
     Geo g = e->g;
     if (vel) {
         g.by = e->vby;
         g.nti = (g.nx + g.by - 1) / g.by;
     }
-    auto t = e->tuned.find(nshots);
-    if (t != e->tuned.end()) {
-        g.cy = vel ? t->second.cyv : t->second.cys;
-        g.nyc = (g.ny + g.cy - 1) / g.cy;
-        return g;
+    int cy;
+    if (const ifosb_engine::Shape *t = shape_for(e, nshots)) {
+        cy = vel ? t->cyv : t->cys;
+    } else {
+        int dev = 0, sms = 148;
+        if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaGetLastError();
+        const long long per_set = (long long)g.ntk * g.nti * nshots;
+        const long long chunks = std::max<long long>(1, (4LL * sms + per_set - 1) / per_set);
+        cy = (int)((g.ny + chunks - 1) / chunks);
+        cy = std::min(std::max(cy, DEFAULT_CY), 16);
     }
-    int dev = 0, sms = 148;
-    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaGetLastError();
-    const long long per_set = (long long)g.ntk * g.nti * nshots;
-    const long long chunks = std::max<long long>(1, (4LL * sms + per_set - 1) / per_set);
-    int cy = (int)((g.ny + chunks - 1) / chunks);
-    cy = std::min(std::max(cy, DEFAULT_CY), 64);
+    cy = std::min(cy, g.ny);
+    while (cy < g.ny && (long long)((g.ny + cy - 1) / cy) * nshots > 65535) ++cy;  // grid.z limit
     g.cy = cy;
     g.nyc = (g.ny + cy - 1) / cy;
     return g;
@@ -731,9 +746,9 @@ static bool setup_tma(ifosb_engine *e, Loop &L, float *dft) {
     L.stt.a = L.sa;
     L.vt.tma_err = L.stt.tma_err = e->d_tma_err;
     {
-        auto t = e->tuned.find(L.nshots);
-        L.vt.l2ahead = t != e->tuned.end() ? t->second.l2v : L2AHEAD_DEFAULT;
-        L.stt.l2ahead = t != e->tuned.end() ? t->second.l2s : L2AHEAD_DEFAULT;
+        const ifosb_engine::Shape *t = shape_for(e, L.nshots);
+        L.vt.l2ahead = t ? t->l2v : L2AHEAD_VEL_DEFAULT;
+        L.stt.l2ahead = t ? t->l2s : L2AHEAD_STR_DEFAULT;
     }
     L.stt.nsr = nsr;
     L.stt.nm = nm;
@@ -1535,7 +1550,9 @@ extern "C" int ifosb_autotune(ifosb_engine *e, int nshots, const ifosb_shot *sho
     std::sort(cys.begin(), cys.end());
     cys.erase(std::unique(cys.begin(), cys.end()), cys.end());
     double bv = 1e30, bs = 1e30;
-    ifosb_engine::Shape pick{hv.cy, L2AHEAD_DEFAULT, hs.cy, L2AHEAD_DEFAULT};
+    const ifosb_engine::Shape *near = shape_for(e, nshots);
+    ifosb_engine::Shape pick{hv.cy, near ? near->l2v : L2AHEAD_VEL_DEFAULT, hs.cy,
+                             near ? near->l2s : L2AHEAD_STR_DEFAULT};
     int rc = IFOSB_OK;
     e->profile = 1;
     e->nt_limit = steps;

@@ -138,7 +138,10 @@ __device__ __forceinline__ void tma_prefetch4(const CUtensorMap *m, int c0, int 
 
 // Planes are prefetched into L2 `l2ahead` iterations before their shared-memory
 // load (a launch argument, 0 = no L2 prefetch; the engine's autotuner picks it).
-constexpr int L2AHEAD_DEFAULT = 3;
+// Untuned defaults: the distances the autotuner picked on 128^3 to 384x256x384
+// grids (velocity 1-2, stress 1 every time).
+constexpr int L2AHEAD_VEL_DEFAULT = 2;
+constexpr int L2AHEAD_STR_DEFAULT = 1;
 
 // Tensor-map coordinates of a cell: z index k+7, row i+1, plane j+2.
 __device__ __forceinline__ int zc(int k) { return k + 7; }
