@@ -53,6 +53,7 @@ struct ifosb_engine {
     float *d_model = nullptr;  float *d_rho_w = nullptr;
     float *d_dftf = nullptr, *d_dftb = nullptr; long long dft_shot = 0;
     float *d_grad = nullptr;   double *d_grad64 = nullptr;
+    double *d_gradq = nullptr;  // viscoelastic: FP64 gradients with respect to taup and taus
     int *d_err = nullptr;
     // receivers and traces
     int ntr = 0, ns = 0;
@@ -296,6 +297,11 @@ extern "C" int ifosb_create(const ifosb_params *p, int max_shots, int max_nf, if
         ifosb_destroy(e);
         return rc;
     }
+    if (p->nmech > 0 && (rc = dalloc(e, &e->d_gradq, (size_t)(2 * ncell)))) {
+        ifosb_destroy(e);
+        return rc;
+    }
+    if (e->d_gradq) cudaMemsetAsync(e->d_gradq, 0, sizeof(double) * 2 * ncell, e->stream);
     if (max_nf > 0) {
         if ((rc = dalloc(e, &e->d_dftf, (size_t)(e->dft_shot * max_shots))) ||
             (rc = dalloc(e, &e->d_dftb, (size_t)(e->dft_shot * max_shots)))) {
@@ -326,7 +332,7 @@ extern "C" void ifosb_destroy(ifosb_engine *e) {
                     e->d_err, e->d_sec, e->d_diff, e->d_obs, e->d_part, e->d_misfit, e->d_l2, e->d_trig_f,
                     e->d_trig_b, e->d_voff, e->d_soff, e->d_vpts, e->d_spts, e->d_amp, e->d_tma_err, e->d_cpg,
                     e->d_mstage, e->d_green, e->d_gsig, e->d_hess, e->d_sec2, e->d_voff_t, e->d_soff_t,
-                    e->d_voff_a, e->d_vpts_t, e->d_spts_t, e->d_vpts_a, e->d_amp_t};
+                    e->d_voff_a, e->d_vpts_t, e->d_spts_t, e->d_vpts_a, e->d_amp_t, e->d_gradq};
     for (void *b : bufs)
         if (b) cudaFree(b);
     for (cudaEvent_t ev : e->events) cudaEventDestroy(ev);
@@ -1115,6 +1121,22 @@ extern "C" int ifosb_gradient(ifosb_engine *e) {
     a.rdx = p.dx; a.rdy = p.dy; a.rdz = p.dz;
     a.grad = e->d_grad;
     a.grad64 = e->d_grad64;
+    a.gradq = p.nmech > 0 ? e->d_gradq : nullptr;
+    for (int l = 0; l < e->nf; ++l) {
+        const double w = 2.0 * M_PI * (double)e->finv[l];
+        double re = 0.0, im = 0.0;
+        for (int q = 0; q < p.nmech; ++q) {
+            if (!(e->eta[q] > 0.f)) {  // no relaxation: the term is 1 (the unrelaxed modulus)
+                re += 1.0;
+                continue;
+            }
+            const double ts = (double)p.dt / (double)e->eta[q], wt = w * ts, den = 1.0 + wt * wt;
+            re += wt * wt / den;  // s ts / (1 + s ts) with s = -i w (discfourier's e^{+i w t})
+            im -= wt / den;
+        }
+        a.rphi[l] = re;
+        a.iphi[l] = im;
+    }
     dim3 blk(BX, BY), grd(e->g.ntk, e->g.nti, e->g.nyc);
     k_gradient<<<grd, blk, 0, e->stream>>>(a);
     int rc = check_launch(e, "gradient");
@@ -1446,6 +1468,16 @@ extern "C" int ifosb_zero_gradient(ifosb_engine *e) {
     const size_t n = (size_t)3 * e->p.nx * e->p.ny * e->p.nz;
     CU(cudaMemsetAsync(e->d_grad, 0, n * sizeof(float), e->stream));
     CU(cudaMemsetAsync(e->d_grad64, 0, n * sizeof(double), e->stream));
+    if (e->d_gradq) CU(cudaMemsetAsync(e->d_gradq, 0, n / 3 * 2 * sizeof(double), e->stream));
+    CU(cudaStreamSynchronize(e->stream));
+    return IFOSB_OK;
+}
+
+extern "C" int ifosb_get_gradient_q(ifosb_engine *e, double *gradq) {
+    if (!e || !gradq) return IFOSB_EARG;
+    if (!e->d_gradq) return fail(e, IFOSB_ESTATE, "the Q gradient needs a viscoelastic engine (nmech > 0)");
+    const size_t n = (size_t)2 * e->p.nx * e->p.ny * e->p.nz;
+    CU(cudaMemcpyAsync(gradq, e->d_gradq, n * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
     CU(cudaStreamSynchronize(e->stream));
     return IFOSB_OK;
 }

@@ -551,6 +551,11 @@ struct GradArgs {
     float b1, b2, rdx, rdy, rdz;
     float *grad;
     double *grad64;
+    // viscoelastic only: gradients with respect to taup and taus ([2][NY][NX][NZ],
+    // FP64), with Phi(omega_l) = sum_m s tau_m / (1 + s tau_m), s = -i omega_l,
+    // tau_m = DT / eta_m (the memory-variable relaxation of update_s_ssg.c:108-122)
+    double *gradq;
+    double rphi[MAXNF], iphi[MAXNF];
 };
 
 __device__ __forceinline__ void dft_derivs(const float *X, const float *Y, const float *Z, long long c, long long dI,
@@ -581,6 +586,11 @@ __global__ void __launch_bounds__(BX *BY) k_gradient(GradArgs a) {
         const long long m = ((long long)(j - 1) * g.nx + (i - 1)) * g.nz + (k - 1);
         float g1 = a.grad[m], g2 = a.grad[n + m], g3 = a.grad[2 * n + m];
         double h1 = a.grad64[m], h2 = a.grad64[n + m], h3 = a.grad64[2 * n + m];
+        double qp = 0.0, qs = 0.0;
+        if (a.gradq) {
+            qp = a.gradq[m];
+            qs = a.gradq[n + m];
+        }
         const float r = a.rho[c], pp = a.md[MD_PI * F + c], uu = a.md[MD_U * F + c];
         const double sqp = sqrt((double)(r * pp)), squ = sqrt((double)(r * uu));
         for (int s = 0; s < a.nshots; ++s) {
@@ -612,10 +622,41 @@ __global__ void __launch_bounds__(BX *BY) k_gradient(GradArgs a) {
                 h1 += c1;
                 h2 += c2;
                 h3 += (double)c3;
+                if (a.gradq) {
+                    // complex correlations C = F conj(B) of the lambda and mu terms with
+                    // gradient_F's factor -fdummy: its gradlam / gradmu are their real
+                    // parts. A modulus M(1 + tau Phi) perturbed in tau moves the misfit
+                    // by Re[M Phi C] (lambda part for taup; mu - 2 lambda for taus).
+                    const double fd = -(double)fdummy;
+                    const double dfr = (double)fv[0] + fv[4] + fv[8], dfi = (double)fi[0] + fi[4] + fi[8];
+                    const double dbr = (double)bv[0] + bv[4] + bv[8], dbi = (double)bi[0] + bi[4] + bi[8];
+                    const double rl = fd * (dfr * dbr + dfi * dbi), il = fd * (dfi * dbr - dfr * dbi);
+                    double rm = 0.0, im = 0.0;
+                    for (int q = 0; q < 9; q += 4) {  // xx, yy, zz
+                        rm += 2.0 * ((double)fv[q] * bv[q] + (double)fi[q] * bi[q]);
+                        im += 2.0 * ((double)fi[q] * bv[q] - (double)fv[q] * bi[q]);
+                    }
+                    const int pr[3][2] = {{1, 3}, {2, 6}, {5, 7}};  // xy, xz, yz
+                    for (int q = 0; q < 3; ++q) {
+                        const double fr = (double)fv[pr[q][0]] + fv[pr[q][1]], fim = (double)fi[pr[q][0]] + fi[pr[q][1]];
+                        const double br = (double)bv[pr[q][0]] + bv[pr[q][1]], bim = (double)bi[pr[q][0]] + bi[pr[q][1]];
+                        rm += fr * br + fim * bim;
+                        im += fim * br - fr * bim;
+                    }
+                    rm *= fd;
+                    im *= fd;
+                    const double ph = a.rphi[l], qh = a.iphi[l];
+                    qp += (double)pp * (ph * rl - qh * il);
+                    qs += (double)uu * (ph * (rm - 2.0 * rl) - qh * (im - 2.0 * il));
+                }
             }
         }
         a.grad[m] = g1; a.grad[n + m] = g2; a.grad[2 * n + m] = g3;
         a.grad64[m] = h1; a.grad64[n + m] = h2; a.grad64[2 * n + m] = h3;
+        if (a.gradq) {
+            a.gradq[m] = qp;
+            a.gradq[n + m] = qs;
+        }
     }
 }
 

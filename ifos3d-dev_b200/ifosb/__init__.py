@@ -80,6 +80,7 @@ def lib():
             "ifosb_adjoint": (C.c_int, [vp, vp]),
             "ifosb_gradient": (C.c_int, [vp]),
             "ifosb_gradient_td": (C.c_int, [vp, C.c_int, vp]),
+            "ifosb_get_gradient_q": (C.c_int, [vp, vp]),
             "ifosb_zero_gradient": (C.c_int, [vp]),
             "ifosb_get_gradient": (C.c_int, [vp, vp, vp]),
             "ifosb_shot_gradient": (C.c_int, [vp, C.c_int, C.POINTER(Shot), vp, vp]),
@@ -154,7 +155,7 @@ def exported_symbols():
         "ifosb_write_seis", "ifosb_merge_seis", "ifosb_read_seis", "ifosb_read_seis_split",
         "ifosb_write_model", "ifosb_write_gradient", "ifosb_filt_seis", "ifosb_hessian_green", "ifosb_hessian",
         "ifosb_zero_hessian", "ifosb_get_hessian", "ifosb_read_hessian", "ifosb_hess_apply", "ifosb_resample",
-        "ifosb_set_seismo", "ifosb_gradient_td",
+        "ifosb_set_seismo", "ifosb_gradient_td", "ifosb_get_gradient_q",
     ]
 
 
@@ -369,6 +370,13 @@ class Engine:
     def zero_gradient(self):
         self._c(lib().ifosb_zero_gradient(self.h))
 
+    def get_gradient_q(self):
+        """Viscoelastic: FP64 gradients with respect to taup and taus, [2, NY, NX, NZ]
+        (gradient_F's sign: minus the misfit gradient)."""
+        g = np.zeros((2, self.p.ny, self.p.nx, self.p.nz), np.float64)
+        self._c(lib().ifosb_get_gradient_q(self.h, _p(g)))
+        return g
+
     def gradient_td(self, interval):
         """Time-domain kernels of the last forward batch and its residual with a
         checkpoint every `interval` steps: float64 [4, NY, NX, NZ] = rho, lambda,
@@ -531,3 +539,11 @@ def steplength(L2, step, lbfgs=False, it_group=1, teststep=0.0):
     abc = np.zeros(3, np.float64)
     _check(None, lib().ifosb_steplength(_p(L2), _p(step), int(bool(lbfgs)), it_group, teststep, _p(abc)))
     return abc
+
+
+def q_gradient(gradq, taup, taus, q):
+    """d/dQ from get_gradient_q's taup / taus gradients when both tau scale as 1/Q
+    (the tau method): -(taup d/dtaup + taus d/dtaus) / Q, per cell (q scalar or
+    [NY, NX, NZ])."""
+    g = np.asarray(gradq, np.float64)
+    return -(np.asarray(taup, np.float64) * g[0] + np.asarray(taus, np.float64) * g[1]) / np.asarray(q, np.float64)

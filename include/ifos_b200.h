@@ -148,6 +148,19 @@ int ifosb_gradient(ifosb_engine *e);
  * the wavefield state (ifosb_get_field) is the time-domain adjoint's last step. */
 int ifosb_gradient_td(ifosb_engine *e, int interval, double *kernels);
 
+/* Viscoelastic engines (nmech > 0): the accumulated FP64 gradients with respect
+ * to the model's taup and taus (gradq[2][NY][NX][NZ]), summed like grad64 by
+ * ifosb_gradient and zeroed by ifosb_zero_gradient. The reference has no Q
+ * gradient; this one follows from its memory-variable update
+ * (src/update_s_ssg.c:108-122): in the frequency domain of discfourier a modulus
+ * M acts as M (1 + tau Phi(w)), Phi = sum_l s t_l / (1 + s t_l), s = -i w,
+ * t_l = DT / eta_l, so with gradient_F's lambda and mu correlations taken complex
+ * (C = F conj(B), real parts = gradlam, gradmu):
+ *   d/dtaup = pi sum_f Re[Phi C_lambda],  d/dtaus = u sum_f Re[Phi (C_mu - 2 C_lambda)],
+ * with gradient_F's sign (minus the misfit gradient). With tau proportional to
+ * 1/Q (the tau method), d/dQ = -(taup d/dtaup + taus d/dtaus) / Q. */
+int ifosb_get_gradient_q(ifosb_engine *e, double *gradq);
+
 /* Zero the accumulated gradients (zero_grad, src/zero_grad.c). */
 int ifosb_zero_gradient(ifosb_engine *e);
 
