@@ -259,6 +259,8 @@ def main():
     ap.add_argument("--cpu-procs", type=int, default=0)
     ap.add_argument("--cpu-nt", type=int, default=40)
     ap.add_argument("--cpu-warmup", action="store_true")
+    ap.add_argument("--grid", default=None, help="visco384 only: NX,NY,NZ (profiling runs)")
+    ap.add_argument("--nshots", type=int, default=None, help="visco384 only: shots per step (profiling runs)")
     ap.add_argument("--shape", default=None,
                     help="launch shape cy_vel,l2_vel,cy_str,l2_str instead of autotuning (profiling runs)")
     args = ap.parse_args()
@@ -470,7 +472,8 @@ def batched_gradient_workload(args, world, rank, local, dist):
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream(dev)
     nt = args.nt or 200
-    c = synth.case("visco384", nt=nt)
+    grid = tuple(int(x) for x in args.grid.split(",")) if args.grid else None
+    c = synth.case("visco384", nt=nt, nshots=args.nshots, grid=grid)
     p = c["params"]
     m, cp, shots = synth.build_inputs(c)
     nf, nshots = len(c["finv"]), len(shots)
@@ -498,10 +501,17 @@ def batched_gradient_workload(args, world, rank, local, dist):
     nbatch = -(-len(mine) // min(cap, len(mine)))
     B = -(-len(mine) // nbatch)
     eng = engine(B)
-    tuned = eng.autotune([shots[i] for i in mine[:B]], steps=min(40, p.nt))
     last = len(mine) - (nbatch - 1) * B
-    if last != B:  # a shorter last batch gets its own launch shape
-        eng.autotune([shots[i] for i in mine[-last:]], steps=min(40, p.nt))
+    if args.shape:
+        sh = [int(x) for x in args.shape.split(",")]
+        for nb in {B, last}:
+            eng.set_launch_shape(nb, sh)
+        tuned = {"velocity": {"y_planes_per_cta": sh[0], "l2_prefetch_planes": sh[1]},
+                 "stress": {"y_planes_per_cta": sh[2], "l2_prefetch_planes": sh[3]}}
+    else:
+        tuned = eng.autotune([shots[i] for i in mine[:B]], steps=min(40, p.nt))
+        if last != B:  # a shorter last batch gets its own launch shape
+            eng.autotune([shots[i] for i in mine[-last:]], steps=min(40, p.nt))
     # observed data: this rank's shots modelled in the same (true = start) model and
     # scaled, so that the residual is not zero; other ranks' entries are placeholders
     obs = np.zeros((nshots, 3, eng.ntr, eng.ns), np.float32)
@@ -534,6 +544,10 @@ def batched_gradient_workload(args, world, rank, local, dist):
         ms = float(t.item())
     ncell = p.nx * p.ny * p.nz
     cells = 2 * ncell * p.nt * nshots * args.steps
+    if grid or args.nshots:  # a reduced case: name what ran
+        out_grid, out_shots = [p.nx, p.ny, p.nz], nshots
+    else:
+        out_grid, out_shots = None, None
     value = cells / (ms / 1000.0) / 1e9
     launches = args.steps * nbatch * (4 * p.nt + 3)
 
@@ -564,7 +578,7 @@ def batched_gradient_workload(args, world, rank, local, dist):
         "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 2), "higher_is_better": True,
         "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": dict(workload_config("visco384", world, p.nt), shots_per_batch=B, batches_per_gpu=nbatch,
-                       launch_shape=dict(tuned, picked_by="ifosb_autotune")),
+                       launch_shape=dict(tuned, picked_by="--shape" if args.shape else "ifosb_autotune")),
         "clocks": clocks,
         "e2e": {"value": round(value, 3), "unit": UNIT, "note": "the step itself is end to end: host observed "
                 "traces in, the summed FP64 gradient out", "h2d_bytes_per_step": int(obs[mine].nbytes),
@@ -594,6 +608,9 @@ def batched_gradient_workload(args, world, rank, local, dist):
         out["cpu_baseline"] = {"value": round(v1, 5), "unit": UNIT, "cores": 1, "kind": kind,
                                "sample": f"one core, {grid[0]}x{grid[1]}x{grid[2]} grid x {cnt} steps of the "
                                          f"same forward step (L={p.nmech}, FW=10 CPML, free surface)"}
+    if out_grid:
+        out["config"].update(grid=out_grid, shots=out_shots, workload="visco384 reduced for profiling: "
+                             f"{out_grid[0]}x{out_grid[1]}x{out_grid[2]} cells, {out_shots} shots, NT={p.nt}")
     if rank == 0:
         print(json.dumps(out), flush=True)
 

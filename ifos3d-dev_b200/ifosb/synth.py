@@ -65,8 +65,9 @@ def _gauss_field(shape, corr, rng):
     return (f / f.std()).astype(np.float32)
 
 
-def case(name: str, seed: int = 1234, nt: int | None = None, nshots: int | None = None):
-    """A workload dict: params, true/start velocity models, moduli, shots, receivers, frequencies."""
+def case(name: str, seed: int = 1234, nt: int | None = None, nshots: int | None = None, grid=None):
+    """A workload dict: params, true/start velocity models, moduli, shots, receivers, frequencies.
+    grid (visco384 only): (NX, NY, NZ) instead of 384 x 256 x 384, for small profiling runs."""
     rng = np.random.default_rng(seed)
     if name == "elastic128":
         n, fw = 128, 10
@@ -124,7 +125,7 @@ def case(name: str, seed: int = 1234, nt: int | None = None, nshots: int | None 
         start = (bg_vp, vs0, rho0)
         tau, fl = 0.0, None
     elif name == "visco384":
-        nx, ny, nz, fw = 384, 256, 384, 10
+        nx, ny, nz, fw = tuple(grid) + (10,) if grid else (384, 256, 384, 10)
         nt = nt or 2000
         tau, fl = q_tau_fit(50.0, 20.0, 200.0, 3)
         p = make_params(nx, ny, nz, dh=1.0, dt=1e-4, nt=nt, fdcoeff=2, free_surf=1, fw=fw, nmech=3)
