@@ -1138,7 +1138,8 @@ extern "C" int ifosb_gradient(ifosb_engine *e) {
         a.iphi[l] = im;
     }
     dim3 blk(BX, BY), grd(e->g.ntk, e->g.nti, e->g.nyc);
-    k_gradient<<<grd, blk, 0, e->stream>>>(a);
+    if (a.gradq) k_gradient<true><<<grd, blk, 0, e->stream>>>(a);
+    else k_gradient<false><<<grd, blk, 0, e->stream>>>(a);
     int rc = check_launch(e, "gradient");
     if (rc) return rc;
     CU(cudaStreamSynchronize(e->stream));

@@ -571,7 +571,17 @@ __device__ __forceinline__ void dft_derivs(const float *X, const float *Y, const
     d[8] = (b1 * (Z[c] - Z[c - 1]) + b2 * (Z[c + 1] - Z[c - 2])) / DZ;
 }
 
-__global__ void __launch_bounds__(BX *BY) k_gradient(GradArgs a) {
+// Q: also the viscoelastic taup / taus gradient (a.gradq). Two instances, so the
+// elastic one keeps the registers of gradient_F's terms alone. The kernel is
+// latency-bound (156 loads per cell, shot and frequency): three blocks per SM at
+// 80 registers (with spills) ran 1.75x faster than one block at 243-254
+// registers (10.5 vs 18.4 ms for 4 shots x 4 frequencies at 128^3, L=3;
+// 1.2 vs 2.0 ms elastic 128^3, nf=2), with the same bits.
+#ifndef IFOSB_GRAD_MINB
+#define IFOSB_GRAD_MINB 3
+#endif
+template <bool Q>
+__global__ void __launch_bounds__(BX *BY, IFOSB_GRAD_MINB) k_gradient(GradArgs a) {
     const Geo &g = a.g;
     const int k = blockIdx.x * BX + threadIdx.x + 1;
     const int i = blockIdx.y * BY + threadIdx.y + 1;
@@ -587,7 +597,7 @@ __global__ void __launch_bounds__(BX *BY) k_gradient(GradArgs a) {
         float g1 = a.grad[m], g2 = a.grad[n + m], g3 = a.grad[2 * n + m];
         double h1 = a.grad64[m], h2 = a.grad64[n + m], h3 = a.grad64[2 * n + m];
         double qp = 0.0, qs = 0.0;
-        if (a.gradq) {
+        if (Q) {
             qp = a.gradq[m];
             qs = a.gradq[n + m];
         }
@@ -622,7 +632,7 @@ __global__ void __launch_bounds__(BX *BY) k_gradient(GradArgs a) {
                 h1 += c1;
                 h2 += c2;
                 h3 += (double)c3;
-                if (a.gradq) {
+                if (Q) {
                     // complex correlations C = F conj(B) of the lambda and mu terms with
                     // gradient_F's factor -fdummy: its gradlam / gradmu are their real
                     // parts. A modulus M(1 + tau Phi) perturbed in tau moves the misfit
@@ -653,7 +663,7 @@ __global__ void __launch_bounds__(BX *BY) k_gradient(GradArgs a) {
         }
         a.grad[m] = g1; a.grad[n + m] = g2; a.grad[2 * n + m] = g3;
         a.grad64[m] = h1; a.grad64[n + m] = h2; a.grad64[2 * n + m] = h3;
-        if (a.gradq) {
+        if (Q) {
             a.gradq[m] = qp;
             a.gradq[n + m] = qs;
         }
