@@ -760,7 +760,13 @@ struct HessArgs {
     float *hess;
 };
 
-__global__ void __launch_bounds__(BX *BY) k_hessian(HessArgs a) {
+// Two blocks per SM (128 registers, a few spills) ran 1.58x faster than one at
+// 236 registers (62 vs 98 ms: 2 shots x 25 receivers x 2 frequencies, 128^3),
+// with the same bits; three gained nothing more.
+#ifndef IFOSB_HESS_MINB
+#define IFOSB_HESS_MINB 2
+#endif
+__global__ void __launch_bounds__(BX *BY, IFOSB_HESS_MINB) k_hessian(HessArgs a) {
     const Geo &g = a.g;
     const int k = blockIdx.x * BX + threadIdx.x + 1;
     const int i = blockIdx.y * BY + threadIdx.y + 1;
