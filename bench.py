@@ -630,14 +630,14 @@ def shot_gradient_comparison(torch, ifosb, synth, dev, stream, nt_override, nsho
     return _compare_batched(torch, ifosb, synth, dev, stream, c, nshots, f"elastic128, {nshots} shots")
 
 
-def small_grid_comparison(torch, ifosb, synth, dev, stream, nt_override, nshots=16):
+def small_grid_comparison(torch, ifosb, synth, dev, stream, nt_override, nshots=32):
     """The same comparison where one shot cannot fill the GPU: 64^3 elastic cells
-    (10-cell CPML, free surface), 16 shots on a 4x4 surface grid, nf = 2."""
+    (10-cell CPML, free surface), 32 shots on an 8x4 surface grid, nf = 2."""
     c = synth.small_case(nx=64, ny=64, nz=64, nt=nt_override or 800, fw=10, free_surf=1, nmech=0, seed=11,
                          nshots=nshots, ntr=16, finv=(300.0, 500.0))
     for s, sp in enumerate(c["shots"]):
-        sp[0, 0] = 16 + 10 * (s % 4)
-        sp[0, 2] = 16 + 10 * (s // 4)
+        sp[0, 0] = 12 + 6 * (s % 8)
+        sp[0, 2] = 16 + 10 * (s // 8)
     return _compare_batched(torch, ifosb, synth, dev, stream, c, nshots, f"elastic 64^3, {nshots} shots")
 
 
