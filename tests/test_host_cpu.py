@@ -120,3 +120,19 @@ def test_q_fit_constant_q(ifosb_mod):
     b = ((w[:, None] * tl) ** 2 / (1 + (w[:, None] * tl) ** 2)).sum(1)
     q = (1 + tau * b) / (tau * a)
     assert np.all(np.abs(q / 50.0 - 1) < 0.25)
+
+
+def test_q_gradient_chain_rule(ifosb_mod):
+    """ifosb.q_gradient: with tau proportional to 1/Q (the tau method), the Q
+    gradient is the taup / taus gradients through d tau / dQ = -tau / Q; checked
+    by a centred difference of the linear functional <g, tau(Q)> per cell."""
+    rng = np.random.default_rng(3)
+    gq = rng.standard_normal((2, 4, 5, 6))
+    q0 = rng.uniform(20.0, 80.0, (4, 5, 6))
+    tau, _ = synth.q_tau_fit(50.0, 20.0, 200.0, 3)
+    tp = lambda q: tau * 50.0 / q * 1.1  # noqa: E731  taup and taus with their own constants
+    ts = lambda q: tau * 50.0 / q * 0.9  # noqa: E731
+    got = ifosb_mod.q_gradient(gq, tp(q0), ts(q0), q0)
+    h = 1e-4 * q0
+    fd = (gq[0] * (tp(q0 + h) - tp(q0 - h)) + gq[1] * (ts(q0 + h) - ts(q0 - h))) / (2 * h)
+    assert np.allclose(got, fd, rtol=1e-6, atol=0)
