@@ -1,7 +1,7 @@
 #!/usr/bin/env python
 """Benchmark of the B200 IFOS3D wavefield engine.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload visco256|elastic128|visco384]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload visco256|elastic128|visco384|multiscale]
                     [--impl ours|reference]
 
 A step is one pass of the hot path over one batch of synthetic input:
@@ -11,6 +11,10 @@ A step is one pass of the hot path over one batch of synthetic input:
              across ranks, no data-path collective: weak scaling).
   elastic128 one shot-gradient (forward + residual + adjoint + DFT gradient),
              128^3, NT=2000, 2 frequencies.
+  multiscale a two-grid elastic inversion (the reference driver's iterations:
+             shot gradients, precon_grad, CG, step-length test forwards, model
+             update) on 96x64x96 cells at 2 m, then on 192x128x192 at 1 m
+             from the resampled model, 16 shots, three frequency stages.
   visco384   the batched multi-shot gradient: 32 viscoelastic (L=3) shot-gradients
              (4 frequencies, 1024 receivers) on 384 x 256 x 384 cells, in
              HBM-sized batches of shots that share one launch; NT=200 by default
@@ -251,7 +255,7 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="visco256", choices=["visco256", "elastic128", "visco384"])
+    ap.add_argument("--workload", default="visco256", choices=["visco256", "elastic128", "visco384", "multiscale"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nt", type=int, default=None, help="override NT (testing only)")
     ap.add_argument("--no-cpu", action="store_true")
@@ -272,6 +276,13 @@ def main():
             dist.destroy_process_group()
         return
 
+    if args.workload == "multiscale":
+        if rank == 0:
+            multiscale_workload(args, local)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
     if args.workload == "visco384":
         batched_gradient_workload(args, world, rank, local, dist)
         if dist:
@@ -613,6 +624,104 @@ def batched_gradient_workload(args, world, rank, local, dist):
                              f"{out_grid[0]}x{out_grid[1]}x{out_grid[2]} cells, {out_shots} shots, NT={p.nt}")
     if rank == 0:
         print(json.dumps(out), flush=True)
+
+
+def multiscale_workload(args, local):
+    """The multiscale inversion loop reduced to one GPU and about a minute: the
+    reference driver's iterations (ifosb.inversion) on a 2 m grid for two
+    frequency stages, the model resampled to a 1 m grid, one more stage there.
+    The true model is four layers and two Gaussian blobs (+10 % vp); the start
+    model is it smoothed by a 15 m Gaussian. Elastic, as the reference's
+    inversion path is (its viscoelastic stress calls are commented out), CG
+    updating vp (WEIGHT 1 0 0), no free surface (precon_grad's damping types 0-2
+    zero the gradient with one). Timed by the host clock around the synchronous
+    calls: an inversion has no repeatable step to warm up."""
+    import torch
+    from scipy.ndimage import gaussian_filter
+    import ifosb
+    from ifosb import stages as fst
+    from ifosb import synth
+    from ifosb.inversion import Inversion, Settings, Stage
+    torch.cuda.set_device(local)
+    rng = np.random.default_rng(5)
+    fw, fc, nsh_side, h_fine = 10, 150.0, 4, 1.0
+    fine = (128, 192, 192)  # (NY, NX, NZ), y down
+    jj, ii, kk = np.meshgrid(*(np.arange(n) for n in fine), indexing="ij")
+    bounds = np.sort(rng.choice(np.arange(20, fine[0] - 20), 3, replace=False))
+    vps = np.array([2500.0, 3000.0, 3500.0, 4000.0], np.float32)
+    vp_t = vps[np.searchsorted(bounds, np.arange(fine[0]), side="right")][:, None, None] * np.ones(fine, np.float32)
+    for _ in range(2):
+        c = [rng.uniform(40, n - 40) for n in fine]
+        vp_t *= 1 + 0.1 * np.exp(-((jj - c[0]) ** 2 + (ii - c[1]) ** 2 + (kk - c[2]) ** 2) / (2 * 12.0 ** 2))
+    vp_t = vp_t.astype(np.float32)
+    true = (vp_t, (vp_t / np.float32(math.sqrt(3))).astype(np.float32), (1700 + 0.2 * vp_t).astype(np.float32))
+    start = tuple(gaussian_filter(a.astype(np.float64), 15.0, mode="nearest").astype(np.float32) for a in true)
+    grids = [dict(h=2.0, dt=2e-4, nt=500, stages=[Stage([27.0, 53.0, 80.0], 2), Stage([80.0, 120.0, 160.0], 2)]),
+             dict(h=1.0, dt=1e-4, nt=1000, stages=[Stage([160.0, 213.0, 267.0], 2)])]
+    inner = lambda a: a[fw:-fw, fw:-fw, fw:-fw]  # noqa: E731
+    err = lambda vp: float(np.linalg.norm(inner(vp) - inner(vp_t)) / np.linalg.norm(inner(vp_t)))  # noqa: E731
+    cur = start
+    hist, cells, t_total = [], 0, 0.0
+    vp_err = {"start": err(start[0])}
+    for gi, gd in enumerate(grids):
+        s = gd["h"] / h_fine
+        shape = tuple(int(n / s) for n in fine)
+        ny, nx, nz = shape
+        if s != 1:
+            mt = [fst.resample(a, (h_fine,) * 3, shape, (gd["h"],) * 3) for a in true]
+            m0 = [fst.resample(a, (h_fine,) * 3, shape, (gd["h"],) * 3) for a in cur]
+        else:
+            mt, m0 = list(true), list(cur)
+        p = ifosb.make_params(nx, ny, nz, dh=gd["h"], dt=gd["dt"], nt=gd["nt"], fdcoeff=2, free_surf=0, fw=fw,
+                              nmech=0)
+        xs = np.linspace(fw + 6, nx - fw - 6, nsh_side).round().astype(int)
+        zs = np.linspace(fw + 6, nz - fw - 6, nsh_side).round().astype(int)
+        shots = [(sp, ifosb.wavelet(p, 4, sp)) for sp in (synth._src(int(x), fw + 3, int(z), fc) for x in xs for z in zs)]
+        rec = synth._grid_receivers(nx, nz, 16, fw + 2, fw + 3)
+        cp = ifosb.cpml_coeff(p, 4000.0, fc)
+        e = ifosb.Engine(p, max_shots=len(shots), max_nf=0)
+        e.set_cpml(cp)
+        e.set_receivers(rec)
+        mod = ifosb.moduli(p, *(a.ravel() for a in mt))
+        e.set_model(*(mod[k].reshape(shape) for k in ("rho", "pi", "u")), None, None, None)
+        obs = e.forward(shots)
+        e.close()
+        mod0 = ifosb.moduli(p, *(a.ravel() for a in m0))
+        ghost = [ifosb.ghost_wrap(mod0[k].reshape(shape)) for k in ("rho", "pi", "u")]
+        srcpos_m = np.array([[sp[0, 0] * gd["h"], sp[0, 1] * gd["h"], sp[0, 2] * gd["h"]] for sp, _ in shots], np.float32)
+        cfg = Settings(teststep=0.02, damptype=2, lbfgs=False, nshots_step=4, max_batch=len(shots),
+                       weight=(1.0, 0.0, 0.0))
+        inv = Inversion(p, cp, rec, shots, obs, srcpos_m, *ghost, gd["stages"], cfg)
+        iters = sum(st.itmax for st in gd["stages"])
+        ncell = nx * ny * nz
+        for _ in range(iters):
+            t0 = time.perf_counter()
+            mis = inv.iterate()
+            t_total += time.perf_counter() - t0
+            cells += ncell * p.nt * (2 * len(shots) + 2 * cfg.nshots_step)
+            hist.append({"grid": gi, "misfit": mis, "t_s": round(t_total, 3), "step": inv.hist.step[-1]})
+        rho, pi, u = (a[1:-1, 1:-1, 1:-1].astype(np.float64) for a in inv.model)
+        got = ((np.sqrt(pi / rho)).astype(np.float32), (np.sqrt(u / rho)).astype(np.float32), rho.astype(np.float32))
+        inv.close()
+        cur = tuple(fst.resample(a, (gd["h"],) * 3, fine, (h_fine,) * 3) for a in got) if s != 1 else got
+        vp_err[f"after_grid{gi}"] = err(cur[0])
+    per_grid = {}
+    for gi in range(len(grids)):
+        m = [x["misfit"] for x in hist if x["grid"] == gi]
+        per_grid[f"grid{gi}"] = {"first": m[0], "last": m[-1], "reduction": round(1 - m[-1] / m[0], 4)}
+    out = {
+        "metric": METRIC, "value": round(cells / t_total / 1e9, 3), "unit": UNIT, "n_gpus": 1,
+        "steps": len(hist), "warmup": 0, "ms_per_step": round(1000 * t_total / len(hist), 1),
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "multiscale: elastic inversion, 96x64x96 @ 2 m (NT=500, 2 stages x 2 iterations) "
+                               "then 192x128x192 @ 1 m (NT=1000, 1 stage x 2 iterations), 16 shots, 256 receivers, "
+                               "CG on vp, 4 layers + 2 blobs, start smoothed by 15 m",
+                   "timing": "host clock around synchronous calls; value counts the shot gradients and the "
+                             "step-length test forwards"},
+        "inversion": {"iterations": hist, "misfit_per_grid": per_grid, "vp_rel_error": vp_err,
+                      "seconds": round(t_total, 2)},
+    }
+    print(json.dumps(out), flush=True)
 
 
 def shot_gradient_comparison(torch, ifosb, synth, dev, stream, nt_override, nshots=4):
