@@ -185,3 +185,18 @@ def test_time_domain_preconditions():
     k = e.gradient_td(4)
     assert np.abs(k[0]).max() > 0
     e.close()
+
+
+def test_time_domain_partial_batch():
+    """A batch smaller than the engine's max_shots (the recomputation's tensor
+    maps then cover fewer shots than the engine's own) gives the same kernels."""
+    c = synth.small_case(nx=20, ny=22, nz=18, nt=30, fw=4, nmech=0, nshots=2, seed=41, free_surf=1)
+    out = []
+    for cap in (2, 3):
+        e, m, cp, shots = engine_for(c, max_shots=cap, nf=1)
+        syn = e.forward(shots)
+        e.residual((0.5 * np.roll(syn, 2, axis=-1)).astype(np.float32))
+        out.append(e.gradient_td(4))
+        e.close()
+    assert np.abs(out[0][0]).max() > 0
+    assert np.array_equal(out[0], out[1])
