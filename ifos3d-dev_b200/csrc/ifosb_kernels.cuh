@@ -558,8 +558,10 @@ struct GradArgs {
     double rphi[MAXNF], iphi[MAXNF];
 };
 
+// d: a float[9] or a column of shared memory (SCol)
+template <class D>
 __device__ __forceinline__ void dft_derivs(const float *X, const float *Y, const float *Z, long long c, long long dI,
-                                           long long dJ, float b1, float b2, float DX, float DY, float DZ, float *d) {
+                                           long long dJ, float b1, float b2, float DX, float DY, float DZ, D d) {
     d[0] = (b1 * (X[c] - X[c - dI]) + b2 * (X[c + dI] - X[c - 2 * dI])) / DX;
     d[1] = (b1 * (X[c + dJ] - X[c]) + b2 * (X[c + 2 * dJ] - X[c - dJ])) / DY;
     d[2] = (b1 * (X[c + 1] - X[c]) + b2 * (X[c + 2] - X[c - 1])) / DZ;
@@ -571,20 +573,38 @@ __device__ __forceinline__ void dft_derivs(const float *X, const float *Y, const
     d[8] = (b1 * (Z[c] - Z[c - 1]) + b2 * (Z[c + 1] - Z[c - 2])) / DZ;
 }
 
+// The same pointer, hidden from the optimiser (an empty asm that "changes" it).
+__device__ __forceinline__ const float *opaque(const float *p) {
+    asm volatile("" : "+l"(p));
+    return p;
+}
+
+// Nine values of one thread in shared memory, stride one block: the kernel keeps
+// its 36 derivatives there instead of in registers.
+struct SCol {
+    float *p;
+    __device__ __forceinline__ float &operator[](int q) const { return p[q * (BX * BY)]; }
+};
+
 // Q: also the viscoelastic taup / taus gradient (a.gradq). Two instances, so the
 // elastic one keeps the registers of gradient_F's terms alone. The kernel is
-// latency-bound (156 loads per cell, shot and frequency): three blocks per SM at
-// 80 registers (with spills) ran 1.75x faster than one block at 243-254
-// registers (10.5 vs 18.4 ms for 4 shots x 4 frequencies at 128^3, L=3;
-// 1.2 vs 2.0 ms elastic 128^3, nf=2), with the same bits.
+// latency-bound on its 156 loads per cell, shot and frequency. Left to itself the
+// compiler hoisted all of them (and their 64-bit addresses) and used 243-254
+// registers: one block per SM, or spills that went to DRAM at lower caps. With
+// the derivatives in shared memory and each stencil set's pointers opaque, four
+// blocks per SM fit in 62-64 registers: 5.7 ms instead of 18.4 ms for 4 shots x
+// 4 frequencies at 128^3, L=3 (0.66 instead of 2.0 ms elastic, nf=2), same bits.
 #ifndef IFOSB_GRAD_MINB
-#define IFOSB_GRAD_MINB 3
+#define IFOSB_GRAD_MINB 4
 #endif
 template <bool Q>
 __global__ void __launch_bounds__(BX *BY, IFOSB_GRAD_MINB) k_gradient(GradArgs a) {
+    __shared__ float sdv[4 * 9 * BX * BY];
     const Geo &g = a.g;
     const int k = blockIdx.x * BX + threadIdx.x + 1;
     const int i = blockIdx.y * BY + threadIdx.y + 1;
+    const int tid = threadIdx.y * BX + threadIdx.x;
+    const SCol fv{sdv + tid}, bv{sdv + 9 * BX * BY + tid}, fi{sdv + 18 * BX * BY + tid}, bi{sdv + 27 * BX * BY + tid};
     const int yc = blockIdx.z;
     if (k > g.nz || i > g.nx) return;
     const int j0 = yc * g.cy + 1;
@@ -607,11 +627,19 @@ __global__ void __launch_bounds__(BX *BY, IFOSB_GRAD_MINB) k_gradient(GradArgs a
             for (int l = 0; l < a.nf; ++l) {
                 const float *Fb = a.dftf + (long long)s * a.dft_shot + (long long)l * 6 * F;
                 const float *Bb = a.dftb + (long long)s * a.dft_shot + (long long)l * 6 * F;
-                float fv[9], bv[9], fi[9], bi[9];
-                dft_derivs(Fb, Fb + F, Fb + 2 * F, c, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, fv);
-                dft_derivs(Bb, Bb + F, Bb + 2 * F, c, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, bv);
-                dft_derivs(Fb + 3 * F, Fb + 4 * F, Fb + 5 * F, c, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, fi);
-                dft_derivs(Bb + 3 * F, Bb + 4 * F, Bb + 5 * F, c, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, bi);
+                // One stencil set at a time: each set's field pointers pass through an
+                // empty asm, so the compiler can neither hoist the 36 addresses of all
+                // sets out of the loops nor issue the next set's loads early; the
+                // 144 loads then need few registers (no spills to local memory).
+                const float *Fc = Fb + c, *Bc = Bb + c;
+                const float *p0 = opaque(Fc), *p1 = opaque(Fc + F), *p2 = opaque(Fc + 2 * F);
+                dft_derivs(p0, p1, p2, 0, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, fv);
+                p0 = opaque(Bc); p1 = opaque(Bc + F); p2 = opaque(Bc + 2 * F);
+                dft_derivs(p0, p1, p2, 0, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, bv);
+                p0 = opaque(Fc + 3 * F); p1 = opaque(Fc + 4 * F); p2 = opaque(Fc + 5 * F);
+                dft_derivs(p0, p1, p2, 0, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, fi);
+                p0 = opaque(Bc + 3 * F); p1 = opaque(Bc + 4 * F); p2 = opaque(Bc + 5 * F);
+                dft_derivs(p0, p1, p2, 0, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, bi);
                 const float fdummy = a.fdummy[l];
                 float gradlam = (fv[0] + fv[4] + fv[8]) * (bv[0] + bv[4] + bv[8]) + (fi[0] + fi[4] + fi[8]) * (bi[0] + bi[4] + bi[8]);
                 gradlam = -gradlam * fdummy;
@@ -760,16 +788,20 @@ struct HessArgs {
     float *hess;
 };
 
-// Two blocks per SM (128 registers, a few spills) ran 1.58x faster than one at
-// 236 registers (62 vs 98 ms: 2 shots x 25 receivers x 2 frequencies, 128^3),
-// with the same bits; three gained nothing more.
+// With the derivatives in shared memory and opaque stencil pointers (as in
+// k_gradient), four blocks per SM fit in 62 registers without spills: 35.5 ms
+// for 2 shots x 25 receivers x 2 frequencies at 128^3, against 98 ms at one
+// block (236 registers) and 62 ms at two (128, with spills); same bits.
 #ifndef IFOSB_HESS_MINB
-#define IFOSB_HESS_MINB 2
+#define IFOSB_HESS_MINB 4
 #endif
 __global__ void __launch_bounds__(BX *BY, IFOSB_HESS_MINB) k_hessian(HessArgs a) {
+    __shared__ float sdv[4 * 9 * BX * BY];
     const Geo &g = a.g;
     const int k = blockIdx.x * BX + threadIdx.x + 1;
     const int i = blockIdx.y * BY + threadIdx.y + 1;
+    const int tid = threadIdx.y * BX + threadIdx.x;
+    const SCol fv{sdv + tid}, bv{sdv + 9 * BX * BY + tid}, fi{sdv + 18 * BX * BY + tid}, bi{sdv + 27 * BX * BY + tid};
     const int yc = blockIdx.z;
     if (k > g.nz || i > g.nx) return;
     const int j0 = yc * g.cy + 1;
@@ -786,11 +818,16 @@ __global__ void __launch_bounds__(BX *BY, IFOSB_HESS_MINB) k_hessian(HessArgs a)
                 for (int l = 0; l < a.nf; ++l) {
                     const float *Fb = a.dftf + (long long)s * a.dft_shot + (long long)l * 6 * F;
                     const float *Bb = a.green + (long long)q * a.dft_shot + (long long)l * 6 * F;
-                    float fv[9], bv[9], fi[9], bi[9];
-                    dft_derivs(Fb, Fb + F, Fb + 2 * F, c, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, fv);
-                    dft_derivs(Bb, Bb + F, Bb + 2 * F, c, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, bv);
-                    dft_derivs(Fb + 3 * F, Fb + 4 * F, Fb + 5 * F, c, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, fi);
-                    dft_derivs(Bb + 3 * F, Bb + 4 * F, Bb + 5 * F, c, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, bi);
+                    // one stencil set at a time, as in k_gradient
+                    const float *Fc = Fb + c, *Bc = Bb + c;
+                    const float *p0 = opaque(Fc), *p1 = opaque(Fc + F), *p2 = opaque(Fc + 2 * F);
+                    dft_derivs(p0, p1, p2, 0, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, fv);
+                    p0 = opaque(Bc); p1 = opaque(Bc + F); p2 = opaque(Bc + 2 * F);
+                    dft_derivs(p0, p1, p2, 0, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, bv);
+                    p0 = opaque(Fc + 3 * F); p1 = opaque(Fc + 4 * F); p2 = opaque(Fc + 5 * F);
+                    dft_derivs(p0, p1, p2, 0, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, fi);
+                    p0 = opaque(Bc + 3 * F); p1 = opaque(Bc + 4 * F); p2 = opaque(Bc + 5 * F);
+                    dft_derivs(p0, p1, p2, 0, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, bi);
                     const float fd = a.fdummy[l];
                     const float fdiv = fv[0] + fv[4] + fv[8], fidiv = fi[0] + fi[4] + fi[8];
                     const float bdiv = bv[0] + bv[4] + bv[8], bidiv = bi[0] + bi[4] + bi[8];
