@@ -1247,8 +1247,9 @@ extern "C" int ifosb_gradient_td(ifosb_engine *e, int interval, double *kernels)
         La.va.val_comp = (long long)e->ntr * e->ns;
         La.tma = e->use_tma && setup_tma(e, La, nullptr);
         const int nb = 2 * 148, tb = 256;
+        const dim3 grd_c((p.nz + BX - 1) / BX, (p.nx + BY - 1) / BY, p.ny);
         auto integrate = [&](float *u, const float *st) {
-            k_td_integrate<<<nb, tb, 0, e->stream>>>(u, st, e->st_shot, F, nshots, p.dt);
+            k_td_integrate<<<dim3(nb, nshots), tb, 0, e->stream>>>(u, st, e->st_shot, F, nshots, p.dt);
         };
         // 1. the forward again, saving a checkpoint after steps K, 2K, ... and the sums at NT
         CU(cudaMemsetAsync(st2, 0, ss * sizeof(float), e->stream));
@@ -1315,7 +1316,7 @@ extern "C" int ifosb_gradient_td(ifosb_engine *e, int interval, double *kernels)
                 td_step(e, La, ntb);
                 integrate(ub, e->d_state);
                 ta.seg = segb + (size_t)(m - a0) * seg_shot * nshots;
-                k_td_corr<<<nb, tb, 0, e->stream>>>(ta);
+                k_td_corr<<<grd_c, dim3(BX, BY), 0, e->stream>>>(ta);
             }
             if ((r = check_launch(e, "time-domain adjoint"))) return r;
         }

@@ -719,11 +719,15 @@ struct TdArgs {
     double *k;             // [4][NY][NX][NZ]: rho, lambda, mu, dc
 };
 
-__global__ void k_td_corr(TdArgs a) {
+// One thread per interior cell: blocks of BX (z) x BY (x) cells, one plane each
+// (grid ceil(NZ/BX) x ceil(NX/BY) x NY).
+__global__ void __launch_bounds__(BX *BY, 4) k_td_corr(TdArgs a) {
     const Geo &g = a.g;
+    const int k = blockIdx.x * BX + threadIdx.x + 1, i = blockIdx.y * BY + threadIdx.y + 1, j = blockIdx.z + 1;
+    if (k > g.nz || i > g.nx) return;
     const long long n = (long long)g.nx * g.ny * g.nz, F = g.field, dI = g.pz, dJ = g.plane;
-    for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n; m += (long long)gridDim.x * blockDim.x) {
-        const int k = (int)(m % g.nz) + 1, i = (int)((m / g.nz) % g.nx) + 1, j = (int)(m / ((long long)g.nz * g.nx)) + 1;
+    {
+        const long long m = ((long long)(j - 1) * g.nx + (i - 1)) * g.nz + (k - 1);
         const long long c = widx(g, j, i, k);
         double kr = 0.0, kl = 0.0, km = 0.0;
         for (int s = 0; s < a.nshots; ++s) {
@@ -731,8 +735,10 @@ __global__ void k_td_corr(TdArgs a) {
             const float *vf = a.seg + (long long)s * a.seg_shot, *uf = vf + 3 * F;
             kr += (double)vf[c] * vb[c] + (double)vf[F + c] * vb[F + c] + (double)vf[2 * F + c] * vb[2 * F + c];
             float fu[9], bu[9];
-            dft_derivs(uf, uf + F, uf + 2 * F, c, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, fu);
-            dft_derivs(ub, ub + F, ub + 2 * F, c, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, bu);
+            const float *p0 = opaque(uf + c), *p1 = opaque(uf + F + c), *p2 = opaque(uf + 2 * F + c);
+            dft_derivs(p0, p1, p2, 0, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, fu);
+            p0 = opaque(ub + c); p1 = opaque(ub + F + c); p2 = opaque(ub + 2 * F + c);
+            dft_derivs(p0, p1, p2, 0, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, bu);
             kl += ((double)fu[0] + fu[4] + fu[8]) * ((double)bu[0] + bu[4] + bu[8]);
             km += 2.0 * ((double)fu[0] * bu[0] + (double)fu[4] * bu[4] + (double)fu[8] * bu[8]) +
                   ((double)fu[1] + fu[3]) * ((double)bu[1] + bu[3]) + ((double)fu[2] + fu[6]) * ((double)bu[2] + bu[6]) +
@@ -760,12 +766,23 @@ __global__ void k_td_dc(TdArgs a, const float *uf_end) {
     }
 }
 
-// U += v * DT over every shot's three velocity fields (whole padded fields).
+// U += v * DT over the three velocity fields (whole padded fields) of shot
+// blockIdx.y, four floats at a time (a field is a multiple of 8 floats and every
+// base is 16-byte aligned), each component as the scalar u + v * dt.
 __global__ void k_td_integrate(float *u, const float *st, long long st_shot, long long F, int nshots, float dt) {
-    const long long per = 3 * F, total = per * nshots;
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total; q += (long long)gridDim.x * blockDim.x) {
-        const long long s = q / per, r = q % per;
-        u[q] += st[s * st_shot + r] * dt;
+    const int s = blockIdx.y;
+    if (s >= nshots) return;
+    const long long n4 = 3 * F / 4;
+    float4 *U = reinterpret_cast<float4 *>(u + (long long)s * 3 * F);
+    const float4 *S = reinterpret_cast<const float4 *>(st + (long long)s * st_shot);
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n4; q += (long long)gridDim.x * blockDim.x) {
+        float4 x = U[q];
+        const float4 v = S[q];
+        x.x += v.x * dt;
+        x.y += v.y * dt;
+        x.z += v.z * dt;
+        x.w += v.w * dt;
+        U[q] = x;
     }
 }
 
