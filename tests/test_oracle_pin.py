@@ -78,3 +78,44 @@ def test_nsamples_rounding(oracle):
     p = ifo_params(c)
     p.ndt, p.ndtshift = 3, 5
     assert oracle.nsamples(p) == math.ceil((2000 - 5) / 3)
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_restatement_matches_reference_random(seed, oracle, ref_oracle):
+    """Seeded random cases: grid, CPML width, free surface, FD coefficients,
+    mechanisms (the reference has L <= 1), sources and their kind, receivers,
+    frequencies and DFT interval; forward, residual, adjoint and gradient must
+    be bit-identical between the restatement and the reference."""
+    rng = np.random.default_rng(100 + seed)
+    fw = int(rng.integers(3, 7))
+    n = [int(rng.integers(2 * fw + 6, 2 * fw + 16)) for _ in range(3)]
+    nf = int(rng.integers(1, 4))
+    c = synth.small_case(nx=n[0], ny=n[1], nz=n[2], nt=int(rng.integers(20, 50)), fw=fw,
+                         free_surf=int(rng.integers(0, 2)), nmech=int(rng.integers(0, 2)),
+                         fdcoeff=int(rng.integers(1, 3)), seed=seed, nsrc=int(rng.integers(1, 3)),
+                         ntr=int(rng.integers(2, 10)), stype=int(rng.choice([1, 2, 3, 4])),
+                         finv=tuple(float(f) for f in rng.uniform(100.0, 900.0, nf)))
+    ntast = int(rng.integers(1, 4))
+    p = ifo_params(c)
+    vp, vs, rho = c["start"]
+    mr = ref_oracle.readmod(p, vp, vs, rho, tau=c["tau"], fl=c["fl"])
+    mo = oracle.readmod(p, vp, vs, rho, tau=c["tau"], fl=c["fl"])
+    cr, co = ref_oracle.cpml_coeff(p), oracle.cpml_coeff(p)
+    sp = c["shots"][0]
+    sr, so = ref_oracle.wavelet(p, sp), oracle.wavelet(p, sp)
+    fr = ref_oracle.forward(p, mr, cr, sp, sr, c["recpos"], c["finv"], ntast, True, True)
+    fo = oracle.forward(p, mo, co, sp, so, c["recpos"], c["finv"], ntast, True, True)
+    for k in ("sections", "dft", "state"):
+        assert np.array_equal(fr[k], fo[k]), k
+    assert np.abs(fr["state"]).max() > 0 and np.abs(fr["dft"]).max() > 0
+    obs = (fr["sections"] * np.float32(0.9)).astype(np.float32)
+    dr, l2r = ref_oracle.residual(p, obs, fr["sections"])
+    do, l2o = oracle.residual(p, obs, fo["sections"])
+    assert np.array_equal(dr, do) and l2r == l2o
+    br = ref_oracle.adjoint(p, mr, cr, c["recpos"], dr, c["finv"], ntast, True)
+    bo = oracle.adjoint(p, mo, co, c["recpos"], do, c["finv"], ntast, True)
+    for k in ("dft", "state"):
+        assert np.array_equal(br[k], bo[k]), k
+    gr = ref_oracle.gradient(p, mr, c["finv"], fr["dft"], br["dft"])
+    go = oracle.gradient(p, mo, c["finv"], fo["dft"], bo["dft"])
+    assert np.array_equal(gr, go)
