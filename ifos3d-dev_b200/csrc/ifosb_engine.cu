@@ -108,9 +108,11 @@ struct ifosb_engine {
     Pt *d_vpts_t = nullptr, *d_spts_t = nullptr, *d_vpts_a = nullptr;
     size_t cap_vpts_t = 0, cap_spts_t = 0, cap_vpts_a = 0;
     float *d_amp_t = nullptr; size_t cap_amp_t = 0;
-    // TMA staging (default) and its wait-timeout flag
+    // TMA staging (default) and its wait-timeout flag; the failure-path test knobs
     int use_tma = 1;
     int *d_tma_err = nullptr;
+    unsigned long long wait_ns = WAIT_LIMIT_NS;
+    int stop_it = -1, stop_kernel = 0;  // stop_kernel: 1 velocity, 2 stress
     float *d_cpg = nullptr;  // CPML rows in global memory (lane-divergent reads)
     // uniform relaxation times: passed as scalars instead of five model fields
     bool unif_tau = false;
@@ -380,6 +382,15 @@ extern "C" const char *ifosb_last_error(const ifosb_engine *e) { return e ? e->e
 extern "C" long long ifosb_device_bytes(const ifosb_engine *e) { return e ? e->dev_bytes : 0; }
 extern "C" long long ifosb_last_launch_count(const ifosb_engine *e) { return e ? e->launches : 0; }
 extern "C" long long ifosb_graph_captures(const ifosb_engine *e) { return e ? e->captures : 0; }
+
+extern "C" int ifosb_set_wait_test(ifosb_engine *e, long long wait_ns, int kernel, int stop_plane) {
+    if (!e || wait_ns < 1000 || wait_ns > (long long)WAIT_LIMIT_NS || kernel < 0 || kernel > 2 || stop_plane < -1)
+        return IFOSB_EARG;
+    e->wait_ns = (unsigned long long)wait_ns;
+    e->stop_kernel = kernel;
+    e->stop_it = kernel ? stop_plane : -1;
+    return IFOSB_OK;
+}
 
 extern "C" int ifosb_set_launch_mode(ifosb_engine *e, int mode) {
     if (!e || (mode != 0 && mode != 1)) return IFOSB_EARG;
@@ -751,6 +762,8 @@ static bool setup_tma(ifosb_engine *e, Loop &L, float *dft) {
     L.vt.a = L.va;
     L.stt.a = L.sa;
     L.vt.tma_err = L.stt.tma_err = e->d_tma_err;
+    L.vt.w = WaitCtl{e->wait_ns, e->stop_kernel == 1 ? e->stop_it : -1};
+    L.stt.w = WaitCtl{e->wait_ns, e->stop_kernel == 2 ? e->stop_it : -1};
     {
         const ifosb_engine::Shape *t = shape_for(e, L.nshots);
         L.vt.l2ahead = t ? t->l2v : L2AHEAD_VEL_DEFAULT;
@@ -927,7 +940,9 @@ static int check_unstable(ifosb_engine *e, int nshots) {
     CU(cudaMemcpyAsync(errs.data(), e->d_err, sizeof(int) * nshots, cudaMemcpyDeviceToHost, e->stream));
     CU(cudaMemcpyAsync(&terr, e->d_tma_err, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
     CU(cudaStreamSynchronize(e->stream));
-    if (terr) return fail(e, IFOSB_ECUDA, "a TMA stage did not arrive within 1 s (mbarrier wait timed out)");
+    if (terr)
+        return fail(e, IFOSB_ECUDA, "a TMA stage did not arrive within " + std::to_string(e->wait_ns / 1000000ull) +
+                                        " ms (mbarrier wait timed out)");
     for (int s = 0; s < nshots; ++s)
         if (errs[s] != INT_MAX)
             return fail(e, IFOSB_EUNSTABLE,
@@ -1014,12 +1029,12 @@ extern "C" int ifosb_forward(ifosb_engine *e, int nshots, const ifosb_shot *shot
     sa.dft = e->d_dftf;
     sa.trig = e->d_trig_f;
     L.tma = e->use_tma && setup_tma(e, L, e->d_dftf);
+    e->fwd_ok = e->res_ok = e->adj_ok = e->hess_fwd = false;
     if ((rc = run_loop(e, L))) return rc;
     e->nshots = nshots;
+    if ((rc = check_unstable(e, nshots))) return rc;  // a failed batch is not a forward to build on
     e->fwd_ok = true;
     e->hess_fwd = e->nf > 0;
-    e->res_ok = e->adj_ok = false;
-    if ((rc = check_unstable(e, nshots))) return rc;
     if (sections && e->ntr > 0) {
         // [shot][component][ntr][ns] in saveseis's order: vx vy vz (1), p (2), div curl (3), all six (4)
         const size_t tr = (size_t)e->ntr * e->ns;
@@ -1537,13 +1552,43 @@ static __device__ __align__(256) double g_noalloc_part[IFOSB_NOALLOC_MAX_TRACES]
 namespace {
 constexpr int NOALLOC_MAX_DEVICES = 64;
 std::mutex g_noalloc_mu;
-double *g_noalloc_addr[NOALLOC_MAX_DEVICES];  // address of g_noalloc_part on each device
+// Address of g_noalloc_part on each device, with the context it was looked up
+// in: a module loaded into a new context (after cudaDeviceReset, say) may place
+// the array elsewhere, so a changed context means a fresh lookup.
+struct NoallocSlot {
+    CUcontext ctx;
+    double *addr;
+};
+NoallocSlot g_noalloc_slot[NOALLOC_MAX_DEVICES];
+
+PFN_cuCtxGetCurrent_v4000 ctx_getter() {
+    static PFN_cuCtxGetCurrent_v4000 fn = nullptr;
+    if (!fn) {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuCtxGetCurrent_v4000)f;
+    }
+    return fn;
+}
+
+bool overlaps(const void *a, const void *b, size_t bytes) {
+    const char *x = static_cast<const char *>(a), *y = static_cast<const char *>(b);
+    return x < y + bytes && y < x + bytes;
+}
 }  // namespace
 
 extern "C" int ifosb_residual_noalloc(int nshots, int ntr, int ns, float dt, const float *d_syn, const float *d_obs,
                                       float *d_diff, double *d_misfit, void *stream) {
     if (nshots < 1 || ntr < 1 || ns < 1 || !d_syn || !d_obs || !d_diff || !d_misfit) return IFOSB_EARG;
     if ((long long)nshots * 3 * ntr > IFOSB_NOALLOC_MAX_TRACES) return IFOSB_ETOOBIG;
+    // k_residual writes diff[ns-1-t] while it reads syn[t] and obs[t] forward:
+    // an output that overlaps an input would be read after it was overwritten
+    const size_t bytes = (size_t)nshots * 3 * ntr * ns * sizeof(float);
+    if (overlaps(d_diff, d_syn, bytes) || overlaps(d_diff, d_obs, bytes)) return IFOSB_EARG;
+    // an error the caller left pending on this thread stays theirs: report it, do not clear it
+    if (cudaPeekAtLastError() != cudaSuccess) return IFOSB_ECUDA;
     int dev = -1;
     if (cudaGetDevice(&dev) != cudaSuccess) {
         cudaGetLastError();
@@ -1553,19 +1598,26 @@ extern "C" int ifosb_residual_noalloc(int nshots, int ntr, int ns, float dt, con
     double *part;
     {
         std::lock_guard<std::mutex> lock(g_noalloc_mu);
-        if (!g_noalloc_addr[dev]) {
+        CUcontext ctx = nullptr;
+        auto get_ctx = ctx_getter();
+        if (!get_ctx || get_ctx(&ctx) != CUDA_SUCCESS) return IFOSB_ECUDA;
+        NoallocSlot &slot = g_noalloc_slot[dev];
+        if (!slot.addr || slot.ctx != ctx) {
             void *addr = nullptr;
             if (cudaGetSymbolAddress(&addr, g_noalloc_part) != cudaSuccess || !addr) {
                 cudaGetLastError();
+                slot.addr = nullptr;
                 return IFOSB_ECUDA;
             }
-            g_noalloc_addr[dev] = static_cast<double *>(addr);
+            slot.addr = static_cast<double *>(addr);
+            slot.ctx = ctx;
         }
-        part = g_noalloc_addr[dev];
+        part = slot.addr;
     }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const int nthr = nshots * 3 * ntr;
     k_residual<<<(nthr + 127) / 128, 128, 0, s>>>(d_syn, d_obs, d_diff, part, nshots, ntr, ns, dt);
+    if (cudaGetLastError() != cudaSuccess) return IFOSB_ECUDA;
     k_misfit<<<nshots, 32, 0, s>>>(part, d_misfit, 3 * ntr);
     return cudaGetLastError() == cudaSuccess ? IFOSB_OK : IFOSB_ECUDA;
 }

@@ -100,14 +100,16 @@ __device__ __forceinline__ uint64_t gtimer() {
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
 }
-// Bounded wait: gives up after 1 s of wall time (a TMA box lands in microseconds).
-__device__ __forceinline__ bool mbar_wait(uint64_t *b, uint32_t parity) {
+// Bounded wait: gives up after `limit_ns` of wall time (1 s unless a test lowers
+// it; a TMA box lands in microseconds).
+__device__ __forceinline__ bool mbar_wait(uint64_t *b, uint32_t parity, uint64_t limit_ns) {
     if (mbar_try(b, parity)) return true;
     const uint64_t t0 = gtimer();
     while (!mbar_try(b, parity))
-        if (gtimer() - t0 > 1000000000ull) return false;
+        if (gtimer() - t0 > limit_ns) return false;
     return true;
 }
+constexpr uint64_t WAIT_LIMIT_NS = 1000000000ull;
 __device__ __forceinline__ void tma_load5(void *dst, const CUtensorMap *m, int c0, int c1, int c2, int c3, int c4,
                                           uint64_t *bar) {
     asm volatile(
@@ -148,6 +150,15 @@ __device__ __forceinline__ int zc(int k) { return k + 7; }
 __device__ __forceinline__ int xc(int i) { return i + 1; }
 __device__ __forceinline__ int yc_(int j) { return j + 2; }
 
+// Failure-path test knobs of the TMA kernels: the mbarrier wait limit, and the
+// chunk iteration at which the producer warp stops issuing loads (-1 = never).
+// A producer that stops waits for the boxes it has issued and returns; the
+// consumers' waits for the boxes never issued then run out.
+struct WaitCtl {
+    uint64_t limit_ns;
+    int stop_it;
+};
+
 struct VelTma {
     CUtensorMap m_halo;  // state, box {RZ, RX, 1, 3, 1}
     CUtensorMap m_pt;    // state, box {TZ, TX, 1, 3, 1}
@@ -155,6 +166,7 @@ struct VelTma {
     VelArgs a;
     int *tma_err;
     int l2ahead;
+    WaitCtl w;
 };
 
 struct StrTma {
@@ -168,6 +180,7 @@ struct StrTma {
     float idx, idy, idz;          // exact 1/DX, 1/DY, 1/DZ (power-of-two spacings)
     int *tma_err;
     int l2ahead;
+    WaitCtl w;
 };
 
 // PML memory values of one cell (x, y, z slabs: three each), read one plane ahead

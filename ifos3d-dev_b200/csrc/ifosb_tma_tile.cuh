@@ -50,16 +50,29 @@ __device__ __forceinline__ bool pipeline_start(uint64_t *bar, const int *err) {
 }
 
 // Consumer side of one plane: wait for the stencil planes and the stage.
-__device__ __forceinline__ bool consumer_wait(uint64_t *bar, int it, int j, int j0, int rfirst) {
+__device__ __forceinline__ bool consumer_wait(uint64_t *bar, int it, int j, int j0, int rfirst, uint64_t lim) {
     bool ok = true;
     if (it == 0) {
-        for (int P = j0 - 2; P <= j0 + 2; ++P) ok &= mbar_wait(&bar[(P - rfirst) % RING], ((P - rfirst) / RING) & 1);
+        for (int P = j0 - 2; P <= j0 + 2; ++P) ok = ok && mbar_wait(&bar[(P - rfirst) % RING], ((P - rfirst) / RING) & 1, lim);
     } else {
         const int r = j + 2 - rfirst;
-        ok &= mbar_wait(&bar[r % RING], (r / RING) & 1);
+        ok = ok && mbar_wait(&bar[r % RING], (r / RING) & 1, lim);
     }
-    ok &= mbar_wait(&bar[2 * RING + it % NSTAGE], (it / NSTAGE) & 1);
+    ok = ok && mbar_wait(&bar[2 * RING + it % NSTAGE], (it / NSTAGE) & 1, lim);
     return ok;
+}
+
+// Producer exit on a failure path (a timed-out wait, or the test stop): wait,
+// bounded, for the boxes already issued, so that no copy is still landing in
+// shared memory when the CTA's warps have all returned. ring_hi / stage_hi are
+// the last ring plane and stage iteration issued; a slot's latest phase is the
+// only one not yet known to be complete.
+template <int NR, int NS>
+__device__ __forceinline__ void producer_drain(uint64_t *bar, int rfirst, int ring_hi, int stage_hi, uint64_t lim) {
+    for (int P = max(rfirst, ring_hi - NR + 1); P <= ring_hi; ++P)
+        if (!mbar_wait(&bar[(P - rfirst) % NR], ((P - rfirst) / NR) & 1, lim)) break;
+    for (int q = max(0, stage_hi - NS + 1); q <= stage_hi; ++q)
+        if (!mbar_wait(&bar[2 * NR + q % NS], (q / NS) & 1, lim)) break;
 }
 
 // Consumer hands back the ring plane j-2 and/or the stage of iteration `it`.
@@ -106,12 +119,12 @@ __device__ __forceinline__ void vel_rows(const VelTma &T, int nt, const float *r
     for (int it = 0, j = j0; j <= j1; ++it, ++j, V += g.plane) {
         bool ok = true;
         if (it == 0) {
-            for (int r = 0; r < 5; ++r) ok &= mbar_wait(&bar[r], 0);
+            for (int r = 0; r < 5; ++r) ok = ok && mbar_wait(&bar[r], 0, T.w.limit_ns);
         } else {
-            ok &= mbar_wait(&bar[wslot], wpar);
+            ok = ok && mbar_wait(&bar[wslot], wpar, T.w.limit_ns);
             if (++wslot == VRING) { wslot = 0; wpar ^= 1; }
         }
-        ok &= mbar_wait(&bar[2 * VRING + it % VNSTAGE], (it / VNSTAGE) & 1);
+        ok = ok && mbar_wait(&bar[2 * VRING + it % VNSTAGE], (it / VNSTAGE) & 1, T.w.limit_ns);
         if (!ok) { if (tz == 0) atomicExch(T.tma_err, 1); return; }
         // everything this row needs from the stage, so the stage can go back at once
         float sxx_x = 0.f, sxz_z = 0.f, szz_z = 0.f, sxz_x = 0.f;
@@ -232,24 +245,35 @@ __global__ void __launch_bounds__(NTHR, 3) k_velocity_tma(const __grid_constant_
             tma_prefetch4(&T.m_mod, zc(k0), xc(i0), yc_(j), MD_RIP);
         };
         auto ring_prefetch = [&](int P) { tma_prefetch5(&T.m_halo, zc(k0) - HZ, xc(i0) - HX, yc_(P), SYY, s); };
-        for (int P = rfirst; P <= min(rfirst + VRING - 1, rlast); ++P) ring_load(P);
-        for (int it = 0; it < VNSTAGE && it < n; ++it) stage_load(it);
+        const uint64_t lim = T.w.limit_ns;
+        int ring_hi = min(rfirst + VRING - 1, rlast), stage_hi = min(VNSTAGE, n) - 1;
+        for (int P = rfirst; P <= ring_hi; ++P) ring_load(P);
+        for (int it = 0; it <= stage_hi; ++it) stage_load(it);
         for (int q = 0; q < T.l2ahead; ++q) {
             if (VNSTAGE + q < n) stage_prefetch(VNSTAGE + q);
             if (rfirst + VRING + q <= rlast) ring_prefetch(rfirst + VRING + q);
         }
         for (int it = 0; it < n; ++it) {
+            if (it == T.w.stop_it) {  // failure-path test: issue nothing more
+                producer_drain<VRING, VNSTAGE>(bar, rfirst, ring_hi, stage_hi, lim);
+                return;
+            }
             if (rfirst + it + VRING <= rlast) {
-                if (!mbar_wait(&bar[VRING + it % VRING], (it / VRING) & 1)) { atomicExch(T.tma_err, 1); return; }
-                ring_load(rfirst + it + VRING);
+                if (!mbar_wait(&bar[VRING + it % VRING], (it / VRING) & 1, lim)) {
+                    atomicExch(T.tma_err, 1);
+                    producer_drain<VRING, VNSTAGE>(bar, rfirst, ring_hi, stage_hi, lim);
+                    return;
+                }
+                ring_load(ring_hi = rfirst + it + VRING);
                 if (T.l2ahead > 0 && rfirst + it + VRING + T.l2ahead <= rlast) ring_prefetch(rfirst + it + VRING + T.l2ahead);
             }
             if (it + VNSTAGE < n) {
-                if (!mbar_wait(&bar[2 * VRING + VNSTAGE + it % VNSTAGE], (it / VNSTAGE) & 1)) {
+                if (!mbar_wait(&bar[2 * VRING + VNSTAGE + it % VNSTAGE], (it / VNSTAGE) & 1, lim)) {
                     atomicExch(T.tma_err, 1);
+                    producer_drain<VRING, VNSTAGE>(bar, rfirst, ring_hi, stage_hi, lim);
                     return;
                 }
-                stage_load(it + VNSTAGE);
+                stage_load(stage_hi = it + VNSTAGE);
                 if (T.l2ahead > 0 && it + VNSTAGE + T.l2ahead < n) stage_prefetch(it + VNSTAGE + T.l2ahead);
             }
         }
@@ -315,24 +339,35 @@ __global__ void __maxnreg__(L == 0 ? STR_REGS_ELASTIC : STR_REGS_MECH) k_stress_
             if (ndf) tma_prefetch5(&T.m_dft, zc(k0), xc(i0), yc_(j), 0, s);
         };
         auto ring_prefetch = [&](int P) { tma_prefetch5(&T.m_halo, zc(k0) - HZ, xc(i0) - HX, yc_(P), VX, s); };
-        for (int P = rfirst; P <= min(rfirst + RING - 1, rlast); ++P) ring_load(P);
-        for (int it = 0; it < NSTAGE && it < n; ++it) stage_load(it);
+        const uint64_t lim = T.w.limit_ns;
+        int ring_hi = min(rfirst + RING - 1, rlast), stage_hi = min(NSTAGE, n) - 1;
+        for (int P = rfirst; P <= ring_hi; ++P) ring_load(P);
+        for (int it = 0; it <= stage_hi; ++it) stage_load(it);
         for (int q = 0; q < T.l2ahead; ++q) {
             if (NSTAGE + q < n) stage_prefetch(NSTAGE + q);
             if (rfirst + RING + q <= rlast) ring_prefetch(rfirst + RING + q);
         }
         for (int it = 0; it < n; ++it) {
+            if (it == T.w.stop_it) {  // failure-path test: issue nothing more
+                producer_drain<RING, NSTAGE>(bar, rfirst, ring_hi, stage_hi, lim);
+                return;
+            }
             if (rfirst + it + RING <= rlast) {
-                if (!mbar_wait(&bar[RING + it % RING], (it / RING) & 1)) { atomicExch(T.tma_err, 1); return; }
-                ring_load(rfirst + it + RING);
+                if (!mbar_wait(&bar[RING + it % RING], (it / RING) & 1, lim)) {
+                    atomicExch(T.tma_err, 1);
+                    producer_drain<RING, NSTAGE>(bar, rfirst, ring_hi, stage_hi, lim);
+                    return;
+                }
+                ring_load(ring_hi = rfirst + it + RING);
                 if (T.l2ahead > 0 && rfirst + it + RING + T.l2ahead <= rlast) ring_prefetch(rfirst + it + RING + T.l2ahead);
             }
             if (it + NSTAGE < n) {
-                if (!mbar_wait(&bar[2 * RING + NSTAGE + it % NSTAGE], (it / NSTAGE) & 1)) {
+                if (!mbar_wait(&bar[2 * RING + NSTAGE + it % NSTAGE], (it / NSTAGE) & 1, lim)) {
                     atomicExch(T.tma_err, 1);
+                    producer_drain<RING, NSTAGE>(bar, rfirst, ring_hi, stage_hi, lim);
                     return;
                 }
-                stage_load(it + NSTAGE);
+                stage_load(stage_hi = it + NSTAGE);
                 if (T.l2ahead > 0 && it + NSTAGE + T.l2ahead < n) stage_prefetch(it + NSTAGE + T.l2ahead);
             }
         }
@@ -356,7 +391,7 @@ __global__ void __maxnreg__(L == 0 ? STR_REGS_ELASTIC : STR_REGS_MECH) k_stress_
     PsiPre q{};
     if (active && (hx || hz || face_y(g, j0))) psi_load(q, ps, a.sl, g, j0, i, k, hx, hz);
     for (int it = 0, j = j0; j <= j1; ++it, ++j) {
-        if (!consumer_wait(bar, it, j, j0, rfirst)) { if (tz == 0) atomicExch(T.tma_err, 1); return; }
+        if (!consumer_wait(bar, it, j, j0, rfirst, T.w.limit_ns)) { if (tz == 0) atomicExch(T.tma_err, 1); return; }
         if (active) {
             const float *stage = stg + (it % NSTAGE) * SP;
             const int sm2 = sl >= 2 ? sl - 2 : sl + RING - 2, sm1 = sl >= 1 ? sl - 1 : sl + RING - 1;

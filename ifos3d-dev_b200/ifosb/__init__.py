@@ -132,6 +132,7 @@ def lib():
             "ifosb_resample": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float, vp,
                                          C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float]),
             "ifosb_set_seismo": (C.c_int, [vp, C.c_int]),
+            "ifosb_set_wait_test": (C.c_int, [vp, C.c_longlong, C.c_int, C.c_int]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -155,7 +156,7 @@ def exported_symbols():
         "ifosb_write_seis", "ifosb_merge_seis", "ifosb_read_seis", "ifosb_read_seis_split",
         "ifosb_write_model", "ifosb_write_gradient", "ifosb_filt_seis", "ifosb_hessian_green", "ifosb_hessian",
         "ifosb_zero_hessian", "ifosb_get_hessian", "ifosb_read_hessian", "ifosb_hess_apply", "ifosb_resample",
-        "ifosb_set_seismo", "ifosb_gradient_td", "ifosb_get_gradient_q",
+        "ifosb_set_seismo", "ifosb_gradient_td", "ifosb_get_gradient_q", "ifosb_set_wait_test",
     ]
 
 
@@ -284,6 +285,12 @@ class Engine:
         nf = 0 if f is None else len(f)
         self._c(lib().ifosb_set_frequencies(self.h, nf, _p(f), ntast))
         self.nf = nf
+
+    def set_wait_test(self, wait_ns: int = 1_000_000_000, kernel: int = 0, stop_plane: int = -1):
+        """Failure-path test knobs (ifosb_set_wait_test): the TMA kernels' mbarrier
+        wait limit, and the kernel (1 velocity, 2 stress) whose producer warp stops
+        issuing loads at chunk iteration stop_plane. Defaults restore normal runs."""
+        self._c(lib().ifosb_set_wait_test(self.h, int(wait_ns), kernel, stop_plane))
 
     def set_launch_mode(self, mode: int):
         self._c(lib().ifosb_set_launch_mode(self.h, mode))

@@ -181,6 +181,17 @@ int ifosb_get_field(ifosb_engine *e, int shot, int field, float *out);
  * and replayed (default); 1 = plain stream launches, one per kernel. */
 int ifosb_set_launch_mode(ifosb_engine *e, int mode);
 
+/* Failure-path test of the bounded waits (no counterpart in the reference, whose
+ * failures end in err(), src/util.c:30-40). Every mbarrier wait of the TMA time-step
+ * kernels gives up after wait_ns (default and maximum 1e9 = 1 s, minimum 1000);
+ * the call then returns IFOSB_ECUDA and the engine stays usable. With kernel = 1
+ * (velocity) or 2 (stress) and stop_plane >= 0, that kernel's producer warp stops
+ * issuing loads at iteration stop_plane of each CTA's y chunk, waits for the boxes
+ * it has issued and returns, so the consumers' waits for the rest run out: the
+ * path from an expired wait to the error status, made to run without a GPU fault.
+ * kernel = 0 (and stop_plane = -1) restores normal launches. For tests only. */
+int ifosb_set_wait_test(ifosb_engine *e, long long wait_ns, int kernel, int stop_plane);
+
 /* Kernels launched by the last forward/adjoint call (per-step kernels x steps). */
 long long ifosb_last_launch_count(const ifosb_engine *e);
 
@@ -346,17 +357,23 @@ int ifosb_hess_apply(ifosb_optim *o, float *grad, const float *hess, const float
  * synchronise the device; a host whose device memory all comes from its own pool.
  *
  * d_syn, d_obs, d_diff: device [nshots][3][ntr][ns] float (synthetic, observed,
- * residual out); d_misfit: device [nshots] double. The work is enqueued on
+ * residual out); d_misfit: device [nshots] double. d_diff must not overlap d_syn
+ * or d_obs (the residual is written time-reversed while the inputs are read
+ * forward): an overlapping call returns IFOSB_EARG. The work is enqueued on
  * `stream` (a cudaStream_t as void*, NULL = the legacy default stream) and the
- * call returns without waiting for it — unlike the other entry points.
+ * call returns without waiting for it — unlike the other entry points. A CUDA
+ * error already pending on the calling thread is left in place and the call
+ * returns IFOSB_ECUDA without launching.
  *
  * The per-trace partial sums live in a fixed device array of
  * IFOSB_NOALLOC_MAX_TRACES doubles (512 KiB) per device; nothing in it has to be
  * zero at the start of a call. Limit: nshots*3*ntr <= IFOSB_NOALLOC_MAX_TRACES,
  * else IFOSB_ETOOBIG and nothing is launched. The first call on each device
- * looks up that array's address (cudaGetSymbolAddress); make it before any
- * stream capture. Calls on one stream run in order; calls that overlap in time
- * on the same device (two streams, two host threads) share the array and race. */
+ * looks up that array's address (cudaGetSymbolAddress), and so does the first
+ * call after the device's context changed (e.g. after cudaDeviceReset); make
+ * those calls before any stream capture. Calls on one stream run in order; calls
+ * that overlap in time on the same device (two streams, two host threads) share
+ * the array and race. */
 #define IFOSB_ETOOBIG 7
 #define IFOSB_NOALLOC_MAX_TRACES 65536
 int ifosb_residual_noalloc(int nshots, int ntr, int ns, float dt, const float *d_syn, const float *d_obs,

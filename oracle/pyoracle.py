@@ -17,7 +17,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_LIB = os.path.join(HERE, "_ref", "libifos_ref.so")
 ORC_LIB = os.path.join(HERE, "lib", "libifos_oracle.so")
-REFERENCE_SRC = os.environ.get("IFOS_REFERENCE_SRC", "/root/reference")
+# the reference checkout: IFOS_REFERENCE_SRC, else a sibling of this repository
+REFERENCE_SRC = os.environ.get("IFOS_REFERENCE_SRC",
+                               os.path.normpath(os.path.join(HERE, "..", "..", "reference")))
 
 
 class IfoParams(C.Structure):

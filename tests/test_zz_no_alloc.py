@@ -21,6 +21,10 @@ def test_argument_and_size_checks_launch_nothing(ifosb_mod):
     assert ifosb.residual_noalloc(0, 4, 8, 1e-4, FAKE, FAKE, FAKE, FAKE) == ifosb.EARG
     assert ifosb.residual_noalloc(1, 4, 0, 1e-4, FAKE, FAKE, FAKE, FAKE) == ifosb.EARG
     assert ifosb.residual_noalloc(1, 4, 8, 1e-4, FAKE, 0, FAKE, FAKE) == ifosb.EARG
+    # the residual may not overlap the traces it is formed from (written reversed while they are read)
+    n = 3 * 4 * 8 * 4  # bytes of one shot's traces
+    assert ifosb.residual_noalloc(1, 4, 8, 1e-4, FAKE, FAKE + 2 * n, FAKE, FAKE) == ifosb.EARG
+    assert ifosb.residual_noalloc(1, 4, 8, 1e-4, FAKE, FAKE + 2 * n, FAKE + 2 * n + n - 4, FAKE) == ifosb.EARG
 
 
 def _np_residual(syn, obs, dt):
