@@ -134,32 +134,57 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # CPU side: the oracle (reported baseline and the reference arm)
 
+def cpu_model() -> str:
+    """The host CPU's model name (first /proc/cpuinfo entry)."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def _cpu_sample_worker(args):
-    """One process: the CPU implementation on a bounded sample grid."""
-    kind, nx, ny, nz, nmech, nt = args
+    """One process: the CPU implementation on a bounded sample grid. With nf > 0 a
+    whole shot-gradient (forward, residual, adjoint with the backward DFT,
+    gradient_F), else one forward. Returns (seconds, cell-updates)."""
+    kind, nx, ny, nz, nmech, nt, nf = args
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from pyoracle import Oracle, IfoParams
     from ifosb import synth
-    c = synth.small_case(nx=nx, ny=ny, nz=nz, nt=nt, fw=10, nmech=nmech, ntr=16, finv=())
+    finv = tuple(float(f) for f in np.linspace(200.0, 800.0, nf)) if nf else ()
+    c = synth.small_case(nx=nx, ny=ny, nz=nz, nt=nt, fw=10, nmech=nmech, ntr=16, finv=finv)
     p = c["params"]
     ip = IfoParams(nx=p.nx, ny=p.ny, nz=p.nz, dx=p.dx, dy=p.dy, dz=p.dz, dt=p.dt, nt=p.nt, time=p.time,
                    fdcoeff=p.fdcoeff, free_surf=p.free_surf, fw=p.fw, nmech=p.nmech, ndt=1, ndtshift=0,
                    vppml=c["vppml"], fpml=c["fpml"], alpha=0.0, beta=0.0, source_shape=4)
-    O = Oracle(kind)
+    O = Oracle(kind, threads=1)  # one core per process
     vp, vs, rho = c["start"]
     m = O.readmod(ip, vp, vs, rho, tau=c["tau"], fl=c["fl"])
     cp = O.cpml_coeff(ip)
     sp = c["shots"][0]
     sig = O.wavelet(ip, sp)
     t0 = time.perf_counter()
-    O.forward(ip, m, cp, sp, sig, c["recpos"])
-    return time.perf_counter() - t0, nx * ny * nz * nt
+    if nf:
+        f = O.forward(ip, m, cp, sp, sig, c["recpos"], c["finv"], 1, True)
+        obs = (f["sections"] * np.float32(0.9)).astype(np.float32)
+        d, _ = O.residual(ip, obs, f["sections"])
+        b = O.adjoint(ip, m, cp, c["recpos"], d, c["finv"], 1)
+        O.gradient(ip, m, c["finv"], f["dft"], b["dft"])
+        cells = 2 * nx * ny * nz * nt
+    else:
+        O.forward(ip, m, cp, sp, sig, c["recpos"])
+        cells = nx * ny * nz * nt
+    return time.perf_counter() - t0, cells
 
 
-def cpu_run(kind, nmech, procs, grid, nt):
-    """Run `procs` single-threaded oracle processes (spawned) on the sample; returns Gcell/s."""
+def cpu_run(kind, nmech, procs, grid, nt, nf=0):
+    """Run `procs` single-threaded oracle processes (spawned) on the sample; returns
+    (aggregate Gcell/s over the busiest process's time, over wall time, cells)."""
     import multiprocessing as mp
-    args = [(kind, grid[0], grid[1], grid[2], nmech, nt)] * procs
+    args = [(kind, grid[0], grid[1], grid[2], nmech, nt, nf)] * procs
     t0 = time.perf_counter()
     if procs == 1:
         res = [_cpu_sample_worker(args[0])]
@@ -170,6 +195,15 @@ def cpu_run(kind, nmech, procs, grid, nt):
     cells = sum(r[1] for r in res)
     busy = max(r[0] for r in res)
     return cells / busy / 1e9, cells / wall / 1e9, cells
+
+
+def cpu_sample(wl):
+    """The bounded CPU sample of a workload: (nmech, nf, grid, nt, what)."""
+    if wl == "visco384":
+        return 3, 4, (48, 48, 48), 40, "shot-gradient (forward + residual + adjoint + DFT + gradient_F)"
+    if wl == "elastic128":
+        return 0, 2, (64, 64, 64), 40, "shot-gradient (forward + residual + adjoint + DFT + gradient_F)"
+    return 3, 0, (64, 64, 64), 40, "forward step"
 
 
 def cpu_kind(nmech):
@@ -200,42 +234,56 @@ def setup_dist(args):
 
 
 def reference_arm(args, world, rank, dist):
-    """Times the reference's CPU implementation on this host's cores (rank 0 only)."""
+    """Times the reference's CPU implementation on this host's cores (rank 0 only):
+    one single-threaded process per core, each on a bounded sample of the workload's
+    step (shot parallelism, as the reference runs its MPI ranks per shot)."""
     if rank != 0:
         return
     import multiprocessing as mp
     wl = args.workload
-    nmech = 3 if wl == "visco256" else 0
+    nmech, nf, grid, nt, what = cpu_sample(wl)
+    nt = args.cpu_nt or nt
     code, kind = cpu_kind(nmech)
     procs = max(1, min(mp.cpu_count(), args.cpu_procs or mp.cpu_count()))
-    grid, nt = (64, 64, 64), args.cpu_nt
     for _ in range(args.warmup if args.cpu_warmup else 0):
-        cpu_run(code, nmech, procs, grid, max(2, nt // 4))
+        cpu_run(code, nmech, procs, grid, max(2, nt // 4), nf)
     vals, walls = [], []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        agg, _, cells = cpu_run(code, nmech, procs, grid, nt)
+        agg, _, cells = cpu_run(code, nmech, procs, grid, nt, nf)
         walls.append(time.perf_counter() - t0)
         vals.append(agg)
     value = float(np.median(vals))
-    sample = (f"{procs} single-threaded processes, each a {grid[0]}x{grid[1]}x{grid[2]} grid x {nt} steps "
-              f"(FW=10 CPML, free surface, L={nmech}) of the same algorithm; Gcell-updates/s aggregated")
+    impl = "the reference's own C functions (oracle/_ref)" if kind == "reference" else \
+        "the C restatement of the reference's algorithm (the reference stops at L=1)"
+    sample = (f"{procs} single-threaded processes on {cpu_model()}, each one {what} on a "
+              f"{grid[0]}x{grid[1]}x{grid[2]} grid x {nt} steps (FW=10 CPML, free surface, L={nmech}, nf={nf}) "
+              f"with {impl}; Gcell-updates/s aggregated")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": round(value, 5), "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * float(np.median(walls)), 1),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": workload_config(wl, world),
-        "cpu_baseline": {"value": round(value, 5), "unit": UNIT, "cores": procs, "kind": kind, "sample": sample},
+        "cpu_baseline": {"value": round(value, 5), "unit": UNIT, "cores": procs, "kind": kind, "sample": sample,
+                         "cpu_model": cpu_model()},
         "e2e": {"value": round(value, 5), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
 
+NT_VISCO384 = 100  # the batched-gradient configuration names no NT; 100 steps keep a step near 23 s
+
+
 def workload_config(wl, world, nt=None):
     if wl == "visco384":
+        nt = nt or NT_VISCO384
         return {"workload": "visco384: batched viscoelastic L=3 (Q=50, 20-200 Hz) shot-gradients (forward+residual+"
-                            f"adjoint+DFT gradient), 384x256x384 cells, NT={nt or 200}, 4 frequencies, 32 shots on an "
-                            "8x4 surface grid, 1024 receivers, 3 Gaussian blobs in a depth gradient",
-                "grid": [384, 256, 384], "nt": nt or 200, "nmech": 3, "nf": 4, "shots": 32, "receivers": 1024,
+                            f"adjoint+DFT gradient), 384x384 horizontal x 256 deep cells, NT={nt}, 4 frequencies, "
+                            "32 shots on an 8x4 surface grid, 1024 receivers, 3 Gaussian blobs in a depth gradient",
+                "grid": [384, 256, 384],
+                "grid_axes": "NX x NY x NZ with y the reference's depth axis: 384 x 384 horizontal (x, z), 256 deep",
+                "nt": nt, "nt_choice": "the configuration names no NT; DT=1e-4 s, NT chosen so that a step "
+                                       "(all 32 shot-gradients) takes about 23 s on one B200",
+                "nmech": 3, "nf": 4, "shots": 32, "receivers": 1024,
                 "parallelism": f"shot-sharded x{world}, FP64 gradient all-reduce per step",
                 "l2_flush": "state+DFT about 11 GB per shot > 126 MB L2"}
     if wl == "visco256":
@@ -255,13 +303,15 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="visco256", choices=["visco256", "elastic128", "visco384", "multiscale"])
+    ap.add_argument("--workload", default="visco384", choices=["visco384", "visco256", "elastic128", "multiscale"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nt", type=int, default=None, help="override NT (testing only)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--cpu-procs", type=int, default=0)
-    ap.add_argument("--cpu-nt", type=int, default=40)
+    ap.add_argument("--cpu-nt", type=int, default=0, help="time steps of the CPU sample (0 = the workload's)")
+    ap.add_argument("--e2e-steps", type=int, default=3, help="timed end-to-end steps (at most --steps)")
+    ap.add_argument("--per-shot-n", type=int, default=4, help="shots timed on the one-shot-per-launch path")
     ap.add_argument("--cpu-warmup", action="store_true")
     ap.add_argument("--grid", default=None, help="visco384 only: NX,NY,NZ (profiling runs)")
     ap.add_argument("--nshots", type=int, default=None, help="visco384 only: shots per step (profiling runs)")
@@ -417,18 +467,13 @@ def main():
     ach_str = b["stress"] * ncell / (ts / nsteps / 1000.0) / 1e9
     ach_vel = b["vel"] * ncell / (tv / nsteps / 1000.0) / 1e9
     # DRAM bytes per launch from an ncu capture of the same kernels (committed
-    # summary); null when no capture of this workload exists
-    traffic = None
-    tf = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tf):
-        try:
-            traffic = json.load(open(tf)).get(wl)
-        except Exception:
-            traffic = None
+    # summary, not this run); null when no capture of this workload exists
+    traffic = load_traffic(wl, ncell)
     roofline = {"bound": "hbm", "kernel": "time step = k_velocity + k_stress<L> (one launch each)",
                 "achieved": round(ach_step, 1), "peak": peak, "unit": "GB/s", "frac": round(ach_step / peak, 4),
                 "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
                 "traffic": traffic["time_step"] if traffic else None,
+                "traffic_source": traffic["source"] if traffic else "no ncu capture of this workload",
                 "alg_bytes_per_step": round(b["total"] * ncell), "alg_bytes_per_cell_step": round(b["total"], 2),
                 "per_kernel": {"k_stress": {"alg_bytes_per_cell": round(b["stress"], 2), "ms": round(ts / nsteps, 4),
                                             "achieved_gbs": round(ach_str, 1), "frac": round(ach_str / peak, 4),
@@ -457,12 +502,7 @@ def main():
         out["shot_gradients_small_grid"] = small_grid_comparison(torch, ifosb, synth, dev, stream, args.nt)
     # ---- CPU baseline (rank 0, N=1): the oracle on a bounded sample of this workload
     if rank == 0 and world == 1 and not args.no_cpu:
-        code, kind = cpu_kind(p.nmech)
-        grid, nt = (64, 64, 64), args.cpu_nt
-        v1, _, cells = cpu_run(code, p.nmech, 1, grid, nt)
-        out["cpu_baseline"] = {"value": round(v1, 5), "unit": UNIT, "cores": 1, "kind": kind,
-                               "sample": f"one core, {grid[0]}x{grid[1]}x{grid[2]} grid x {nt} steps of the "
-                                         f"same forward step (L={p.nmech}, FW=10 CPML, free surface)"}
+        out["cpu_baseline"] = cpu_baseline_line(wl, args)
     if rank == 0:
         print(json.dumps(out), flush=True)
     if dist:
@@ -470,11 +510,21 @@ def main():
         dist.destroy_process_group()
 
 
+def _pinned(torch, a):
+    return torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+
+
 def batched_gradient_workload(args, world, rank, local, dist):
-    """visco384: every rank takes its share of the 32 shots in batches as large as
-    its HBM holds (one launch per kernel and time step for a whole batch, the time
-    loop replayed from a CUDA graph); a step is the gradient of all 32 shots,
-    host observed traces in and the summed FP64 gradient out on every rank."""
+    """visco384 (the default): every rank takes its share of the 32 shots in batches
+    as large as its HBM holds (one launch per kernel and time step for a whole
+    batch, the time loop replayed from a CUDA graph); a step is the gradient of all
+    32 shots, summed in FP64 on every rank.
+
+    value: observed traces already resident in HBM, the gradient left there (and
+           all-reduced there when N > 1);
+    e2e:   the same step through the public API from host memory: the model and
+           the observed traces copied in from pinned buffers, the FP64 gradient and
+           the misfits read back, every step."""
     import torch
     import ifosb
     from ifosb import synth
@@ -482,7 +532,7 @@ def batched_gradient_workload(args, world, rank, local, dist):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream(dev)
-    nt = args.nt or 200
+    nt = args.nt or NT_VISCO384
     grid = tuple(int(x) for x in args.grid.split(",")) if args.grid else None
     c = synth.case("visco384", nt=nt, nshots=args.nshots, grid=grid)
     p = c["params"]
@@ -528,9 +578,10 @@ def batched_gradient_workload(args, world, rank, local, dist):
     obs = np.zeros((nshots, 3, eng.ntr, eng.ns), np.float32)
     for chunk in batches(mine, B):
         obs[chunk] = eng.forward([shots[i] for i in chunk]) * np.float32(0.9)
+    obs_dev = torch.from_numpy(obs).to(dev)
 
     def step():
-        return distributed_shot_gradient(eng, shots, obs, max_batch=B, dist=dist)
+        return distributed_shot_gradient(eng, shots, obs_dev, max_batch=B, dist=dist)
 
     for _ in range(args.warmup):
         step()
@@ -554,15 +605,36 @@ def batched_gradient_workload(args, world, rank, local, dist):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
     ncell = p.nx * p.ny * p.nz
-    cells = 2 * ncell * p.nt * nshots * args.steps
-    if grid or args.nshots:  # a reduced case: name what ran
-        out_grid, out_shots = [p.nx, p.ny, p.nz], nshots
-    else:
-        out_grid, out_shots = None, None
-    value = cells / (ms / 1000.0) / 1e9
+    cells_step = 2 * ncell * p.nt * nshots
+    value = cells_step * args.steps / (ms / 1000.0) / 1e9
     launches = args.steps * nbatch * (4 * p.nt + 3)
 
-    # roofline: per-kernel CUDA events over one profiled batched forward (with DFT)
+    # ---- end to end: host model and host observed traces in, FP64 gradient out, every step
+    hm = {k: _pinned(torch, ifosb.ghost_wrap(m[k])) for k in ("rho", "pi", "u", "taus", "taup")}
+    obs_pin = _pinned(torch, obs)
+    e2e_steps = max(1, min(args.steps, args.e2e_steps))
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    ev2, ev3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev2.record(stream)
+    for _ in range(e2e_steps):
+        eng.set_model(*(hm[k].numpy() for k in ("rho", "pi", "u", "taus", "taup")), m["eta"], ghosted=True)
+        hgrad, hmis = distributed_shot_gradient(eng, shots, obs_pin.numpy(), max_batch=B, dist=dist)
+    ev3.record(stream)
+    torch.cuda.synchronize(dev)
+    ms_e2e = ev2.elapsed_time(ev3)
+    if dist:
+        t = torch.tensor([ms_e2e], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    e2e = cells_step * e2e_steps / (ms_e2e / 1000.0) / 1e9
+    # the device-resident and host paths give the same gradient
+    same = bool(np.array_equal(grad.cpu().numpy(), hgrad) and np.array_equal(mis, hmis))
+    h2d = int(obs[mine].nbytes + sum(t.numel() * 4 for t in hm.values()))
+    d2h = int(hgrad.nbytes + hmis.nbytes)
+
+    # ---- roofline: per-kernel CUDA events over one profiled batched forward (with DFT)
     eng.set_profiling(True)
     eng.forward([shots[i] for i in mine[:B]], want_sections=False)
     tv, ts, nsteps = eng.kernel_times()
@@ -575,15 +647,21 @@ def batched_gradient_workload(args, world, rank, local, dist):
     ach = b["total"] * cb / ((tv + ts) / nsteps / 1000.0) / 1e9
     ach_s = b["stress"] * cb / (ts / nsteps / 1000.0) / 1e9
     ach_v = b["vel"] * cb / (tv / nsteps / 1000.0) / 1e9
+    traffic = load_traffic("visco384", cb)
     roofline = {"bound": "hbm", "kernel": f"time step of a {B}-shot batch = k_velocity + k_stress<3> with DFT",
                 "achieved": round(ach, 1), "peak": peak, "unit": "GB/s", "frac": round(ach / peak, 4),
                 "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
-                "traffic": None, "alg_bytes_per_cell_step": round(b["total"], 2),
+                "traffic": traffic["time_step"] if traffic else None,
+                "traffic_source": traffic["source"] if traffic else "no ncu capture of this workload",
+                "alg_bytes_per_cell_step": round(b["total"], 2), "alg_bytes_per_step": round(b["total"] * cb),
                 "per_kernel": {"k_stress": {"alg_bytes_per_cell": round(b["stress"], 2), "ms": round(ts / nsteps, 4),
-                                            "achieved_gbs": round(ach_s, 1), "frac": round(ach_s / peak, 4)},
+                                            "achieved_gbs": round(ach_s, 1), "frac": round(ach_s / peak, 4),
+                                            "traffic": traffic["k_stress"] if traffic else None},
                                "k_velocity": {"alg_bytes_per_cell": round(b["vel"], 2), "ms": round(tv / nsteps, 4),
-                                              "achieved_gbs": round(ach_v, 1), "frac": round(ach_v / peak, 4)}},
-                "adjoint_ms_per_step": {"k_stress": round(ats / ansteps, 4), "k_velocity": round(atv / ansteps, 4)}}
+                                              "achieved_gbs": round(ach_v, 1), "frac": round(ach_v / peak, 4),
+                                              "traffic": traffic["k_velocity"] if traffic else None}},
+                "adjoint_ms_per_step": {"k_stress": round(ats / ansteps, 4), "k_velocity": round(atv / ansteps, 4)},
+                "timing": "CUDA events around every launch of one forward and one adjoint, on the engine's stream"}
     out = {
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 2), "higher_is_better": True,
@@ -591,39 +669,143 @@ def batched_gradient_workload(args, world, rank, local, dist):
         "config": dict(workload_config("visco384", world, p.nt), shots_per_batch=B, batches_per_gpu=nbatch,
                        launch_shape=dict(tuned, picked_by="--shape" if args.shape else "ifosb_autotune")),
         "clocks": clocks,
-        "e2e": {"value": round(value, 3), "unit": UNIT, "note": "the step itself is end to end: host observed "
-                "traces in, the summed FP64 gradient out", "h2d_bytes_per_step": int(obs[mine].nbytes),
-                "d2h_bytes_per_step": int(grad.nbytes + mis.nbytes)},
-        "gpu_launches": int(launches), "roofline": roofline,
+        "e2e": {"value": round(e2e, 3), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "steps": e2e_steps, "shot_gradients_per_s": round(nshots * e2e_steps / (ms_e2e / 1000.0), 4),
+                "inputs": "ghosted model (rho, pi, u, taus, taup) and observed traces from pinned host memory",
+                "outputs": "FP64 gradient [3][NY][NX][NZ] and per-shot FP64 misfits to host",
+                "same_gradient_as_device_path": same},
+        "gpu_launches": int(launches), "graph_captures": eng.graph_captures, "roofline": roofline,
         "shot_gradients_per_s": round(nshots * args.steps / (ms / 1000.0), 4),
     }
     eng.close()
-    # one shot per launch sequence (plain launches) on the same GPU, two shots timed
+    del obs_dev
     if rank == 0 and world == 1 and not args.no_extras:
-        e1 = engine(1, 1)
-        e1.shot_gradient(shots[:1], obs[:1])
-        torch.cuda.synchronize(dev)
-        t0 = time.perf_counter()
-        for s in range(2):
-            e1.shot_gradient(shots[s:s + 1], obs[s:s + 1])
-        torch.cuda.synchronize(dev)
-        t1 = (time.perf_counter() - t0) / 2
-        e1.close()
-        out["per_shot_path"] = {"shot_gradients_per_s": round(1.0 / t1, 4),
-                                "batched_speedup": round(t1 * nshots * args.steps / (ms / 1000.0), 3),
-                                "timing": "host wall clock around 2 synchronised one-shot gradients"}
+        out["per_shot_path"] = per_shot_comparison(torch, ifosb, dev, stream, engine, shots, obs, B, tuned,
+                                                   nshots * args.steps / (ms / 1000.0), args.per_shot_n)
+        out["visco256_forward"] = visco256_forward(torch, ifosb, synth, dev, stream)
+        out["shot_gradients_elastic128"] = shot_gradient_comparison(torch, ifosb, synth, dev, stream, None)
+        out["shot_gradients_small_grid"] = small_grid_comparison(torch, ifosb, synth, dev, stream, None)
     if rank == 0 and world == 1 and not args.no_cpu:
-        code, kind = cpu_kind(p.nmech)
-        grid, cnt = (64, 64, 64), args.cpu_nt
-        v1, _, _ = cpu_run(code, p.nmech, 1, grid, cnt)
-        out["cpu_baseline"] = {"value": round(v1, 5), "unit": UNIT, "cores": 1, "kind": kind,
-                               "sample": f"one core, {grid[0]}x{grid[1]}x{grid[2]} grid x {cnt} steps of the "
-                                         f"same forward step (L={p.nmech}, FW=10 CPML, free surface)"}
-    if out_grid:
-        out["config"].update(grid=out_grid, shots=out_shots, workload="visco384 reduced for profiling: "
-                             f"{out_grid[0]}x{out_grid[1]}x{out_grid[2]} cells, {out_shots} shots, NT={p.nt}")
+        out["cpu_baseline"] = cpu_baseline_line("visco384", args)
+    if grid or args.nshots:  # a reduced case: name what ran
+        out["config"].update(grid=[p.nx, p.ny, p.nz], shots=nshots, workload="visco384 reduced for profiling: "
+                             f"{p.nx}x{p.ny}x{p.nz} cells, {nshots} shots, NT={p.nt}")
     if rank == 0:
         print(json.dumps(out), flush=True)
+
+
+def cpu_baseline_line(wl, args):
+    """The CPU implementation on one host core over a bounded sample of the workload's step."""
+    nmech, nf, grid, nt, what = cpu_sample(wl)
+    nt = args.cpu_nt or nt
+    code, kind = cpu_kind(nmech)
+    v1, _, _ = cpu_run(code, nmech, 1, grid, nt, nf)
+    impl = "the reference's own C functions (oracle/_ref)" if kind == "reference" else \
+        "the C restatement of the reference's algorithm (the reference stops at L=1)"
+    return {"value": round(v1, 5), "unit": UNIT, "cores": 1, "kind": kind, "cpu_model": cpu_model(),
+            "sample": f"one core, one {what} on a {grid[0]}x{grid[1]}x{grid[2]} grid x {nt} steps "
+                      f"(L={nmech}, nf={nf}, FW=10 CPML, free surface) with {impl}"}
+
+
+def per_shot_comparison(torch, ifosb, dev, stream, engine, shots, obs, B, tuned_batch, batched_rate, n):
+    """One shot per launch sequence on the same GPU, the time loop also replayed
+    from a CUDA graph (so the ratio isolates batching), autotuned for one shot;
+    its gradient of the first shots compared bit for bit with one batched launch."""
+    e1 = engine(1, 0)
+    tuned1 = e1.autotune(shots[:1], steps=min(40, e1.p.nt))
+    e1.shot_gradient(shots[:1], obs[:1])  # warm-up: graph capture
+    e1.zero_gradient()
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for s in range(n):
+        e1.shot_gradient(shots[s:s + 1], obs[s:s + 1])
+    torch.cuda.synchronize(dev)
+    t1 = (time.perf_counter() - t0) / n
+    g1 = e1.get_gradient()
+    e1.close()
+    # and kernel by kernel, without the graph (the plain one-shot-per-launch path)
+    e1 = engine(1, 1)
+    e1.set_launch_shape(1, tuned1)
+    e1.shot_gradient(shots[:1], obs[:1])
+    e1.zero_gradient()
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for s in range(n):
+        e1.shot_gradient(shots[s:s + 1], obs[s:s + 1])
+    torch.cuda.synchronize(dev)
+    tp = (time.perf_counter() - t0) / n
+    same_modes = np.array_equal(e1.get_gradient(), g1)
+    e1.close()
+    eb = engine(B, 0)
+    eb.set_launch_shape(n, tuned_batch)
+    eb.shot_gradient(shots[:n], obs[:n])
+    gb = eb.get_gradient()
+    eb.close()
+    return {"shot_gradients_per_s": round(1.0 / t1, 4), "batched_speedup": round(batched_rate * t1, 3),
+            "launch": "CUDA graph per shot (the same time-loop replay as the batched path)",
+            "plain_launch_shot_gradients_per_s": round(1.0 / tp, 4),
+            "batched_speedup_vs_plain_launch": round(batched_rate * tp, 3),
+            "launch_shape_one_shot": tuned1,
+            "timing": f"host wall clock around {n} synchronised one-shot gradients after a warm-up",
+            "gradients_bit_identical": bool(np.array_equal(g1, gb) and same_modes),
+            "compared": f"gradient of shots 0..{n - 1}: one shot per launch vs one {n}-shot launch"}
+
+
+def visco256_forward(torch, ifosb, synth, dev, stream, steps=2):
+    """The plain viscoelastic forward-modelling configuration (256^3, L=3, NT=3000,
+    400 receivers, one shot): Gcell-updates/s and the time-step roofline."""
+    c = synth.case("visco256")
+    p = c["params"]
+    m, cp, shots = synth.build_inputs(c)
+    e = ifosb.Engine(p, max_shots=1, max_nf=0)
+    e.set_stream(stream.cuda_stream)
+    e.set_cpml(cp)
+    e.set_model(m["rho"], m["pi"], m["u"], m["taus"], m["taup"], m["eta"])
+    e.set_receivers(c["recpos"])
+    e.set_frequencies(None, 1)
+    tuned = e.autotune(shots, steps=60)
+    e.forward(shots, want_sections=False)
+    torch.cuda.synchronize(dev)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(steps):
+        e.forward(shots, want_sections=False)
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = ev0.elapsed_time(ev1) / steps
+    e.set_profiling(True)
+    e.forward(shots, want_sections=False)
+    tv, ts, n = e.kernel_times()
+    e.close()
+    ncell = p.nx * p.ny * p.nz
+    b = alg_bytes_per_cell_step(p, 0, 1)
+    peak, _ = load_peaks()
+    ach = b["total"] * ncell / ((tv + ts) / n / 1000.0) / 1e9
+    return {"workload": "visco256: L=3 forward modelling, 256^3, NT=3000, 400 receivers, 1 shot",
+            "gcell_updates_per_s": round(ncell * p.nt / (ms / 1000.0) / 1e9, 3), "ms_per_forward": round(ms, 1),
+            "steps": steps, "launch_shape": tuned,
+            "roofline_time_step": {"alg_bytes_per_cell_step": round(b["total"], 2), "achieved_gbs": round(ach, 1),
+                                   "frac": round(ach / peak, 4), "k_velocity_ms": round(tv / n, 4),
+                                   "k_stress_ms": round(ts / n, 4)}}
+
+
+def load_traffic(wl, cell_shots):
+    """DRAM bytes per launch from the committed ncu summaries (profiles/traffic.json),
+    per cell-shot scaled to this launch when the capture ran a smaller case; None
+    when no capture of the workload exists."""
+    tf = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        d = json.load(open(tf)).get(wl)
+    except Exception:
+        return None
+    if not d:
+        return None
+    scale = cell_shots / d["cell_shots"] if d.get("cell_shots") else 1.0
+    src = "profiles/traffic.json (an earlier ncu capture, not this run)"
+    if scale != 1.0:
+        src += f": {d['captured']}, scaled by cell-shots x{scale:.1f}"
+    return {"k_velocity": int(d["k_velocity"] * scale), "k_stress": int(d["k_stress"] * scale),
+            "time_step": int(d["time_step"] * scale), "source": src}
 
 
 def multiscale_workload(args, local):
@@ -782,22 +964,32 @@ def _compare_batched(torch, ifosb, synth, dev, stream, c, nshots, label):
     tb = time.perf_counter() - t0
     gb = eb.get_gradient()
     eb.close()
-    e1 = make(1, 1)
-    e1.set_model(m["rho"], m["pi"], m["u"], m["taus"], m["taup"], m["eta"])
-    e1.shot_gradient(shots[:1], obs[:1])  # warm-up
-    e1.zero_gradient()
-    torch.cuda.synchronize(dev)
-    t0 = time.perf_counter()
-    for s in range(nshots):
-        e1.shot_gradient(shots[s:s + 1], obs[s:s + 1])
-    torch.cuda.synchronize(dev)
-    t1 = time.perf_counter() - t0
-    g1 = e1.get_gradient()
-    e1.close()
+    per_shot, g1 = {}, None
+    for mode, name in ((0, "graph"), (1, "plain")):
+        e1 = make(1, mode)
+        e1.set_model(m["rho"], m["pi"], m["u"], m["taus"], m["taup"], m["eta"])
+        e1.shot_gradient(shots[:1], obs[:1])  # warm-up (graph capture in mode 0)
+        e1.zero_gradient()
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        for s in range(nshots):
+            e1.shot_gradient(shots[s:s + 1], obs[s:s + 1])
+        torch.cuda.synchronize(dev)
+        per_shot[name] = time.perf_counter() - t0
+        g = e1.get_gradient()
+        g1 = g if g1 is None else g1
+        same_modes = np.array_equal(g, g1)
+        e1.close()
+    t1 = per_shot["graph"]
     return {"workload": f"{label}, NT={p.nt}, nf={len(c['finv'])}", "batched_per_s": round(nshots / tb, 4),
             "per_shot_per_s": round(nshots / t1, 4), "speedup": round(t1 / tb, 3),
+            "per_shot_plain_launch_per_s": round(nshots / per_shot["plain"], 4),
+            "speedup_vs_plain_launch": round(per_shot["plain"] / tb, 3),
             "gcells_batched": round(2 * nshots * p.nx * p.ny * p.nz * p.nt / tb / 1e9, 3),
-            "gradients_bit_identical": bool(np.array_equal(gb, g1)), "timing": "host wall clock around synchronised calls"}
+            "gradients_bit_identical": bool(np.array_equal(gb, g1) and same_modes),
+            "per_shot": "one shot per launch sequence, the time loop replayed from a CUDA graph (per_shot_per_s, "
+                        "speedup) or launched kernel by kernel (plain_launch)",
+            "timing": "host wall clock around synchronised calls"}
 
 
 if __name__ == "__main__":

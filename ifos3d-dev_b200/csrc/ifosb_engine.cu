@@ -1057,7 +1057,8 @@ extern "C" int ifosb_residual(ifosb_engine *e, const float *obs, double *misfit_
     if (!e->fwd_ok || e->ntr == 0) return fail(e, IFOSB_ESTATE, "residual needs a forward batch with receivers");
     const int nshots = e->nshots, ntr = e->ntr, ns = e->ns;
     const size_t n = (size_t)nshots * 3 * ntr * ns;
-    CU(cudaMemcpyAsync(e->d_obs, obs, n * sizeof(float), cudaMemcpyHostToDevice, e->stream));
+    // obs may be host or device memory (unified addressing picks the copy's direction)
+    CU(cudaMemcpyAsync(e->d_obs, obs, n * sizeof(float), cudaMemcpyDefault, e->stream));
     const int nthr = nshots * 3 * ntr;
     k_residual<<<(nthr + 127) / 128, 128, 0, e->stream>>>(e->d_sec, e->d_obs, e->d_diff, e->d_part, nshots, ntr, ns, e->p.dt);
     k_misfit<<<nshots, 32, 0, e->stream>>>(e->d_part, e->d_misfit, 3 * ntr);
@@ -1502,8 +1503,9 @@ extern "C" int ifosb_get_gradient_q(ifosb_engine *e, double *gradq) {
 extern "C" int ifosb_get_gradient(ifosb_engine *e, float *grad, double *grad64) {
     if (!e) return IFOSB_EARG;
     const size_t n = (size_t)3 * e->p.nx * e->p.ny * e->p.nz;
-    if (grad) CU(cudaMemcpyAsync(grad, e->d_grad, n * sizeof(float), cudaMemcpyDeviceToHost, e->stream));
-    if (grad64) CU(cudaMemcpyAsync(grad64, e->d_grad64, n * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+    // host or device destinations (unified addressing)
+    if (grad) CU(cudaMemcpyAsync(grad, e->d_grad, n * sizeof(float), cudaMemcpyDefault, e->stream));
+    if (grad64) CU(cudaMemcpyAsync(grad64, e->d_grad64, n * sizeof(double), cudaMemcpyDefault, e->stream));
     CU(cudaStreamSynchronize(e->stream));
     return IFOSB_OK;
 }

@@ -168,6 +168,22 @@ def _f32(a):
     return None if a is None else np.ascontiguousarray(a, dtype=np.float32)
 
 
+def _is_tensor(a) -> bool:
+    return hasattr(a, "data_ptr") and hasattr(a, "is_cuda")
+
+
+def _traces(a):
+    """(keep-alive object, address) of observed traces: a numpy array (host) or a
+    contiguous float32 CUDA tensor (device-resident traces, no host copy)."""
+    if _is_tensor(a):
+        import torch
+        if not (a.is_cuda and a.dtype == torch.float32 and a.is_contiguous()):
+            raise ValueError("device traces must be a contiguous float32 CUDA tensor")
+        return a, a.data_ptr()
+    h = _f32(a)
+    return h, _p(h)
+
+
 def make_params(nx, ny, nz, dh=1.0, dt=1e-4, nt=100, fdcoeff=2, free_surf=1, fw=10, nmech=0, ndt=1, ndtshift=0,
                 alpha=0.0, beta=0.0, dx=None, dy=None, dz=None) -> Params:
     """Parameters as the reference derives them: TIME=(NT-1)*DT in float (ifos3d.c:176-177)."""
@@ -360,11 +376,12 @@ class Engine:
         self._c(lib().ifosb_set_launch_shape(self.h, nshots, _p(arr)))
 
     def residual(self, obs, want_l2_ref=False):
-        obs = _f32(obs)
+        """obs: host traces (numpy) or device-resident ones (a float32 CUDA tensor)."""
+        obs, addr = _traces(obs)
         nsh = obs.shape[0]
         mis = np.zeros(nsh, np.float64)
         l2 = np.zeros(nsh, np.float32) if want_l2_ref else None
-        self._c(lib().ifosb_residual(self.h, _p(obs), _p(mis), _p(l2)))
+        self._c(lib().ifosb_residual(self.h, addr, _p(mis), _p(l2)))
         return (mis, l2) if want_l2_ref else mis
 
     def adjoint(self, diff=None):
@@ -417,19 +434,35 @@ class Engine:
         self._c(lib().ifosb_get_hessian(self.h, _p(h)))
         return h
 
-    def get_gradient(self, fp64=False):
-        g = np.zeros((3, self.p.ny, self.p.nx, self.p.nz), np.float64 if fp64 else np.float32)
-        if fp64:
-            self._c(lib().ifosb_get_gradient(self.h, None, _p(g)))
+    def get_gradient(self, fp64=False, out=None):
+        """The accumulated gradient [3, NY, NX, NZ]: a new host array, or copied into
+        `out` (a host array, or a contiguous CUDA tensor of the right dtype)."""
+        shape = (3, self.p.ny, self.p.nx, self.p.nz)
+        if out is None:
+            out = np.zeros(shape, np.float64 if fp64 else np.float32)
+        if _is_tensor(out):
+            import torch
+            want = torch.float64 if fp64 else torch.float32
+            if not (out.is_cuda and out.dtype == want and out.is_contiguous() and tuple(out.shape) == shape):
+                raise ValueError(f"gradient tensor must be a contiguous CUDA {want} tensor of shape {shape}")
+            addr = out.data_ptr()
         else:
-            self._c(lib().ifosb_get_gradient(self.h, _p(g), None))
-        return g
+            if out.dtype != (np.float64 if fp64 else np.float32) or not out.flags.c_contiguous or out.shape != shape:
+                raise ValueError("gradient array of the wrong dtype, layout or shape")
+            addr = _p(out)
+        if fp64:
+            self._c(lib().ifosb_get_gradient(self.h, None, addr))
+        else:
+            self._c(lib().ifosb_get_gradient(self.h, addr, None))
+        return out
 
     def shot_gradient(self, shots, obs):
+        """forward + residual + adjoint + gradient of a batch; obs host (numpy) or
+        device-resident (float32 CUDA tensor). Returns the FP64 misfit per shot."""
         arr, keep = self._shots(shots)
-        obs = _f32(obs)
+        obs, addr = _traces(obs)
         mis = np.zeros(len(shots), np.float64)
-        self._c(lib().ifosb_shot_gradient(self.h, len(shots), arr, _p(obs), _p(mis)))
+        self._c(lib().ifosb_shot_gradient(self.h, len(shots), arr, addr, _p(mis)))
         return mis
 
     def get_field(self, shot: int, field: int) -> np.ndarray:

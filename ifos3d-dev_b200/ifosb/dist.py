@@ -53,20 +53,34 @@ def distributed_shot_gradient(eng, shots, obs, max_batch: int, dist=None, group=
 
     eng: this rank's engine (``ifosb.Engine`` or an object with the same
     ``zero_gradient``/``shot_gradient``/``get_gradient`` methods); shots: the
-    full list of (srcpos, signals); obs: [nshots][3][ntr][ns] observed traces.
+    full list of (srcpos, signals); obs: [nshots][3][ntr][ns] observed traces,
+    host (numpy) or already resident on this rank's GPU (a float32 CUDA tensor).
     Returns (gradient FP64 [3][NY][NX][NZ] summed over all shots, misfit FP64
-    [nshots]) — identical on every rank."""
+    [nshots]) — identical on every rank. With host traces the gradient comes back
+    as a host array; with device traces it stays on the device (a CUDA tensor)
+    and the exchange runs there."""
     world = dist.get_world_size(group) if dist is not None else 1
     rank = dist.get_rank(group) if dist is not None else 0
     nshots = len(shots)
+    device = hasattr(obs, "is_cuda") and obs.is_cuda
     mis = np.zeros(nshots, np.float64)
     grad = None
     err = None
     try:
         eng.zero_gradient()
         for chunk in batches(shard(nshots, world, rank), max_batch):
-            mis[chunk] = eng.shot_gradient([shots[i] for i in chunk], np.asarray(obs)[chunk])
-        grad = np.asarray(eng.get_gradient(fp64=True), np.float64)
+            if device:
+                contiguous = chunk == list(range(chunk[0], chunk[-1] + 1))
+                o = obs[chunk[0]:chunk[-1] + 1] if contiguous else obs[chunk].contiguous()
+            else:
+                o = np.asarray(obs)[chunk]
+            mis[chunk] = eng.shot_gradient([shots[i] for i in chunk], o)
+        if device:
+            import torch
+            grad = torch.empty((3, eng.p.ny, eng.p.nx, eng.p.nz), dtype=torch.float64, device=obs.device)
+            eng.get_gradient(fp64=True, out=grad)
+        else:
+            grad = np.asarray(eng.get_gradient(fp64=True), np.float64)
     except Exception as e:  # reported to every rank below, then raised everywhere
         err = e
     if dist is None or world == 1:
@@ -82,6 +96,12 @@ def distributed_shot_gradient(eng, shots, obs, max_batch: int, dist=None, group=
     failed = [r for r, v in enumerate(st.cpu().numpy()) if v != 0.0]
     if failed:
         raise ShotGradientError(failed, err) from err
+    if device:
+        # the gradient stays where it is: one all-reduce of it, one of the misfits
+        dist.all_reduce(grad, op=dist.ReduceOp.SUM, group=group)
+        mt = _buffer(torch, dist, group, mis)
+        dist.all_reduce(mt, op=dist.ReduceOp.SUM, group=group)
+        return grad, mt.cpu().numpy()
     buf = _buffer(torch, dist, group, np.concatenate([grad.ravel(), mis]))
     dist.all_reduce(buf, op=dist.ReduceOp.SUM, group=group)
     out = buf.cpu().numpy()

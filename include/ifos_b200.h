@@ -114,7 +114,8 @@ int ifosb_set_frequencies(ifosb_engine *e, int nf, const float *finv, int ntast)
 int ifosb_forward(ifosb_engine *e, int nshots, const ifosb_shot *shots, float *sections);
 
 /* residual() for every shot of the last forward batch (src/ifos3d.c:837-858):
- * obs [nshots][3][ntr][ns] observed traces (host). Forms the time-reversed
+ * obs [nshots][3][ntr][ns] observed traces (host memory, or device memory of the
+ * engine's GPU for traces already resident there). Forms the time-reversed
  * displacement residual on the device. misfit_fp64 (optional, [nshots]) gets
  * sum(residual^2) reduced in FP64; l2_ref (optional, [nshots]) gets the same
  * sum in the reference's float accumulation order. */
@@ -165,11 +166,13 @@ int ifosb_get_gradient_q(ifosb_engine *e, double *gradq);
 int ifosb_zero_gradient(ifosb_engine *e);
 
 /* Copy the accumulated gradient out: grad[3][NY][NX][NZ] (vp, vs, rho; the layout of
- * grad1..3 interior) and/or the FP64 accumulation grad64[3][NY][NX][NZ]. */
+ * grad1..3 interior) and/or the FP64 accumulation grad64[3][NY][NX][NZ]. Either may
+ * be host memory or device memory (e.g. a buffer for a device-side all-reduce). */
 int ifosb_get_gradient(ifosb_engine *e, float *grad, double *grad64);
 
 /* forward + residual + adjoint + gradient for a batch: the per-shot body of
- * src/ifos3d.c:712-975 for nshots shots at once. misfit (optional): [nshots] FP64. */
+ * src/ifos3d.c:712-975 for nshots shots at once. obs as for ifosb_residual (host or
+ * device memory); misfit (optional): [nshots] FP64, host. */
 int ifosb_shot_gradient(ifosb_engine *e, int nshots, const ifosb_shot *shots,
                         const float *obs, double *misfit);
 

@@ -25,6 +25,56 @@
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
+#include <pthread.h>
+#include <unistd.h>
+
+/* Threads of the cell loops (1 unless ifo_set_threads says otherwise). Every
+ * cell of a parallel loop reads only fields that the loop does not write and
+ * writes only its own entries, so the results do not depend on the count. */
+#define MAX_THREADS 256
+static int g_threads = 1;
+
+void ifo_set_threads(int n) {
+    if (n <= 0) n = (int)sysconf(_SC_NPROCESSORS_ONLN);
+    g_threads = n < 1 ? 1 : (n > MAX_THREADS ? MAX_THREADS : n);
+}
+
+/* rows lo..hi of a loop, split into contiguous blocks over the threads */
+typedef void (*rows_fn)(void *ctx, int lo, int hi);
+typedef struct {
+    rows_fn fn;
+    void *ctx;
+    int lo, hi;
+} par_job;
+
+static void *par_body(void *a) {
+    par_job *q = a;
+    q->fn(q->ctx, q->lo, q->hi);
+    return NULL;
+}
+
+static void par_rows(int lo, int hi, rows_fn fn, void *ctx) {
+    const int n = hi - lo + 1, T = g_threads < n ? g_threads : n;
+    if (T <= 1) {
+        fn(ctx, lo, hi);
+        return;
+    }
+    pthread_t th[MAX_THREADS];
+    par_job jb[MAX_THREADS];
+    int ok[MAX_THREADS];
+    for (int t = 0; t < T; t++) {
+        jb[t].fn = fn;
+        jb[t].ctx = ctx;
+        jb[t].lo = lo + (int)((long long)n * t / T);
+        jb[t].hi = lo + (int)((long long)n * (t + 1) / T) - 1;
+    }
+    for (int t = 1; t < T; t++) ok[t] = pthread_create(&th[t], NULL, par_body, &jb[t]) == 0;
+    par_body(&jb[0]);
+    for (int t = 1; t < T; t++) {
+        if (ok[t]) pthread_join(th[t], NULL);
+        else par_body(&jb[t]); /* no thread: run the block here */
+    }
+}
 
 #define PI_REF (3.141592653589793) /* fd.h:39 */
 #define MAXMECH 8
@@ -587,6 +637,29 @@ static void orc_state_out(orc_t *o, float *state9) {
 }
 
 /* disc_fourier.c:28-61 */
+typedef struct {
+    orc_t *o;
+    float *F[6];
+    double trig1, trig2;
+} dft_ctx;
+
+static void dft_rows(void *vc, int j0, int j1) {
+    dft_ctx *d = vc;
+    orc_t *o = d->o;
+    const geo_t G = o->G;
+    for (int j = j0; j <= j1; j++)
+        for (int i = 1; i <= G.nx; i++)
+            for (int k = 1; k <= G.nz; k++) {
+                size_t c = W(j, i, k);
+                d->F[0][c] += o->vx[c] * d->trig1;
+                d->F[1][c] += o->vy[c] * d->trig1;
+                d->F[2][c] += o->vz[c] * d->trig1;
+                d->F[3][c] += o->vx[c] * d->trig2;
+                d->F[4][c] += o->vy[c] * d->trig2;
+                d->F[5][c] += o->vz[c] * d->trig2;
+            }
+}
+
 static void dft_step(orc_t *o, int nt, int back, int nf, const float *finv, int ntast, float *dft) {
     const geo_t G = o->G;
     const ifo_params *p = o->p;
@@ -594,21 +667,12 @@ static void dft_step(orc_t *o, int nt, int back, int nf, const float *finv, int 
     if (back == 0) t = nt * p->dt;
     if (back == 1) t = p->time - nt * p->dt;
     for (int l = 0; l < nf; l++) {
-        double trig1 = cos(2.0 * t * finv[l] * M_PI) * p->dt * ntast;
-        double trig2 = sin(2.0 * t * finv[l] * M_PI) * p->dt * ntast;
-        float *F[6];
-        for (int q = 0; q < 6; q++) F[q] = dft + ((size_t)q * nf + l) * G.wn;
-        for (int j = 1; j <= G.ny; j++)
-            for (int i = 1; i <= G.nx; i++)
-                for (int k = 1; k <= G.nz; k++) {
-                    size_t c = W(j, i, k);
-                    F[0][c] += o->vx[c] * trig1;
-                    F[1][c] += o->vy[c] * trig1;
-                    F[2][c] += o->vz[c] * trig1;
-                    F[3][c] += o->vx[c] * trig2;
-                    F[4][c] += o->vy[c] * trig2;
-                    F[5][c] += o->vz[c] * trig2;
-                }
+        dft_ctx d;
+        d.o = o;
+        d.trig1 = cos(2.0 * t * finv[l] * M_PI) * p->dt * ntast;
+        d.trig2 = sin(2.0 * t * finv[l] * M_PI) * p->dt * ntast;
+        for (int q = 0; q < 6; q++) d.F[q] = dft + ((size_t)q * nf + l) * G.wn;
+        par_rows(1, G.ny, dft_rows, &d);
     }
 }
 
@@ -621,6 +685,35 @@ static float psource_amp(const ifo_params *p, const float *s, int nt) {
     return amp;
 }
 
+typedef struct {
+    orc_t *o;
+    int nt, back, npt;
+    const pt_t *pts;
+    const float *sigx, *sigy, *sigz;
+} vrow_ctx;
+
+static void v_rows(void *vc, int j0, int j1) {
+    vrow_ctx *v = vc;
+    const geo_t G = v->o->G;
+    for (int j = j0; j <= j1; j++)
+        for (int i = 1; i <= G.nx; i++)
+            for (int k = 1; k <= G.nz; k++) v_cell(v->o, j, i, k, v->nt, v->back, v->npt, v->pts, v->sigx, v->sigy, v->sigz);
+}
+
+static void s_rows(void *vc, int j0, int j1) {
+    orc_t *o = vc;
+    const geo_t G = o->G;
+    for (int j = j0; j <= j1; j++)
+        for (int i = 1; i <= G.nx; i++)
+            for (int k = 1; k <= G.nz; k++) s_cell(o, j, i, k);
+}
+
+static void surface_cols(void *vc, int k0, int k1) {
+    orc_t *o = vc;
+    for (int k = k0; k <= k1; k++)
+        for (int i = 1; i <= o->G.nx; i++) surface_cell(o, i, k);
+}
+
 static void run_loop(orc_t *o, int back, int npt, const pt_t *pts, const float *sigx, const float *sigy,
                      const float *sigz, int ntr, const int *recpos, float *sections,
                      int nf, const float *finv, int ntast, float *dft) {
@@ -628,12 +721,9 @@ static void run_loop(orc_t *o, int back, int npt, const pt_t *pts, const float *
     const ifo_params *p = o->p;
     int ns = ifo_nsamples(p), lsamp = p->ndtshift + 1, nlsamp = 1;
     for (int nt = 1; nt <= p->nt; nt++) {
-        for (int j = 1; j <= G.ny; j++)
-            for (int i = 1; i <= G.nx; i++)
-                for (int k = 1; k <= G.nz; k++) v_cell(o, j, i, k, nt, back, npt, pts, sigx, sigy, sigz);
-        for (int j = 1; j <= G.ny; j++)
-            for (int i = 1; i <= G.nx; i++)
-                for (int k = 1; k <= G.nz; k++) s_cell(o, j, i, k);
+        vrow_ctx vc = {o, nt, back, npt, pts, sigx, sigy, sigz};
+        par_rows(1, G.ny, v_rows, &vc);
+        par_rows(1, G.ny, s_rows, o);
         if (!back)
             for (int l = 0; l < npt; l++)
                 if (pts[l].kind == 1) {
@@ -642,9 +732,7 @@ static void run_loop(orc_t *o, int back, int npt, const pt_t *pts, const float *
                     o->sxx[c] += amp; o->syy[c] += amp; o->szz[c] += amp;
                 }
         if (nf > 0 && nt % ntast == 0) dft_step(o, nt, back, nf, finv, ntast, dft);
-        if (p->free_surf)
-            for (int k = 1; k <= G.nz; k++)
-                for (int i = 1; i <= G.nx; i++) surface_cell(o, i, k);
+        if (p->free_surf) par_rows(1, G.nz, surface_cols, o);
         if (ntr > 0 && nt == lsamp) {
             if (sections && nlsamp <= ns)
                 for (int t = 0; t < ntr; t++) {
@@ -731,56 +819,81 @@ int ifo_adjoint(const ifo_params *p, const float *rho, const float *pi, const fl
 }
 
 /* gradient_F.c:62-139 */
+/* gradient_F.c:30-171 for one frequency, rows j0..j1 */
+typedef struct {
+    const ifo_params *p;
+    geo_t G;
+    float b1, b2, fdummy;
+    const float *f[6], *bk[6];
+    const float *rho, *pi, *u;
+    float *grad;
+} grad_ctx;
+
+static void grad_rows(void *vc, int j0, int j1) {
+    const grad_ctx *q = vc;
+    const geo_t G = q->G;
+    const float b1 = q->b1, b2 = q->b2, fdummy = q->fdummy;
+    const float DX = q->p->dx, DY = q->p->dy, DZ = q->p->dz;
+    const float *const *f = q->f, *const *bk = q->bk;
+    const float *rho = q->rho, *pi = q->pi, *u = q->u;
+    float *grad = q->grad;
+    const size_t n = (size_t)G.nx * G.ny * G.nz;
+    for (int j = j0; j <= j1; j++)
+        for (int i = 1; i <= G.nx; i++)
+            for (int k = 1; k <= G.nz; k++) {
+                float d[4][9]; /* fwd re, back re, fwd im, back im; xx xy xz yx yy yz zx zy zz */
+                const float *src[4][3] = {{f[0], f[1], f[2]}, {bk[0], bk[1], bk[2]}, {f[3], f[4], f[5]}, {bk[3], bk[4], bk[5]}};
+                for (int s = 0; s < 4; s++) {
+                    const float *X = src[s][0], *Y = src[s][1], *Z = src[s][2];
+                    d[s][0] = (b1 * (X[W(j, i, k)] - X[W(j, i - 1, k)]) + b2 * (X[W(j, i + 1, k)] - X[W(j, i - 2, k)])) / DX;
+                    d[s][1] = (b1 * (X[W(j + 1, i, k)] - X[W(j, i, k)]) + b2 * (X[W(j + 2, i, k)] - X[W(j - 1, i, k)])) / DY;
+                    d[s][2] = (b1 * (X[W(j, i, k + 1)] - X[W(j, i, k)]) + b2 * (X[W(j, i, k + 2)] - X[W(j, i, k - 1)])) / DZ;
+                    d[s][3] = (b1 * (Y[W(j, i + 1, k)] - Y[W(j, i, k)]) + b2 * (Y[W(j, i + 2, k)] - Y[W(j, i - 1, k)])) / DX;
+                    d[s][4] = (b1 * (Y[W(j, i, k)] - Y[W(j - 1, i, k)]) + b2 * (Y[W(j + 1, i, k)] - Y[W(j - 2, i, k)])) / DY;
+                    d[s][5] = (b1 * (Y[W(j, i, k + 1)] - Y[W(j, i, k)]) + b2 * (Y[W(j, i, k + 2)] - Y[W(j, i, k - 1)])) / DZ;
+                    d[s][6] = (b1 * (Z[W(j, i + 1, k)] - Z[W(j, i, k)]) + b2 * (Z[W(j, i + 2, k)] - Z[W(j, i - 1, k)])) / DX;
+                    d[s][7] = (b1 * (Z[W(j + 1, i, k)] - Z[W(j, i, k)]) + b2 * (Z[W(j + 2, i, k)] - Z[W(j - 1, i, k)])) / DY;
+                    d[s][8] = (b1 * (Z[W(j, i, k)] - Z[W(j, i, k - 1)]) + b2 * (Z[W(j, i, k + 1)] - Z[W(j, i, k - 2)])) / DZ;
+                }
+                float *fv = d[0], *bv = d[1], *fi = d[2], *bi = d[3];
+                float gradlam = 0.0, gradmu = 0.0, gradrho = 0.0;
+                gradlam = (fv[0] + fv[4] + fv[8]) * (bv[0] + bv[4] + bv[8]) + (fi[0] + fi[4] + fi[8]) * (bi[0] + bi[4] + bi[8]);
+                gradlam = -gradlam * fdummy;
+                gradmu = 2 * fv[0] * bv[0] + 2 * fv[4] * bv[4] + 2 * fv[8] * bv[8] + 2 * fi[0] * bi[0] + 2 * fi[4] * bi[4] +
+                         2 * fi[8] * bi[8] + (fv[1] + fv[3]) * (bv[1] + bv[3]) + (fi[1] + fi[3]) * (bi[1] + bi[3]) +
+                         (fv[2] + fv[6]) * (bv[2] + bv[6]) + (fi[2] + fi[6]) * (bi[2] + bi[6]) +
+                         (fv[5] + fv[7]) * (bv[5] + bv[7]) + (fi[5] + fi[7]) * (bi[5] + bi[7]);
+                gradmu = -gradmu * fdummy;
+                size_t c = W(j, i, k), m = M(j, i, k);
+                gradrho = (f[0][c] * bk[0][c] + f[1][c] * bk[1][c] + f[2][c] * bk[2][c]) +
+                          (f[3][c] * bk[3][c] + f[4][c] * bk[4][c] + f[5][c] * bk[5][c]);
+                float r = rho[m], pp = pi[m], uu = u[m];
+                grad[0 * n + m] += sqrt(r * pp) * 2 * gradlam;
+                grad[1 * n + m] += -4 * sqrt(r * uu) * gradlam + 2 * sqrt(r * uu) * gradmu;
+                grad[2 * n + m] += gradrho + uu / r * gradmu + (pp - 2 * uu) / r * gradlam;
+            }
+}
+
 int ifo_gradient(const ifo_params *p, const float *rho, const float *pi, const float *u,
                  int nf, const float *finv, const float *dft_fwd, const float *dft_back, float *grad) {
-    geo_t G = mkgeo(p);
-    float b1, b2;
-    fd_coeffs(p, &b1, &b2);
-    const float DX = p->dx, DY = p->dy, DZ = p->dz;
-    size_t n = (size_t)G.nx * G.ny * G.nz;
+    grad_ctx q;
+    q.p = p;
+    q.G = mkgeo(p);
+    fd_coeffs(p, &q.b1, &q.b2);
+    q.rho = rho;
+    q.pi = pi;
+    q.u = u;
+    q.grad = grad;
     for (int l = 0; l < nf; l++) {
         float fdummy = 0.0;
         fdummy = 2.0 * 2.0 * finv[l] * finv[l] * M_PI * M_PI;
         fdummy = 1 / fdummy;
-        const float *f[6], *bk[6];
-        for (int q = 0; q < 6; q++) {
-            f[q] = dft_fwd + ((size_t)q * nf + l) * G.wn;
-            bk[q] = dft_back + ((size_t)q * nf + l) * G.wn;
+        q.fdummy = fdummy;
+        for (int c = 0; c < 6; c++) {
+            q.f[c] = dft_fwd + ((size_t)c * nf + l) * q.G.wn;
+            q.bk[c] = dft_back + ((size_t)c * nf + l) * q.G.wn;
         }
-        for (int j = 1; j <= G.ny; j++)
-            for (int i = 1; i <= G.nx; i++)
-                for (int k = 1; k <= G.nz; k++) {
-                    float d[4][9]; /* fwd re, back re, fwd im, back im; xx xy xz yx yy yz zx zy zz */
-                    const float *src[4][3] = {{f[0], f[1], f[2]}, {bk[0], bk[1], bk[2]}, {f[3], f[4], f[5]}, {bk[3], bk[4], bk[5]}};
-                    for (int s = 0; s < 4; s++) {
-                        const float *X = src[s][0], *Y = src[s][1], *Z = src[s][2];
-                        d[s][0] = (b1 * (X[W(j, i, k)] - X[W(j, i - 1, k)]) + b2 * (X[W(j, i + 1, k)] - X[W(j, i - 2, k)])) / DX;
-                        d[s][1] = (b1 * (X[W(j + 1, i, k)] - X[W(j, i, k)]) + b2 * (X[W(j + 2, i, k)] - X[W(j - 1, i, k)])) / DY;
-                        d[s][2] = (b1 * (X[W(j, i, k + 1)] - X[W(j, i, k)]) + b2 * (X[W(j, i, k + 2)] - X[W(j, i, k - 1)])) / DZ;
-                        d[s][3] = (b1 * (Y[W(j, i + 1, k)] - Y[W(j, i, k)]) + b2 * (Y[W(j, i + 2, k)] - Y[W(j, i - 1, k)])) / DX;
-                        d[s][4] = (b1 * (Y[W(j, i, k)] - Y[W(j - 1, i, k)]) + b2 * (Y[W(j + 1, i, k)] - Y[W(j - 2, i, k)])) / DY;
-                        d[s][5] = (b1 * (Y[W(j, i, k + 1)] - Y[W(j, i, k)]) + b2 * (Y[W(j, i, k + 2)] - Y[W(j, i, k - 1)])) / DZ;
-                        d[s][6] = (b1 * (Z[W(j, i + 1, k)] - Z[W(j, i, k)]) + b2 * (Z[W(j, i + 2, k)] - Z[W(j, i - 1, k)])) / DX;
-                        d[s][7] = (b1 * (Z[W(j + 1, i, k)] - Z[W(j, i, k)]) + b2 * (Z[W(j + 2, i, k)] - Z[W(j - 1, i, k)])) / DY;
-                        d[s][8] = (b1 * (Z[W(j, i, k)] - Z[W(j, i, k - 1)]) + b2 * (Z[W(j, i, k + 1)] - Z[W(j, i, k - 2)])) / DZ;
-                    }
-                    float *fv = d[0], *bv = d[1], *fi = d[2], *bi = d[3];
-                    float gradlam = 0.0, gradmu = 0.0, gradrho = 0.0;
-                    gradlam = (fv[0] + fv[4] + fv[8]) * (bv[0] + bv[4] + bv[8]) + (fi[0] + fi[4] + fi[8]) * (bi[0] + bi[4] + bi[8]);
-                    gradlam = -gradlam * fdummy;
-                    gradmu = 2 * fv[0] * bv[0] + 2 * fv[4] * bv[4] + 2 * fv[8] * bv[8] + 2 * fi[0] * bi[0] + 2 * fi[4] * bi[4] +
-                             2 * fi[8] * bi[8] + (fv[1] + fv[3]) * (bv[1] + bv[3]) + (fi[1] + fi[3]) * (bi[1] + bi[3]) +
-                             (fv[2] + fv[6]) * (bv[2] + bv[6]) + (fi[2] + fi[6]) * (bi[2] + bi[6]) +
-                             (fv[5] + fv[7]) * (bv[5] + bv[7]) + (fi[5] + fi[7]) * (bi[5] + bi[7]);
-                    gradmu = -gradmu * fdummy;
-                    size_t c = W(j, i, k), m = M(j, i, k);
-                    gradrho = (f[0][c] * bk[0][c] + f[1][c] * bk[1][c] + f[2][c] * bk[2][c]) +
-                              (f[3][c] * bk[3][c] + f[4][c] * bk[4][c] + f[5][c] * bk[5][c]);
-                    float r = rho[m], pp = pi[m], uu = u[m];
-                    grad[0 * n + m] += sqrt(r * pp) * 2 * gradlam;
-                    grad[1 * n + m] += -4 * sqrt(r * uu) * gradlam + 2 * sqrt(r * uu) * gradmu;
-                    grad[2 * n + m] += gradrho + uu / r * gradmu + (pp - 2 * uu) / r * gradlam;
-                }
+        par_rows(1, q.G.ny, grad_rows, &q);
     }
     return 0;
 }

@@ -60,7 +60,9 @@ def _f32(a):
 class Oracle:
     """One of the two CPU oracle implementations behind the same API."""
 
-    def __init__(self, kind: str = "oracle"):
+    def __init__(self, kind: str = "oracle", threads: int = 0):
+        """kind "ref" (the reference build, single-threaded) or "oracle" (the
+        restatement; its cell loops use `threads` OpenMP threads, 0 = all cores)."""
         path = REF_LIB if kind == "ref" else ORC_LIB
         if not os.path.exists(path):
             if kind == "ref" and not os.path.isdir(os.path.join(REFERENCE_SRC, "src")):
@@ -71,6 +73,10 @@ class Oracle:
         for name in ("ifo_readmod", "ifo_cpml_coeff", "ifo_wavelet", "ifo_av_mat", "ifo_forward",
                      "ifo_residual", "ifo_adjoint", "ifo_gradient", "ifo_nsamples"):
             getattr(self.lib, name).restype = C.c_int
+        if hasattr(self.lib, "ifo_set_threads"):
+            self.lib.ifo_set_threads.restype = None
+            self.lib.ifo_set_threads.argtypes = [C.c_int]
+            self.lib.ifo_set_threads(int(threads))
 
     # -- helpers ---------------------------------------------------------------
     @staticmethod
