@@ -94,6 +94,8 @@ struct ifosb_engine {
     int nt_limit = 0;
     long long captures = 0;  // time-loop graphs captured (a replay reuses one)
     float *d_mstage = nullptr;  // ifosb_set_model's staging of the raw model (5 ghosted fields)
+    float *d_smod = nullptr;    // free-surface moduli of plane j=1 [2][NX][NZ] (ifosb_set_surface_moduli)
+    bool smod_on = false;
     // approximate Hessian: receivers' Green's-function DFT fields and the accumulated diagonal
     float *d_green = nullptr; int ngreen = 0, cap_green = 0;
     float *d_gsig = nullptr;   // [max_shots][3][NT] injection traces of a Green's-function batch
@@ -334,7 +336,7 @@ extern "C" void ifosb_destroy(ifosb_engine *e) {
                     e->d_err, e->d_sec, e->d_diff, e->d_obs, e->d_part, e->d_misfit, e->d_l2, e->d_trig_f,
                     e->d_trig_b, e->d_voff, e->d_soff, e->d_vpts, e->d_spts, e->d_amp, e->d_tma_err, e->d_cpg,
                     e->d_mstage, e->d_green, e->d_gsig, e->d_hess, e->d_sec2, e->d_voff_t, e->d_soff_t,
-                    e->d_voff_a, e->d_vpts_t, e->d_spts_t, e->d_vpts_a, e->d_amp_t, e->d_gradq};
+                    e->d_voff_a, e->d_vpts_t, e->d_spts_t, e->d_vpts_a, e->d_amp_t, e->d_gradq, e->d_smod};
     for (void *b : bufs)
         if (b) cudaFree(b);
     for (cudaEvent_t ev : e->events) cudaEventDestroy(ev);
@@ -470,6 +472,39 @@ extern "C" int ifosb_set_model(ifosb_engine *e, const float *rho, const float *p
     }
     e->have_model = true;
     e->fwd_ok = e->res_ok = e->adj_ok = false;
+    return IFOSB_OK;
+}
+
+// The elastic free surface's own moduli: the reference's step-length forwards
+// propagate in the test model but call surface_elastic with the current model's
+// u and pi (src/ifos3d.c:1087-1090), which matters at the plane j = 1 only.
+extern "C" int ifosb_set_surface_moduli(ifosb_engine *e, const float *pi, const float *u) {
+    if (!e || (!pi) != (!u)) return IFOSB_EARG;
+    e->fwd_ok = e->res_ok = e->adj_ok = false;
+    if (!pi) {
+        e->smod_on = false;
+        return IFOSB_OK;
+    }
+    const ifosb_params &p = e->p;
+    if (p.nmech > 0) return fail(e, IFOSB_EARG, "separate surface moduli apply to the elastic free surface only");
+    const size_t plane = (size_t)p.nx * p.nz;
+    std::vector<float> h(2 * plane);
+    for (int i = 1; i <= p.nx; ++i)
+        for (int k = 1; k <= p.nz; ++k) {
+            const size_t gidx = ((size_t)1 * (p.nx + 2) + i) * (p.nz + 2) + k;  // [j=1][i][k] of the ghosted array
+            const size_t q = (size_t)(i - 1) * p.nz + (k - 1);
+            if (!(pi[gidx] > 0.f) || !std::isfinite(pi[gidx]) || !(u[gidx] >= 0.f) || !std::isfinite(u[gidx]))
+                return fail(e, IFOSB_EARG, "surface modulus not positive and finite");
+            h[q] = pi[gidx];
+            h[plane + q] = u[gidx];
+        }
+    if (!e->d_smod) {
+        const int rc = dalloc(e, &e->d_smod, 2 * plane);
+        if (rc) return rc;
+    }
+    CU(cudaMemcpyAsync(e->d_smod, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice, e->stream));
+    CU(cudaStreamSynchronize(e->stream));
+    e->smod_on = true;
     return IFOSB_OK;
 }
 
@@ -666,6 +701,7 @@ static void fill_common(ifosb_engine *e, Loop &L) {
     sa.sec_shot = 3 * sa.sec_comp;
     sa.nf = e->nf;
     sa.dft_shot = e->dft_shot;
+    sa.smod = e->smod_on ? e->d_smod : nullptr;
 }
 
 // cuTensorMapEncodeTiled from the driver, reached through the runtime (no libcuda link).

@@ -152,6 +152,8 @@ struct StrArgs {
     int seismo;           // SEISMO: 1 particle velocities; 2, 3, 4 add p / div, curl (sec2)
     float *sec2;          // [shot][3][ntr][ns]: p, div, curl
     float hrx, hry, hrz;  // 1.0/DX etc. in float (seismo_ssg.c:38-40)
+    const float *smod;    // elastic free surface: pi, u of plane j=1 ([2][NX][NZ]) when they
+                          // differ from the propagation model's, else null
 };
 
 // seismo (seismo_ssg.c:48-125), SEISMO 2-4: pressure from the cell's new
@@ -461,7 +463,13 @@ __global__ void __launch_bounds__(BX *BY) k_stress(StrArgs a, int nt, int do_dft
         if (g.free_surf && j == 1) {
             syy = 0.0f;
             if constexpr (L == 0) {
-                const float f = (float)((double)um * 2.0), gg = pim;
+                float spi = pim, su = um;
+                if (a.smod) {
+                    const long long q = (long long)(i - 1) * g.nz + (k - 1);
+                    spi = a.smod[q];
+                    su = a.smod[(long long)g.nx * g.nz + q];
+                }
+                const float f = (float)((double)su * 2.0), gg = spi;
                 const float h = -(DT * (gg - f) * (gg - f) * (svxx + svzz) / gg) - (DT * (gg - f) * svyy);
                 sxx += h;
                 szz += h;

@@ -549,7 +549,13 @@ __global__ void __maxnreg__(L == 0 ? STR_REGS_ELASTIC : STR_REGS_MECH) k_stress_
                 // surface_ssg_elastic.c:69-111 / surface_ssg.c:117-160
                 syy = 0.0f;
                 if constexpr (L == 0) {
-                    const float f = (float)((double)um * 2.0), gg = pim;
+                    float spi = pim, su = um;
+                    if (a.smod) {  // the surface's own moduli (the reference's step-length forwards)
+                        const long long q = (long long)(i - 1) * g.nz + (k - 1);
+                        spi = a.smod[q];
+                        su = a.smod[(long long)g.nx * g.nz + q];
+                    }
+                    const float f = (float)((double)su * 2.0), gg = spi;
                     const float h = -(DT * (gg - f) * (gg - f) * (svxx + svzz) / gg) - (DT * (gg - f) * svyy);
                     sxx += h;
                     szz += h;

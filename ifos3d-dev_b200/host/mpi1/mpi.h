@@ -1,16 +1,18 @@
 /*
- * One-rank MPI stub used ONLY to compile the reference IFOS3D sources as a
- * CPU oracle (test infrastructure; never linked into the CUDA product).
+ * One-rank MPI for the reference's host C code where no MPI library is
+ * installed: the drop-in host (ifos3d-dev_b200/host, the reference's ifos3d.c
+ * driving the B200 engine on one rank) and the CPU builds of the reference
+ * that the tests compare against.
  *
- * Semantics chosen to match a real one-rank MPI run of the reference:
+ * Semantics are those of a real one-rank MPI run:
  *  - point-to-point calls are no-ops that leave the receive buffer untouched,
  *    exactly like MPI_Recv/Sendrecv_replace from MPI_PROC_NULL (this is what
  *    makes matcopy.c wrap the model ghost layers periodically on one rank);
  *  - Allreduce copies send -> recv (sum over one rank), Bcast/Barrier are no-ops;
  *  - MPI_Wtime is clock_gettime(CLOCK_MONOTONIC).
  */
-#ifndef IFOS_ORACLE_MPI_STUB_H
-#define IFOS_ORACLE_MPI_STUB_H
+#ifndef IFOSB_ONE_RANK_MPI_H
+#define IFOSB_ONE_RANK_MPI_H
 
 #include <string.h>
 #include <stdlib.h>

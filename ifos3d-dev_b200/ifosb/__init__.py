@@ -133,6 +133,7 @@ def lib():
                                          C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float]),
             "ifosb_set_seismo": (C.c_int, [vp, C.c_int]),
             "ifosb_set_wait_test": (C.c_int, [vp, C.c_longlong, C.c_int, C.c_int]),
+            "ifosb_set_surface_moduli": (C.c_int, [vp, vp, vp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -157,6 +158,7 @@ def exported_symbols():
         "ifosb_write_model", "ifosb_write_gradient", "ifosb_filt_seis", "ifosb_hessian_green", "ifosb_hessian",
         "ifosb_zero_hessian", "ifosb_get_hessian", "ifosb_read_hessian", "ifosb_hess_apply", "ifosb_resample",
         "ifosb_set_seismo", "ifosb_gradient_td", "ifosb_get_gradient_q", "ifosb_set_wait_test",
+        "ifosb_set_surface_moduli",
     ]
 
 
@@ -290,6 +292,17 @@ class Engine:
         arrs = [w(rho), w(pi), w(u), w(taus), w(taup), _f32(eta)]
         self._keep = arrs
         self._c(lib().ifosb_set_model(self.h, *[_p(a) for a in arrs]))
+
+    def set_surface_moduli(self, pi=None, u=None, ghosted=False):
+        """Moduli of the elastic free surface at j = 1 when they differ from the
+        propagation model's (the reference's step-length forwards); None restores
+        the model's own."""
+        if pi is None:
+            self._c(lib().ifosb_set_surface_moduli(self.h, None, None))
+            return
+        w = (lambda a: _f32(a)) if ghosted else ghost_wrap
+        arrs = [w(pi), w(u)]
+        self._c(lib().ifosb_set_surface_moduli(self.h, _p(arrs[0]), _p(arrs[1])))
 
     def set_receivers(self, recpos):
         rec = np.ascontiguousarray(recpos, dtype=np.int32).reshape(-1, 3)

@@ -97,6 +97,14 @@ int ifosb_set_cpml(ifosb_engine *e, const float *coeff);
 int ifosb_set_model(ifosb_engine *e, const float *rho, const float *pi, const float *u,
                     const float *taus, const float *taup, const float *eta);
 
+/* The moduli the elastic free surface uses at j = 1, when they are not the
+ * propagation model's: the reference's step-length forwards propagate in the test
+ * model but call surface_elastic with the current model's u and pi
+ * (src/ifos3d.c:1087-1090, src/surface_ssg_elastic.c:102-103). pi, u: ghosted
+ * [NY+2][NX+2][NZ+2] arrays as for ifosb_set_model (plane j = 1 is read);
+ * NULL, NULL = the propagation model's (the default). Elastic engines only. */
+int ifosb_set_surface_moduli(ifosb_engine *e, const float *pi, const float *u);
+
 /* Receivers (recpos_loc[1..3][itr], src/ifos3d.c:197-204): recpos[ntr][3] x, y, z index. */
 int ifosb_set_receivers(ifosb_engine *e, int ntr, const int *recpos);
 

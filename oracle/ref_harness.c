@@ -2,7 +2,7 @@
  * Reference harness — TEST INFRASTRUCTURE ONLY (the CPU oracle).
  *
  * Drives the UNMODIFIED reference functions (compiled from the reference's
- * src/ by oracle/Makefile, with the one-rank MPI stub in oracle/mpi_stub)
+ * src/ by oracle/Makefile, with the one-rank MPI of ifos3d-dev_b200/host/mpi1)
  * through flat arrays, in the call order of the reference driver:
  *   forward   : src/ifos3d.c:738-814  (zero_wavefield, zero_invers, NT loop of
  *               update_v, update_v_CPML, update_s_elastic, update_s_CPML_elastic,
