@@ -31,6 +31,14 @@ constexpr int DEFAULT_CY = 8;
 struct GraphCache {
     cudaGraphExec_t exec = nullptr;
     std::vector<unsigned char> key;
+    long long used = 0;  // last use, for replacing the least recently used
+};
+// Time-loop graphs kept per direction: a run of batches alternates between a few
+// shapes (full batches and a shorter last one), and each keeps its own graph.
+constexpr int GRAPHS_PER_DIRECTION = 4;
+struct GraphSet {
+    GraphCache g[GRAPHS_PER_DIRECTION];
+    long long tick = 0;
 };
 
 struct HostPt {
@@ -77,7 +85,7 @@ struct ifosb_engine {
     int launch_mode = 0;
     long long launches = 0;
     long long dev_bytes = 0;
-    GraphCache gfwd, gadj;
+    GraphSet gfwd, gadj;
     // kernel timing
     int profile = 0;
     double t_vel_ms = 0.0, t_str_ms = 0.0;
@@ -185,6 +193,10 @@ static void release_graph(GraphCache &gc) {
     if (gc.exec) cudaGraphExecDestroy(gc.exec);
     gc.exec = nullptr;
     gc.key.clear();
+}
+
+static void release_graph(GraphSet &gs) {
+    for (GraphCache &gc : gs.g) release_graph(gc);
 }
 
 static int check_launch(ifosb_engine *e, const char *what) {
@@ -937,7 +949,7 @@ static int run_loop_profiled(ifosb_engine *e, const Loop &L) {
 }
 
 static int run_loop(ifosb_engine *e, const Loop &L) {
-    GraphCache &gc = L.back ? e->gadj : e->gfwd;
+    GraphSet &gs = L.back ? e->gadj : e->gfwd;
     e->launches = 2LL * e->p.nt;
     if (e->profile) return run_loop_profiled(e, L);
     if (e->launch_mode == 1) {
@@ -946,7 +958,15 @@ static int run_loop(ifosb_engine *e, const Loop &L) {
     }
     std::vector<unsigned char> key(sizeof(Loop));
     std::memcpy(key.data(), &L, sizeof(Loop));
-    if (!gc.exec || gc.key != key) {
+    GraphCache *hit = nullptr, *lru = &gs.g[0];
+    for (GraphCache &c : gs.g) {
+        if (c.exec && c.key == key) hit = &c;
+        if (!c.exec) { if (lru->exec) lru = &c; }
+        else if (lru->exec && c.used < lru->used) lru = &c;
+    }
+    GraphCache &gc = hit ? *hit : *lru;
+    gc.used = ++gs.tick;
+    if (!hit) {
         release_graph(gc);
         cudaGraph_t graph = nullptr;
         CU(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));

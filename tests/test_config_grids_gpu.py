@@ -11,7 +11,8 @@
 - The batched viscoelastic gradient configuration: 384 x 384 horizontal x 256
   deep cells (NX x NZ x NY), L=3, 4 frequencies, 1024 receivers, two of its
   32 shots in one batch, 12 steps: traces, DFT fields and gradient against the
-  C restatement (the reference has no L=3), bit for bit.
+  C restatement (the reference has no L=3), bit for bit. The wave does not reach
+  the receivers in 12 steps, so a seeded residual drives the adjoint.
 - The viscoelastic forward-modelling configuration (256^3, L=3, 8 layers, 400
   receivers) for 120 steps: traces and every wavefield against the restatement.
 
@@ -78,9 +79,12 @@ def test_visco384_full_grid_two_shot_batch_against_the_restatement():
     assert (p.nx, p.ny, p.nz) == (384, 256, 384)
     e, m, cp, shots = engine_for(c)
     sec = e.forward(shots)
-    obs = (sec * np.float32(0.9)).astype(np.float32)
-    e.residual(obs)
-    e.adjoint()
+    # 12 steps do not carry the wave to the receivers, so the residual of observed
+    # traces would be zero: inject a seeded residual instead (the adjoint's input
+    # either way), which the near-source forward field then correlates with
+    rng = np.random.default_rng(12)
+    diff = (1e-9 * rng.standard_normal(sec.shape)).astype(np.float32)
+    e.adjoint(diff)
     e.gradient()
     g = e.get_gradient()
     ip = ifo_params(c)
@@ -89,8 +93,7 @@ def test_visco384_full_grid_two_shot_batch_against_the_restatement():
     for s, (sp, sig) in enumerate(shots):
         f = O.forward(ip, m, cp, sp, sig, c["recpos"], c["finv"], c["ntast"], True)
         assert np.array_equal(sec[s], f["sections"]), f"traces shot {s}"
-        d, _ = O.residual(ip, obs[s], f["sections"])
-        b = O.adjoint(ip, m, cp, c["recpos"], d, c["finv"], c["ntast"])
+        b = O.adjoint(ip, m, cp, c["recpos"], diff[s], c["finv"], c["ntast"])
         # the engine's DFT fields are those of the last batch: compare before moving on
         assert np.array_equal(e.get_dft(s), f["dft"]), f"forward DFT shot {s}"
         assert np.array_equal(e.get_dft(s, back=True), b["dft"]), f"backward DFT shot {s}"

@@ -262,3 +262,18 @@ def test_time_loop_graph_is_reused():
         e.set_model(m["rho"], m["pi"], m["u"], m["taus"], m["taup"], m["eta"])
         e.shot_gradient(shots, obs)
     assert e.graph_captures == steady
+
+
+def test_alternating_batch_shapes_keep_their_graphs():
+    """Full batches and a shorter last batch alternate in a multi-batch gradient;
+    each shape keeps its own captured graph, so alternating captures nothing new."""
+    c = synth.small_case(nt=30, nshots=3, seed=31)
+    e, m, cp, shots = engine_for(c)
+    full = e.forward(shots[:2])
+    part = e.forward(shots[2:])
+    steady = e.graph_captures
+    for _ in range(3):
+        assert np.array_equal(e.forward(shots[:2]), full)
+        assert np.array_equal(e.forward(shots[2:]), part)
+    assert e.graph_captures == steady
+    e.close()
