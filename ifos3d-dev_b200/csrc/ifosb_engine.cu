@@ -9,6 +9,7 @@
 #include "../../include/ifos_b200.h"
 #include "ifosb_kernels.cuh"
 #include "ifosb_tma.cuh"
+#include "ifosb_vjp.cuh"
 
 #include <cudaTypedefs.h>
 
@@ -118,6 +119,9 @@ struct ifosb_engine {
     Pt *d_vpts_t = nullptr, *d_spts_t = nullptr, *d_vpts_a = nullptr;
     size_t cap_vpts_t = 0, cap_spts_t = 0, cap_vpts_a = 0;
     float *d_amp_t = nullptr; size_t cap_amp_t = 0;
+    // time-domain mode's checkpoint/segment block and kernels, kept between calls
+    float *d_td_blk = nullptr; size_t cap_td_blk = 0;
+    double *d_td_k = nullptr; size_t cap_td_k = 0;
     // TMA staging (default) and its wait-timeout flag; the failure-path test knobs
     int use_tma = 1;
     int *d_tma_err = nullptr;
@@ -348,7 +352,8 @@ extern "C" void ifosb_destroy(ifosb_engine *e) {
                     e->d_err, e->d_sec, e->d_diff, e->d_obs, e->d_part, e->d_misfit, e->d_l2, e->d_trig_f,
                     e->d_trig_b, e->d_voff, e->d_soff, e->d_vpts, e->d_spts, e->d_amp, e->d_tma_err, e->d_cpg,
                     e->d_mstage, e->d_green, e->d_gsig, e->d_hess, e->d_sec2, e->d_voff_t, e->d_soff_t,
-                    e->d_voff_a, e->d_vpts_t, e->d_spts_t, e->d_vpts_a, e->d_amp_t, e->d_gradq, e->d_smod};
+                    e->d_voff_a, e->d_vpts_t, e->d_spts_t, e->d_vpts_a, e->d_amp_t, e->d_gradq, e->d_smod,
+                    e->d_td_blk, e->d_td_k};
     for (void *b : bufs)
         if (b) cudaFree(b);
     for (cudaEvent_t ev : e->events) cudaEventDestroy(ev);
@@ -1236,7 +1241,6 @@ extern "C" int ifosb_gradient_td(ifosb_engine *e, int interval, double *kernels)
     if (!e || !kernels || interval < 1) return IFOSB_EARG;
     const ifosb_params &p = e->p;
     if (!e->fwd_ok || !e->res_ok) return fail(e, IFOSB_ESTATE, "the time-domain gradient needs a forward batch and its residual");
-    if (p.nmech != 0) return fail(e, IFOSB_EARG, "the time-domain gradient is elastic (nmech 0)");
     if (p.ndt != 1 || p.ndtshift != 0) return fail(e, IFOSB_EARG, "the adjoint indexes the residual by step: NDT=1, NDTSHIFT=0");
     // The adjoint's step m stands at time TIME - m DT (discfourier's backward phase), so
     // forward step n meets it at zero lag when n + m = P = TIME / DT (nearest whole step).
@@ -1253,14 +1257,12 @@ extern "C" int ifosb_gradient_td(ifosb_engine *e, int interval, double *kernels)
     const size_t seg_shot = (size_t)6 * F;    // one step of a segment: v and running sums
     // one device block: state2 | psi2 | Uf | Ub | Uf(NT) | checkpoints 1..nseg-1 | segment
     const size_t total = ss + ps + 3 * us + (size_t)(nseg - 1) * ck + (size_t)K * seg_shot * nshots;
-    float *blk = nullptr;
-    double *dk = nullptr;
-    CU(cudaMalloc(&blk, total * sizeof(float)));
-    cudaError_t ce = cudaMalloc(&dk, (size_t)4 * n * sizeof(double));
-    if (ce != cudaSuccess) {
-        cudaFree(blk);
-        CU(ce);
-    }
+    // grow-only blocks kept by the engine: a repeated call allocates nothing
+    int grc;
+    if ((grc = dgrow(e, &e->d_td_blk, &e->cap_td_blk, total)) || (grc = dgrow(e, &e->d_td_k, &e->cap_td_k, (size_t)4 * n)))
+        return grc;
+    float *blk = e->d_td_blk;
+    double *dk = e->d_td_k;
     float *st2 = blk, *psi2 = st2 + ss, *uf = psi2 + ps, *ub = uf + us, *uf_end = ub + us, *ckp = uf_end + us;
     float *segb = ckp + (size_t)(nseg - 1) * ck;
     int rc = IFOSB_OK;
@@ -1320,8 +1322,9 @@ extern "C" int ifosb_gradient_td(ifosb_engine *e, int interval, double *kernels)
         La.tma = e->use_tma && setup_tma(e, La, nullptr);
         const int nb = 2 * 148, tb = 256;
         const dim3 grd_c((p.nz + BX - 1) / BX, (p.nx + BY - 1) / BY, p.ny);
-        auto integrate = [&](float *u, const float *st) {
-            k_td_integrate<<<dim3(nb, nshots), tb, 0, e->stream>>>(u, st, e->st_shot, F, nshots, p.dt);
+        auto integrate = [&](float *u, const float *st, float *seg) {
+            k_td_integrate<<<dim3(nb, nshots), tb, 0, e->stream>>>(u, st, e->st_shot, F, nshots, p.dt, seg,
+                                                                   (long long)seg_shot);
         };
         // 1. the forward again, saving a checkpoint after steps K, 2K, ... and the sums at NT
         CU(cudaMemsetAsync(st2, 0, ss * sizeof(float), e->stream));
@@ -1335,7 +1338,7 @@ extern "C" int ifosb_gradient_td(ifosb_engine *e, int interval, double *kernels)
         }
         for (int nt = 1; nt <= NT; ++nt) {
             td_step(e, Lf, nt);
-            integrate(uf, st2);
+            integrate(uf, st2, nullptr);
             if (nt % K == 0 && nt / K < nseg) {
                 float *c = ckp + (size_t)(nt / K - 1) * ck;
                 CU(cudaMemcpyAsync(c, st2, ss * sizeof(float), cudaMemcpyDeviceToDevice, e->stream));
@@ -1372,21 +1375,13 @@ extern "C" int ifosb_gradient_td(ifosb_engine *e, int interval, double *kernels)
                 CU(cudaMemcpyAsync(psi2, c + ss, ps * sizeof(float), cudaMemcpyDeviceToDevice, e->stream));
                 CU(cudaMemcpyAsync(uf, c + ss + ps, us * sizeof(float), cudaMemcpyDeviceToDevice, e->stream));
             }
-            for (int m = a0; m <= a1; ++m) {
+            for (int m = a0; m <= a1; ++m) {  // v and U of each step go to the segment in the same pass
                 td_step(e, Lf, m);
-                integrate(uf, st2);
-                float *slot = segb + (size_t)(m - a0) * seg_shot * nshots;
-                for (int sh = 0; sh < nshots; ++sh) {
-                    float *d = slot + (size_t)sh * seg_shot;
-                    CU(cudaMemcpyAsync(d, st2 + (size_t)sh * e->st_shot, 3 * F * sizeof(float), cudaMemcpyDeviceToDevice,
-                                       e->stream));
-                    CU(cudaMemcpyAsync(d + 3 * F, uf + (size_t)sh * 3 * F, 3 * F * sizeof(float),
-                                       cudaMemcpyDeviceToDevice, e->stream));
-                }
+                integrate(uf, st2, segb + (size_t)(m - a0) * seg_shot * nshots);
             }
             for (int m = a1; m >= a0; --m, ++ntb) {  // adjoint steps P-a1 .. P-a0, in order
                 td_step(e, La, ntb);
-                integrate(ub, e->d_state);
+                integrate(ub, e->d_state, nullptr);
                 ta.seg = segb + (size_t)(m - a0) * seg_shot * nshots;
                 k_td_corr<<<grd_c, dim3(BX, BY), 0, e->stream>>>(ta);
             }
@@ -1394,7 +1389,7 @@ extern "C" int ifosb_gradient_td(ifosb_engine *e, int interval, double *kernels)
         }
         for (; ntb <= NT; ++ntb) {  // adjoint steps past P-1 meet forward steps before the first (zero)
             td_step(e, La, ntb);
-            integrate(ub, e->d_state);
+            integrate(ub, e->d_state, nullptr);
         }
         k_td_dc<<<nb, tb, 0, e->stream>>>(ta, uf_end);
         if ((r = check_launch(e, "time-domain kernels"))) return r;
@@ -1405,8 +1400,220 @@ extern "C" int ifosb_gradient_td(ifosb_engine *e, int interval, double *kernels)
     };
     rc = run();
     cudaStreamSynchronize(e->stream);
+    return rc;
+}
+
+// ---------------------------------------------------------------------------
+// Exact discrete VJP (ifosb_vjp.cuh): the FP64 forward of each shot of the last
+// batch with a checkpoint every `interval` steps, the misfit and its adjoint
+// source from the residual's observed traces, then the transposed steps in
+// reverse, each segment of forward states recomputed from its checkpoint.
+extern "C" int ifosb_vjp_exact(ifosb_engine *e, int interval, double *grad, double *misfit) {
+    if (!e || !misfit || interval < 1) return IFOSB_EARG;
+    const ifosb_params &p = e->p;
+    if (!e->fwd_ok || !e->res_ok) return fail(e, IFOSB_ESTATE, "the exact VJP needs a forward batch and its residual");
+    if (p.nmech != 0) return fail(e, IFOSB_EARG, "the exact VJP is elastic (nmech 0)");
+    if (p.ndt != 1 || p.ndtshift != 0) return fail(e, IFOSB_EARG, "the exact VJP samples every step: NDT=1, NDTSHIFT=0");
+    if (!e->td_vp.empty()) return fail(e, IFOSB_EARG, "the exact VJP takes explosive sources only");
+    const Geo g = e->g;
+    const int NT = p.nt, ns = e->ns, ntr = e->ntr, nshots = e->nshots;
+    if (ntr < 1) return fail(e, IFOSB_ESTATE, "the exact VJP needs receivers");
+    const int K = std::min(interval, NT), nseg = (NT + K - 1) / K;
+    const long long F = g.field, n = (long long)p.nx * p.ny * p.nz;
+    const size_t SZ = (size_t)NEL * F + (size_t)e->psi_shot;  // one FP64 state: fields, then PML memory
+    const size_t ntrace = (size_t)3 * ntr * ns;
+    // device block: model | checkpoints | segment | adjoint state | ld | ls | gradients | traces | source
+    const size_t total = (size_t)N64 * F + (size_t)nseg * SZ + (size_t)(K + 1) * SZ + SZ + 18 * (size_t)F +
+                         (size_t)N64 * n + 2 * ntrace;
+    double *blk = nullptr;
+    int *ibuf = nullptr;
+    double *damp = nullptr;
+    CU(cudaMalloc(&blk, total * sizeof(double)));
+    double *md = blk, *ck = md + (size_t)N64 * F, *seg = ck + (size_t)nseg * SZ, *lam = seg + (size_t)(K + 1) * SZ;
+    double *ld = lam + SZ, *ls = ld + 9 * (size_t)F, *gq = ls + 9 * (size_t)F, *tr = gq + (size_t)N64 * n;
+    double *asrc = tr + ntrace;
+    int rc = IFOSB_OK;
+    auto run = [&]() -> int {
+        CU(cudaMemsetAsync(blk, 0, total * sizeof(double), e->stream));
+        const size_t ng = (size_t)(p.nx + 2) * (p.ny + 2) * (p.nz + 2);
+        const float *raw = e->d_mstage;  // rho, pi, u as ifosb_set_model received them (ghosted)
+        const dim3 blk3(128), grd3((p.nz + 127) / 128, p.nx, p.ny);
+        k64_model<<<grd3, blk3, 0, e->stream>>>(g, raw, raw + ng, raw + 2 * ng, md);
+        Vjp64 a{};
+        a.g = g;
+        a.sl = e->sl;
+        a.md = md;
+        a.cpg = e->d_cpg;
+        a.b1 = e->b1; a.b2 = e->b2;
+        a.dx = (double)p.dt / p.dx; a.dy = (double)p.dt / p.dy; a.dz = (double)p.dt / p.dz;
+        a.rdx = p.dx; a.rdy = p.dy; a.rdz = p.dz; a.dt = p.dt;
+        a.nt_total = NT;
+        Grad64 gr;
+        for (int q = 0; q < N64; ++q) gr.q[q] = gq + (size_t)q * n;
+        std::vector<int> rec(e->rec.begin(), e->rec.end());
+        std::vector<float> obs((size_t)nshots * ntrace);
+        CU(cudaMemcpyAsync(obs.data(), e->d_obs, obs.size() * sizeof(float), cudaMemcpyDeviceToHost, e->stream));
+        CU(cudaStreamSynchronize(e->stream));
+        std::vector<double> trh(ntrace), src(ntrace);
+        const double DT = p.dt;
+        for (int sh = 0; sh < nshots; ++sh) {
+            // explosive sources of this shot: cell and psource amplitude row
+            std::vector<int> cells;
+            std::vector<double> amps;
+            for (const HostPt &pt : e->td_sp)
+                if (pt.s == sh && pt.kind == PT_EXPLOSIVE) {
+                    cells.insert(cells.end(), {pt.j, pt.i, pt.k});
+                    for (int t = 0; t < NT; ++t) amps.push_back(e->td_amp[(size_t)pt.row * NT + t]);
+                }
+            const int nsrc = (int)cells.size() / 3;
+            if (ibuf) cudaFree(ibuf);
+            if (damp) cudaFree(damp);
+            ibuf = nullptr;
+            damp = nullptr;
+            CU(cudaMalloc(&ibuf, sizeof(int) * (3 * (size_t)ntr + 3 * (size_t)std::max(nsrc, 1))));
+            CU(cudaMalloc(&damp, sizeof(double) * std::max<size_t>(amps.size(), 1)));
+            int *drec = ibuf, *dsrc = ibuf + 3 * ntr;
+            CU(cudaMemcpyAsync(drec, rec.data(), sizeof(int) * 3 * ntr, cudaMemcpyHostToDevice, e->stream));
+            if (nsrc) {
+                CU(cudaMemcpyAsync(dsrc, cells.data(), sizeof(int) * cells.size(), cudaMemcpyHostToDevice, e->stream));
+                CU(cudaMemcpyAsync(damp, amps.data(), sizeof(double) * amps.size(), cudaMemcpyHostToDevice, e->stream));
+            }
+            a.nsrc = nsrc;
+            a.src = dsrc;
+            a.amp = damp;
+            auto step = [&](double *st, int nt) {
+                double *ps = st + (size_t)NEL * F;
+                k64_vel<<<grd3, blk3, 0, e->stream>>>(a, st, ps);
+                k64_str<<<grd3, blk3, 0, e->stream>>>(a, st, ps, nt);
+            };
+            // 1. the forward from rest, checkpoints after steps 0, K, 2K, ..., the traces
+            double *w = seg;
+            CU(cudaMemsetAsync(w, 0, SZ * sizeof(double), e->stream));
+            CU(cudaMemsetAsync(ck, 0, SZ * sizeof(double), e->stream));
+            for (int nt = 1; nt <= NT; ++nt) {
+                step(w, nt);
+                k64_sample<<<(ntr + 127) / 128, 128, 0, e->stream>>>(g, w, drec, ntr, ns, nt - 1, tr);
+                if (nt % K == 0 && nt / K < nseg)
+                    CU(cudaMemcpyAsync(ck + (size_t)(nt / K) * SZ, w, SZ * sizeof(double), cudaMemcpyDeviceToDevice,
+                                       e->stream));
+            }
+            int r;
+            if ((r = check_launch(e, "exact VJP forward"))) return r;
+            CU(cudaMemcpyAsync(trh.data(), tr, ntrace * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+            CU(cudaStreamSynchronize(e->stream));
+            // 2. the misfit sum D^2, D = DT cumsum(syn - obs), and its derivative
+            //    2 DT sum_{n >= k} D[n] with respect to each sample
+            double J = 0.0;
+            const float *ob = obs.data() + (size_t)sh * ntrace;
+            for (size_t t = 0; t < (size_t)3 * ntr; ++t) {
+                const double *sy = trh.data() + t * ns;
+                const float *o = ob + t * ns;
+                std::vector<double> D(ns);
+                double run_sum = 0.0;
+                for (int k = 0; k < ns; ++k) {
+                    run_sum += sy[k] - (double)o[k];
+                    D[k] = DT * run_sum;
+                    J += D[k] * D[k];
+                }
+                double tail = 0.0;
+                for (int k = ns - 1; k >= 0; --k) {
+                    tail += D[k];
+                    src[t * ns + k] = 2.0 * DT * tail;
+                }
+            }
+            misfit[sh] = J;
+            if (!grad) continue;
+            CU(cudaMemcpyAsync(asrc, src.data(), ntrace * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+            // 3. the transposed steps, last to first, each segment recomputed from its checkpoint
+            CU(cudaMemsetAsync(lam, 0, SZ * sizeof(double), e->stream));
+            CU(cudaMemsetAsync(ld, 0, 18 * (size_t)F * sizeof(double), e->stream));
+            double *lps = lam + (size_t)NEL * F;
+            const dim3 grdg((p.nz + 127) / 128, p.nx, p.ny + (g.free_surf ? 2 : 0));
+            const dim3 grds((p.nz + 127) / 128, p.nx);
+            for (int q = nseg - 1; q >= 0; --q) {
+                const int a0 = q * K + 1, a1 = std::min((q + 1) * K, NT);
+                CU(cudaMemcpyAsync(seg, ck + (size_t)q * SZ, SZ * sizeof(double), cudaMemcpyDeviceToDevice, e->stream));
+                for (int nt = a0; nt <= a1; ++nt) {
+                    double *cur = seg + (size_t)(nt - a0 + 1) * SZ;
+                    CU(cudaMemcpyAsync(cur, cur - SZ, SZ * sizeof(double), cudaMemcpyDeviceToDevice, e->stream));
+                    step(cur, nt);
+                }
+                for (int nt = a1; nt >= a0; --nt) {
+                    const double *cur = seg + (size_t)(nt - a0 + 1) * SZ, *prev = cur - SZ;
+                    k64_inject<<<(ntr + 127) / 128, 128, 0, e->stream>>>(g, lam, drec, ntr, ns, nt - 1, asrc);
+                    if (g.free_surf) k64_mirror_T<<<grds, blk3, 0, e->stream>>>(g, lam);
+                    k64_str_T<<<grd3, blk3, 0, e->stream>>>(a, lam, lps, ld, cur, prev + (size_t)NEL * F, gr);
+                    k64_str_T_gather<<<grd3, blk3, 0, e->stream>>>(a, lam, ld);
+                    k64_vel_T<<<grd3, blk3, 0, e->stream>>>(a, lam, lps, ls, cur, prev, gr);
+                    k64_vel_T_gather<<<grdg, blk3, 0, e->stream>>>(a, lam, ls, g.free_surf ? -1 : 1);
+                }
+                if ((r = check_launch(e, "exact VJP adjoint"))) return r;
+            }
+        }
+        if (!grad) return IFOSB_OK;
+        // 4. the averaged moduli's gradients onto the raw model (av_mat.c:45-69 and
+        //    matcopy's periodic ghost layers), then onto vp, vs, rho
+        std::vector<double> gh((size_t)N64 * n);
+        std::vector<float> rawh(3 * ng);
+        CU(cudaMemcpyAsync(gh.data(), gq, gh.size() * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+        CU(cudaMemcpyAsync(rawh.data(), raw, rawh.size() * sizeof(float), cudaMemcpyDeviceToHost, e->stream));
+        CU(cudaStreamSynchronize(e->stream));
+        const int NX = p.nx, NY = p.ny, NZ = p.nz, GX = NX + 2, GZ = NZ + 2;
+        auto G = [&](int j, int i, int k) { return ((size_t)j * GX + i) * GZ + k; };
+        const float *rho = rawh.data(), *pi = rho + ng, *u = pi + ng;
+        std::vector<double> dr(ng, 0.0), dp(ng, 0.0), du(ng, 0.0);
+        auto harm = [&](double gval, int j0, int i0, int k0, int j1, int i1, int k1, int j2, int i2, int k2, int j3,
+                        int i3, int k3) {
+            const size_t c[4] = {G(j0, i0, k0), G(j1, i1, k1), G(j2, i2, k2), G(j3, i3, k3)};
+            double s = 0.0;
+            for (size_t q : c) s += 1.0 / (double)u[q];
+            const double avg = 4.0 / s;
+            for (size_t q : c) du[q] += gval * avg * avg / (4.0 * (double)u[q] * (double)u[q]);
+        };
+        for (int j = 1; j <= NY; ++j)
+            for (int i = 1; i <= NX; ++i)
+                for (int k = 1; k <= NZ; ++k) {
+                    const size_t m = ((size_t)(j - 1) * NX + (i - 1)) * NZ + (k - 1), c = G(j, i, k);
+                    auto gv = [&](int q) { return gh[(size_t)q * n + m]; };
+                    dp[c] += gv(M64_PI);
+                    du[c] += gv(M64_U);
+                    dr[c] += 0.5 * gv(M64_RIP); dr[G(j, i + 1, k)] += 0.5 * gv(M64_RIP);
+                    dr[c] += 0.5 * gv(M64_RJP); dr[G(j + 1, i, k)] += 0.5 * gv(M64_RJP);
+                    dr[c] += 0.5 * gv(M64_RKP); dr[G(j, i, k + 1)] += 0.5 * gv(M64_RKP);
+                    harm(gv(M64_UIPJP), j, i, k, j, i + 1, k, j + 1, i + 1, k, j + 1, i, k);
+                    harm(gv(M64_UJPKP), j, i, k, j, i, k + 1, j + 1, i, k + 1, j + 1, i, k);
+                    harm(gv(M64_UIPKP), j, i, k, j, i, k + 1, j, i + 1, k + 1, j, i + 1, k);
+                }
+        // fold the ghost layers (matcopy on one rank: index 0 = N, N + 1 = 1)
+        auto wrapi = [](int x, int N) { return x == 0 ? N : (x == N + 1 ? 1 : x); };
+        std::vector<double> fr(n, 0.0), fp(n, 0.0), fu(n, 0.0);
+        for (int j = 0; j <= NY + 1; ++j)
+            for (int i = 0; i <= NX + 1; ++i)
+                for (int k = 0; k <= NZ + 1; ++k) {
+                    const size_t c = G(j, i, k);
+                    if (dr[c] == 0.0 && dp[c] == 0.0 && du[c] == 0.0) continue;
+                    const size_t m = ((size_t)(wrapi(j, NY) - 1) * NX + (wrapi(i, NX) - 1)) * NZ + (wrapi(k, NZ) - 1);
+                    fr[m] += dr[c];
+                    fp[m] += dp[c];
+                    fu[m] += du[c];
+                }
+        // pi = rho vp^2, u = rho vs^2 (readmod.c with L = 0)
+        for (int j = 1; j <= NY; ++j)
+            for (int i = 1; i <= NX; ++i)
+                for (int k = 1; k <= NZ; ++k) {
+                    const size_t m = ((size_t)(j - 1) * NX + (i - 1)) * NZ + (k - 1), c = G(j, i, k);
+                    const double r = rho[c], vp = std::sqrt((double)pi[c] / r), vs = std::sqrt((double)u[c] / r);
+                    grad[m] = fp[m] * 2.0 * r * vp;
+                    grad[n + m] = fu[m] * 2.0 * r * vs;
+                    grad[2 * n + m] = fr[m] + fp[m] * vp * vp + fu[m] * vs * vs;
+                }
+        return IFOSB_OK;
+    };
+    rc = run();
+    cudaStreamSynchronize(e->stream);
     cudaFree(blk);
-    cudaFree(dk);
+    if (ibuf) cudaFree(ibuf);
+    if (damp) cudaFree(damp);
     return rc;
 }
 

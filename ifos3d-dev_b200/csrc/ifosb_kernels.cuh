@@ -776,13 +776,18 @@ __global__ void k_td_dc(TdArgs a, const float *uf_end) {
 
 // U += v * DT over the three velocity fields (whole padded fields) of shot
 // blockIdx.y, four floats at a time (a field is a multiple of 8 floats and every
-// base is 16-byte aligned), each component as the scalar u + v * dt.
-__global__ void k_td_integrate(float *u, const float *st, long long st_shot, long long F, int nshots, float dt) {
+// base is 16-byte aligned), each component as the scalar u + v * dt. With seg
+// set, the step's v and new U also go to the shot's segment slot
+// (seg + s * seg_shot: [v 3F][U 3F]), in the same pass.
+__global__ void k_td_integrate(float *u, const float *st, long long st_shot, long long F, int nshots, float dt,
+                               float *seg, long long seg_shot) {
     const int s = blockIdx.y;
     if (s >= nshots) return;
     const long long n4 = 3 * F / 4;
     float4 *U = reinterpret_cast<float4 *>(u + (long long)s * 3 * F);
     const float4 *S = reinterpret_cast<const float4 *>(st + (long long)s * st_shot);
+    float4 *SV = seg ? reinterpret_cast<float4 *>(seg + (long long)s * seg_shot) : nullptr;
+    float4 *SU = seg ? SV + n4 : nullptr;
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n4; q += (long long)gridDim.x * blockDim.x) {
         float4 x = U[q];
         const float4 v = S[q];
@@ -791,6 +796,10 @@ __global__ void k_td_integrate(float *u, const float *st, long long st_shot, lon
         x.z += v.z * dt;
         x.w += v.w * dt;
         U[q] = x;
+        if (SV) {
+            SV[q] = v;
+            SU[q] = x;
+        }
     }
 }
 

@@ -151,7 +151,9 @@ int ifosb_gradient(ifosb_engine *e);
  * the running sum of v DT and e the gradient_F stencils of U; dc  U_f(NT) . U_b(NT).
  * With frequencies f_l = l / (2 NT DT) the rho kernel equals (by Parseval)
  * (dc + 2 sum_{l=1}^{NT-1} gradrho_l + gradrho_NT) / (2 NT DT^2), gradrho_l being
- * gradient_F's rho term. Elastic (NMECH 0), NDT 1, NDTSHIFT 0. Device memory:
+ * gradient_F's rho term. Elastic or viscoelastic (the checkpoints carry the memory
+ * variables with the rest of the state; the kernels are the same correlations that
+ * gradient_F forms at its frequencies), NDT 1, NDTSHIFT 0. Device memory:
  * ceil((TIME/DT - 1)/interval) checkpoints of the batch state plus `interval` steps
  * of six fields per shot. The DFT fields, traces and residual stay as they were;
  * the wavefield state (ifosb_get_field) is the time-domain adjoint's last step. */
@@ -169,6 +171,23 @@ int ifosb_gradient_td(ifosb_engine *e, int interval, double *kernels);
  * with gradient_F's sign (minus the misfit gradient). With tau proportional to
  * 1/Q (the tau method), d/dQ = -(taup d/dtaup + taus d/dtaus) / Q. */
 int ifosb_get_gradient_q(ifosb_engine *e, double *gradq);
+
+/* The exact discrete vector-Jacobian product of the misfit (no counterpart in the
+ * reference, whose gradient_F correlates a back-propagation with the forward operator,
+ * src/ifos3d.c:882-975 — an approximation of the derivative). For each shot of the last
+ * forward batch: the elastic time loop in FP64 (the engine's expressions without float
+ * rounding) with a checkpoint every `interval` steps; the misfit
+ * misfit[s] = sum D^2, D = DT * cumsum(syn - obs) over every trace of the shot (the
+ * residual of residual.c:35-60; obs are the last ifosb_residual's observed traces); then
+ * the transposed time steps in reverse — the CPML memory recursions, the free-surface
+ * update and its image rows, the stress and velocity stencils — each segment of forward
+ * states recomputed from its checkpoint. grad (optional, [3][NY][NX][NZ] FP64): the
+ * derivative of the batch's summed misfit with respect to vp, vs, rho of each interior
+ * cell, through av_mat's averages (src/av_mat.c:45-69), the model's ghost layers taken
+ * as matcopy's periodic copies on one rank, and pi = rho vp^2, u = rho vs^2. NULL grad:
+ * the misfits only. Elastic engines, explosive sources, NDT 1, NDTSHIFT 0. Device
+ * memory: ceil(NT/interval) + interval + 2 FP64 states of one shot. */
+int ifosb_vjp_exact(ifosb_engine *e, int interval, double *grad, double *misfit);
 
 /* Zero the accumulated gradients (zero_grad, src/zero_grad.c). */
 int ifosb_zero_gradient(ifosb_engine *e);

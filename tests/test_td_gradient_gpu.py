@@ -18,7 +18,9 @@
    wavefields instead: the oracle run for NT' = 1..NT steps gives the state after
    each step, and the restatement, in the engine's arithmetic order, must
    reproduce the kernels to FP64 rounding.
-3. The checkpoint interval changes no bit of any kernel."""
+3. The checkpoint interval changes no bit of any kernel.
+Elastic and viscoelastic (L = 3: the checkpoints carry the memory variables
+with the rest of the state)."""
 import numpy as np
 import pytest
 
@@ -50,8 +52,9 @@ def dft_rho_sum(e, shots, obs, freqs, p):
     return rho_sum
 
 
-def test_time_domain_rho_kernel_is_the_dense_dft_sum():
-    c = synth.small_case(nx=22, ny=20, nz=18, nt=40, fw=4, nmech=0, nshots=2, seed=11, free_surf=1)
+@pytest.mark.parametrize("nmech", [0, 3])
+def test_time_domain_rho_kernel_is_the_dense_dft_sum(nmech):
+    c = synth.small_case(nx=22, ny=20, nz=18, nt=40, fw=4, nmech=nmech, nshots=2, seed=11, free_surf=1)
     p = c["params"]
     NT = p.nt
     assert round(float(p.time) / float(p.dt)) == NT - 1  # TIME = (NT-1) DT
@@ -116,9 +119,9 @@ def dot3(a, b, p):
             interior(a[2], p).astype(np.float64) * interior(b[2], p))
 
 
-@pytest.mark.parametrize("free_surf,interval", [(1, 3), (0, 5)])
-def test_time_domain_kernels_match_oracle_restatement(oracle, free_surf, interval):
-    c = synth.small_case(nx=16, ny=15, nz=14, nt=18, fw=3, nmech=0, nshots=1, seed=23 + free_surf,
+@pytest.mark.parametrize("free_surf,interval,nmech", [(1, 3, 0), (0, 5, 0), (1, 4, 3)])
+def test_time_domain_kernels_match_oracle_restatement(oracle, free_surf, interval, nmech):
+    c = synth.small_case(nx=16, ny=15, nz=14, nt=18, fw=3, nmech=nmech, nshots=1, seed=23 + free_surf,
                          free_surf=free_surf, stype=3)  # a y-force: its amplitudes do not depend on NT
     p = c["params"]
     NT, P = p.nt, p.nt - 1
@@ -165,13 +168,6 @@ def test_time_domain_kernels_match_oracle_restatement(oracle, free_surf, interva
 
 
 def test_time_domain_preconditions():
-    cv = synth.small_case(nx=20, ny=18, nz=20, nt=30, fw=4, nmech=1, nshots=1, seed=3)
-    e, m, cp, shots = engine_for(cv)
-    syn = e.forward(shots)
-    e.residual(syn * 0.5)
-    with pytest.raises(ifosb.IfosbError):
-        e.gradient_td(5)  # viscoelastic: not built
-    e.close()
     c = synth.small_case(nx=20, ny=18, nz=20, nt=30, fw=4, nmech=0, nshots=1, seed=3)
     e, m, cp, shots = engine_for(c)
     with pytest.raises(ifosb.IfosbError):
