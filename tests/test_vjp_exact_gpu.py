@@ -163,3 +163,56 @@ def test_exact_vjp_preconditions():
     g, mis = e.vjp_exact(4)
     assert np.abs(g).max() > 0 and mis[0] > 0
     e.close()
+
+
+def test_exact_vjp_on_the_adjoint_check_configuration():
+    """The adjoint-gradient configuration at its own size: 192 x 192 x 160 cells,
+    the Gaussian random-field model (+-3 %, correlation length 8 cells) for the
+    observed data, its smooth depth-gradient background as the model, 4 shots, 64
+    surface receivers, free surface and CPML; centred differences of the GPU's FP32
+    misfit along 8 seeded directions (eps = 1e-3, vp, vs, rho mixed) against the
+    exact VJP, within 1e-3 each."""
+    c = synth.case("elastic192", nt=600)
+    p = c["params"]
+    m_true, cp, shots = synth.build_inputs(c, "true")
+    e = ifosb.Engine(p, max_shots=len(shots), max_nf=0)
+    e.set_cpml(cp)
+    e.set_receivers(c["recpos"])
+    e.set_frequencies(None, 1)
+    shape = (p.ny, p.nx, p.nz)
+
+    def mods_of(vp, vs, rho):
+        m = ifosb.moduli(p, vp.ravel(), vs.ravel(), rho.ravel())
+        return tuple(m[k].reshape(shape) for k in ("rho", "pi", "u"))
+
+    e.set_model(*mods_of(*c["true"]), None, None, None)
+    obs = e.forward(shots)
+    start = c["start"]
+
+    def gpu_misfit(model):
+        e.set_model(*mods_of(*model), None, None, None)
+        e.forward(shots, want_sections=False)
+        return float(e.residual(obs).sum())
+
+    j0 = gpu_misfit(start)
+    g, mis = e.vjp_exact(40)
+    assert abs(mis[:len(shots)].sum() / j0 - 1) < 1e-5
+    rng = np.random.default_rng(5)
+    worst = 0.0
+    for _ in range(8):
+        w = rng.uniform(-1, 1, 3)
+        f = synth._gauss_field(shape, 8.0, rng).astype(np.float64)
+        plus, minus, half = [], [], []
+        for a, wi in zip(start, w):
+            a64 = a.astype(np.float64)
+            plus.append((a64 * (1 + 1e-3 * wi * f)).astype(np.float32))
+            minus.append((a64 * (1 - 1e-3 * wi * f)).astype(np.float32))
+            half.append((plus[-1].astype(np.float64) - minus[-1].astype(np.float64)) / 2)
+        fd = (gpu_misfit(plus) - gpu_misfit(minus)) / 2
+        dot = sum(float((gq * hq).sum()) for gq, hq in zip(g, half))
+        rel = abs(dot - fd) / abs(fd)
+        worst = max(worst, rel)
+        print(f"config-3 grid: <g,d> {dot:.6e} FD {fd:.6e} rel {rel:.2e}")
+        assert rel <= 1e-3
+    print(f"config-3 grid: worst relative difference {worst:.2e}")
+    e.close()
