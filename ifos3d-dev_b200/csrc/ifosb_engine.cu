@@ -1407,12 +1407,14 @@ extern "C" int ifosb_gradient_td(ifosb_engine *e, int interval, double *kernels)
 // Exact discrete VJP (ifosb_vjp.cuh): the FP64 forward of each shot of the last
 // batch with a checkpoint every `interval` steps, the misfit and its adjoint
 // source from the residual's observed traces, then the transposed steps in
-// reverse, each segment of forward states recomputed from its checkpoint.
-extern "C" int ifosb_vjp_exact(ifosb_engine *e, int interval, double *grad, double *misfit) {
+// reverse, each segment of forward states recomputed from its checkpoint. The
+// gradient comes out with respect to the raw model ifosb_set_model received,
+// interior cells, [5][NY*NX*NZ]: rho, pi, u, taus, taup (the last two zero for
+// L = 0).
+static int vjp_exact_moduli(ifosb_engine *e, int interval, double *gmod, double *misfit) {
     if (!e || !misfit || interval < 1) return IFOSB_EARG;
     const ifosb_params &p = e->p;
     if (!e->fwd_ok || !e->res_ok) return fail(e, IFOSB_ESTATE, "the exact VJP needs a forward batch and its residual");
-    if (p.nmech != 0) return fail(e, IFOSB_EARG, "the exact VJP is elastic (nmech 0)");
     if (p.ndt != 1 || p.ndtshift != 0) return fail(e, IFOSB_EARG, "the exact VJP samples every step: NDT=1, NDTSHIFT=0");
     if (!e->td_vp.empty()) return fail(e, IFOSB_EARG, "the exact VJP takes explosive sources only");
     const Geo g = e->g;
@@ -1420,7 +1422,8 @@ extern "C" int ifosb_vjp_exact(ifosb_engine *e, int interval, double *grad, doub
     if (ntr < 1) return fail(e, IFOSB_ESTATE, "the exact VJP needs receivers");
     const int K = std::min(interval, NT), nseg = (NT + K - 1) / K;
     const long long F = g.field, n = (long long)p.nx * p.ny * p.nz;
-    const size_t SZ = (size_t)NEL * F + (size_t)e->psi_shot;  // one FP64 state: fields, then PML memory
+    const int L = p.nmech, NELV = NEL + 6 * L;                       // fields, then L x 6 memory variables
+    const size_t SZ = (size_t)NELV * F + (size_t)e->psi_shot;  // one FP64 state: those, then PML memory
     const size_t ntrace = (size_t)3 * ntr * ns;
     // device block: model | checkpoints | segment | adjoint state | ld | ls | gradients | traces | source
     const size_t total = (size_t)N64 * F + (size_t)nseg * SZ + (size_t)(K + 1) * SZ + SZ + 18 * (size_t)F +
@@ -1436,9 +1439,10 @@ extern "C" int ifosb_vjp_exact(ifosb_engine *e, int interval, double *grad, doub
     auto run = [&]() -> int {
         CU(cudaMemsetAsync(blk, 0, total * sizeof(double), e->stream));
         const size_t ng = (size_t)(p.nx + 2) * (p.ny + 2) * (p.nz + 2);
-        const float *raw = e->d_mstage;  // rho, pi, u as ifosb_set_model received them (ghosted)
+        const float *raw = e->d_mstage;  // rho, pi, u, taus, taup as ifosb_set_model received them (ghosted)
         const dim3 blk3(128), grd3((p.nz + 127) / 128, p.nx, p.ny);
-        k64_model<<<grd3, blk3, 0, e->stream>>>(g, raw, raw + ng, raw + 2 * ng, md);
+        k64_model<<<grd3, blk3, 0, e->stream>>>(g, raw, raw + ng, raw + 2 * ng, L ? raw + 3 * ng : nullptr,
+                                                 L ? raw + 4 * ng : nullptr, md);
         Vjp64 a{};
         a.g = g;
         a.sl = e->sl;
@@ -1448,6 +1452,14 @@ extern "C" int ifosb_vjp_exact(ifosb_engine *e, int interval, double *grad, doub
         a.dx = (double)p.dt / p.dx; a.dy = (double)p.dt / p.dy; a.dz = (double)p.dt / p.dz;
         a.rdx = p.dx; a.rdy = p.dy; a.rdz = p.dz; a.dt = p.dt;
         a.nt_total = NT;
+        a.nmech = L;
+        for (int l = 0; l < L; ++l) {  // update_s_ssg.c:123-124, surface_ssg.c:152, in double
+            const double eta = e->eta[l];
+            a.eta[l] = eta;
+            a.bb[l] = 1.0 / (1.0 + eta * 0.5);
+            a.cc[l] = 1.0 - eta * 0.5;
+            a.msb[l] = eta / (1.0 + eta * 0.5);
+        }
         Grad64 gr;
         for (int q = 0; q < N64; ++q) gr.q[q] = gq + (size_t)q * n;
         std::vector<int> rec(e->rec.begin(), e->rec.end());
@@ -1482,7 +1494,7 @@ extern "C" int ifosb_vjp_exact(ifosb_engine *e, int interval, double *grad, doub
             a.src = dsrc;
             a.amp = damp;
             auto step = [&](double *st, int nt) {
-                double *ps = st + (size_t)NEL * F;
+                double *ps = st + (size_t)NELV * F;
                 k64_vel<<<grd3, blk3, 0, e->stream>>>(a, st, ps);
                 k64_str<<<grd3, blk3, 0, e->stream>>>(a, st, ps, nt);
             };
@@ -1522,12 +1534,12 @@ extern "C" int ifosb_vjp_exact(ifosb_engine *e, int interval, double *grad, doub
                 }
             }
             misfit[sh] = J;
-            if (!grad) continue;
+            if (!gmod) continue;
             CU(cudaMemcpyAsync(asrc, src.data(), ntrace * sizeof(double), cudaMemcpyHostToDevice, e->stream));
             // 3. the transposed steps, last to first, each segment recomputed from its checkpoint
             CU(cudaMemsetAsync(lam, 0, SZ * sizeof(double), e->stream));
             CU(cudaMemsetAsync(ld, 0, 18 * (size_t)F * sizeof(double), e->stream));
-            double *lps = lam + (size_t)NEL * F;
+            double *lps = lam + (size_t)NELV * F;
             const dim3 grdg((p.nz + 127) / 128, p.nx, p.ny + (g.free_surf ? 2 : 0));
             const dim3 grds((p.nz + 127) / 128, p.nx);
             for (int q = nseg - 1; q >= 0; --q) {
@@ -1542,7 +1554,7 @@ extern "C" int ifosb_vjp_exact(ifosb_engine *e, int interval, double *grad, doub
                     const double *cur = seg + (size_t)(nt - a0 + 1) * SZ, *prev = cur - SZ;
                     k64_inject<<<(ntr + 127) / 128, 128, 0, e->stream>>>(g, lam, drec, ntr, ns, nt - 1, asrc);
                     if (g.free_surf) k64_mirror_T<<<grds, blk3, 0, e->stream>>>(g, lam);
-                    k64_str_T<<<grd3, blk3, 0, e->stream>>>(a, lam, lps, ld, cur, prev + (size_t)NEL * F, gr);
+                    k64_str_T<<<grd3, blk3, 0, e->stream>>>(a, lam, lps, ld, cur, prev + (size_t)NELV * F, gr);
                     k64_str_T_gather<<<grd3, blk3, 0, e->stream>>>(a, lam, ld);
                     k64_vel_T<<<grd3, blk3, 0, e->stream>>>(a, lam, lps, ls, cur, prev, gr);
                     k64_vel_T_gather<<<grdg, blk3, 0, e->stream>>>(a, lam, ls, g.free_surf ? -1 : 1);
@@ -1550,9 +1562,9 @@ extern "C" int ifosb_vjp_exact(ifosb_engine *e, int interval, double *grad, doub
                 if ((r = check_launch(e, "exact VJP adjoint"))) return r;
             }
         }
-        if (!grad) return IFOSB_OK;
+        if (!gmod) return IFOSB_OK;
         // 4. the averaged moduli's gradients onto the raw model (av_mat.c:45-69 and
-        //    matcopy's periodic ghost layers), then onto vp, vs, rho
+        //    matcopy's periodic ghost layers)
         std::vector<double> gh((size_t)N64 * n);
         std::vector<float> rawh(3 * ng);
         CU(cudaMemcpyAsync(gh.data(), gq, gh.size() * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
@@ -1560,8 +1572,10 @@ extern "C" int ifosb_vjp_exact(ifosb_engine *e, int interval, double *grad, doub
         CU(cudaStreamSynchronize(e->stream));
         const int NX = p.nx, NY = p.ny, NZ = p.nz, GX = NX + 2, GZ = NZ + 2;
         auto G = [&](int j, int i, int k) { return ((size_t)j * GX + i) * GZ + k; };
-        const float *rho = rawh.data(), *pi = rho + ng, *u = pi + ng;
-        std::vector<double> dr(ng, 0.0), dp(ng, 0.0), du(ng, 0.0);
+        const float *u = rawh.data() + 2 * ng;
+        // ghosted accumulators in the order of the output: rho, pi, u, taus, taup
+        std::vector<double> acc(5 * ng, 0.0);
+        double *dr = acc.data(), *dp = dr + ng, *du = dp + ng, *dts = du + ng, *dtp = dts + ng;
         auto harm = [&](double gval, int j0, int i0, int k0, int j1, int i1, int k1, int j2, int i2, int k2, int j3,
                         int i3, int k3) {
             const size_t c[4] = {G(j0, i0, k0), G(j1, i1, k1), G(j2, i2, k2), G(j3, i3, k3)};
@@ -1569,6 +1583,11 @@ extern "C" int ifosb_vjp_exact(ifosb_engine *e, int interval, double *grad, doub
             for (size_t q : c) s += 1.0 / (double)u[q];
             const double avg = 4.0 / s;
             for (size_t q : c) du[q] += gval * avg * avg / (4.0 * (double)u[q] * (double)u[q]);
+        };
+        auto quarter = [&](double gval, int j0, int i0, int k0, int j1, int i1, int k1, int j2, int i2, int k2, int j3,
+                           int i3, int k3) {
+            dts[G(j0, i0, k0)] += 0.25 * gval; dts[G(j1, i1, k1)] += 0.25 * gval;
+            dts[G(j2, i2, k2)] += 0.25 * gval; dts[G(j3, i3, k3)] += 0.25 * gval;
         };
         for (int j = 1; j <= NY; ++j)
             for (int i = 1; i <= NX; ++i)
@@ -1583,29 +1602,23 @@ extern "C" int ifosb_vjp_exact(ifosb_engine *e, int interval, double *grad, doub
                     harm(gv(M64_UIPJP), j, i, k, j, i + 1, k, j + 1, i + 1, k, j + 1, i, k);
                     harm(gv(M64_UJPKP), j, i, k, j, i, k + 1, j + 1, i, k + 1, j + 1, i, k);
                     harm(gv(M64_UIPKP), j, i, k, j, i, k + 1, j, i + 1, k + 1, j, i + 1, k);
+                    if (L) {  // tausipjp ... are plain means of four cells (av_mat.c:57-59)
+                        dts[c] += gv(M64_TAUS);
+                        dtp[c] += gv(M64_TAUP);
+                        quarter(gv(M64_TSIPJP), j, i, k, j, i + 1, k, j + 1, i + 1, k, j + 1, i, k);
+                        quarter(gv(M64_TSJPKP), j, i, k, j + 1, i, k, j + 1, i, k + 1, j, i, k + 1);
+                        quarter(gv(M64_TSIPKP), j, i, k, j, i + 1, k, j, i + 1, k + 1, j, i, k + 1);
+                    }
                 }
         // fold the ghost layers (matcopy on one rank: index 0 = N, N + 1 = 1)
         auto wrapi = [](int x, int N) { return x == 0 ? N : (x == N + 1 ? 1 : x); };
-        std::vector<double> fr(n, 0.0), fp(n, 0.0), fu(n, 0.0);
+        std::fill(gmod, gmod + 5 * n, 0.0);
         for (int j = 0; j <= NY + 1; ++j)
             for (int i = 0; i <= NX + 1; ++i)
                 for (int k = 0; k <= NZ + 1; ++k) {
                     const size_t c = G(j, i, k);
-                    if (dr[c] == 0.0 && dp[c] == 0.0 && du[c] == 0.0) continue;
                     const size_t m = ((size_t)(wrapi(j, NY) - 1) * NX + (wrapi(i, NX) - 1)) * NZ + (wrapi(k, NZ) - 1);
-                    fr[m] += dr[c];
-                    fp[m] += dp[c];
-                    fu[m] += du[c];
-                }
-        // pi = rho vp^2, u = rho vs^2 (readmod.c with L = 0)
-        for (int j = 1; j <= NY; ++j)
-            for (int i = 1; i <= NX; ++i)
-                for (int k = 1; k <= NZ; ++k) {
-                    const size_t m = ((size_t)(j - 1) * NX + (i - 1)) * NZ + (k - 1), c = G(j, i, k);
-                    const double r = rho[c], vp = std::sqrt((double)pi[c] / r), vs = std::sqrt((double)u[c] / r);
-                    grad[m] = fp[m] * 2.0 * r * vp;
-                    grad[n + m] = fu[m] * 2.0 * r * vs;
-                    grad[2 * n + m] = fr[m] + fp[m] * vp * vp + fu[m] * vs * vs;
+                    for (int q = 0; q < 5; ++q) gmod[(size_t)q * n + m] += acc[(size_t)q * ng + c];
                 }
         return IFOSB_OK;
     };
@@ -1615,6 +1628,39 @@ extern "C" int ifosb_vjp_exact(ifosb_engine *e, int interval, double *grad, doub
     if (ibuf) cudaFree(ibuf);
     if (damp) cudaFree(damp);
     return rc;
+}
+
+extern "C" int ifosb_vjp_exact_moduli(ifosb_engine *e, int interval, double *grad, double *misfit) {
+    return vjp_exact_moduli(e, interval, grad, misfit);
+}
+
+// The elastic form: the moduli gradient through pi = rho vp^2, u = rho vs^2
+// (readmod.c with L = 0) onto vp, vs, rho, [3][NY*NX*NZ].
+extern "C" int ifosb_vjp_exact(ifosb_engine *e, int interval, double *grad, double *misfit) {
+    if (!e || !misfit || interval < 1) return IFOSB_EARG;
+    const ifosb_params &p = e->p;
+    if (p.nmech != 0)
+        return fail(e, IFOSB_EARG, "the (vp, vs, rho) form is elastic; ifosb_vjp_exact_moduli takes L > 0");
+    if (!grad) return vjp_exact_moduli(e, interval, nullptr, misfit);
+    const size_t n = (size_t)p.nx * p.ny * p.nz, ng = (size_t)(p.nx + 2) * (p.ny + 2) * (p.nz + 2);
+    std::vector<double> gm(5 * n);
+    int rc = vjp_exact_moduli(e, interval, gm.data(), misfit);
+    if (rc) return rc;
+    std::vector<float> rawh(3 * ng);
+    CU(cudaMemcpy(rawh.data(), e->d_mstage, rawh.size() * sizeof(float), cudaMemcpyDeviceToHost));
+    const int NX = p.nx, NY = p.ny, NZ = p.nz, GX = NX + 2, GZ = NZ + 2;
+    const float *rho = rawh.data(), *pi = rho + ng, *u = pi + ng;
+    const double *fr = gm.data(), *fp = fr + n, *fu = fp + n;
+    for (int j = 1; j <= NY; ++j)
+        for (int i = 1; i <= NX; ++i)
+            for (int k = 1; k <= NZ; ++k) {
+                const size_t m = ((size_t)(j - 1) * NX + (i - 1)) * NZ + (k - 1), c = ((size_t)j * GX + i) * GZ + k;
+                const double r = rho[c], vp = std::sqrt((double)pi[c] / r), vs = std::sqrt((double)u[c] / r);
+                grad[m] = fp[m] * 2.0 * r * vp;
+                grad[n + m] = fu[m] * 2.0 * r * vs;
+                grad[2 * n + m] = fr[m] + fp[m] * vp * vp + fu[m] * vs * vs;
+            }
+    return IFOSB_OK;
 }
 
 // ---------------------------------------------------------------------------

@@ -37,22 +37,31 @@ namespace ifosb {
 struct Vjp64 {
     Geo g;
     Slabs sl;
-    const double *md;   // [8][field]: pi, u, uipjp, ujpkp, uipkp, rip, rjp, rkp
+    const double *md;   // [N64][field]: pi, u, uipjp, ujpkp, uipkp, rip, rjp, rkp, taus, taup, tausipjp, tausjpkp, tausipkp
     const float *cpg;   // CPML rows [18][2*MAXFW] (float, as the engine's)
     double b1, b2, dx, dy, dz, rdx, rdy, rdz, dt;  // dx = DT/DX (velocity update), rdx = DX
     int nsrc;
     const int *src;     // [nsrc][3] j, i, k of explosive sources
     const double *amp;  // [nsrc][NT] psource amplitudes
     int nt_total;
+    // L relaxation mechanisms (0 = elastic): eta_l = DT/tau_l and the update's
+    // 1/(1+eta/2), 1-eta/2 and the surface's eta/(1+eta/2) (update_s_ssg.c:123-124,
+    // surface_ssg.c:152)
+    int nmech;
+    double eta[MAXMECH], bb[MAXMECH], cc[MAXMECH], msb[MAXMECH];
 };
 
-enum { M64_PI = 0, M64_U, M64_UIPJP, M64_UJPKP, M64_UIPKP, M64_RIP, M64_RJP, M64_RKP, N64 };
+enum {
+    M64_PI = 0, M64_U, M64_UIPJP, M64_UJPKP, M64_UIPKP, M64_RIP, M64_RJP, M64_RKP,
+    M64_TAUS, M64_TAUP, M64_TSIPJP, M64_TSJPKP, M64_TSIPKP, N64
+};
 
 __device__ __forceinline__ double cp64(const float *cpg, int row, int h) { return (double)cpg[row * 2 * MAXFW + h - 1]; }
 
 // the averaged model in double from the raw ghosted model ([NY+2][NX+2][NZ+2] floats):
 // the expressions of av_mat (av_mat.c:45-69) without their float rounding
-__global__ void k64_model(Geo g, const float *rho, const float *pi, const float *u, double *md) {
+__global__ void k64_model(Geo g, const float *rho, const float *pi, const float *u, const float *taus,
+                          const float *taup, double *md) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x + 1, i = blockIdx.y + 1, j = blockIdx.z + 1;
     if (k > g.nz) return;
     const long long F = g.field, c = widx(g, j, i, k);
@@ -66,6 +75,13 @@ __global__ void k64_model(Geo g, const float *rho, const float *pi, const float 
     md[M64_RIP * F + c] = 0.5 * (G(rho, j, i, k) + G(rho, j, i + 1, k));
     md[M64_RJP * F + c] = 0.5 * (G(rho, j, i, k) + G(rho, j + 1, i, k));
     md[M64_RKP * F + c] = 0.5 * (G(rho, j, i, k) + G(rho, j, i, k + 1));
+    if (taus) {
+        md[M64_TAUS * F + c] = G(taus, j, i, k);
+        md[M64_TAUP * F + c] = G(taup, j, i, k);
+        md[M64_TSIPJP * F + c] = 0.25 * (G(taus, j, i, k) + G(taus, j, i + 1, k) + G(taus, j + 1, i + 1, k) + G(taus, j + 1, i, k));
+        md[M64_TSJPKP * F + c] = 0.25 * (G(taus, j, i, k) + G(taus, j + 1, i, k) + G(taus, j + 1, i, k + 1) + G(taus, j, i, k + 1));
+        md[M64_TSIPKP * F + c] = 0.25 * (G(taus, j, i, k) + G(taus, j, i + 1, k) + G(taus, j, i + 1, k + 1) + G(taus, j, i, k + 1));
+    }
 }
 
 // 4th-order differences: "up" reads f[c+1] - f[c] (and f[c+2] - f[c-1]),
@@ -192,8 +208,35 @@ __device__ __forceinline__ void vel_derivs(const Vjp64 &a, const double *st, dou
     }
 }
 
-// stress update, explosive sources, free surface and its mirror rows
-// (update_s_ssg_elastic.c:106-140, psource.c:38-52, surface_ssg_elastic.c:69-111)
+// stress update with L memory-variable mechanisms, explosive sources, free
+// surface and its mirror rows (update_s_ssg_elastic.c:106-140 for L = 0,
+// update_s_ssg.c:108-140 generalised to L mechanisms, psource.c:38-52,
+// surface_ssg_elastic.c:69-111 and surface_ssg.c:117-160). With
+// gg = pi (1 + L taup), f = 2u (1 + L taus), f_xy = DT uipjp (1 + L tausipjp) ...:
+//   sigma' = sigma + DT C(gg, f, f_xy..) e + DT/2 (sum_l r_l + sum_l r_l')
+//   r_l'   = bb_l (cc_l r_l - D_l(e)),  D_l with E_l = pi eta_l taup, D_l = 2u eta_l taus
+//            (normal) and uipjp eta_l tausipjp ... (shear)
+// At the surface (j = 1): syy = 0, r_yy = 0, sxx and szz gain h + DT/2 sum_l hh_l and
+// r_xx, r_zz gain hh_l, hh_l = msb_l ((dd - ee)(f/gg - 1)(dxx + dzz) - (dd - ee) dyy),
+// dd = 2u taus, ee = pi taup, on the plain derivatives.
+struct Mod64 {
+    double pim, um, uipjp, ujpkp, uipkp, taus, taup, tsipjp, tsjpkp, tsipkp;
+};
+__device__ __forceinline__ Mod64 mod64(const Vjp64 &a, long long c) {
+    const long long F = a.g.field;
+    const double *md = a.md;
+    Mod64 m;
+    m.pim = md[M64_PI * F + c]; m.um = md[M64_U * F + c];
+    m.uipjp = md[M64_UIPJP * F + c]; m.ujpkp = md[M64_UJPKP * F + c]; m.uipkp = md[M64_UIPKP * F + c];
+    if (a.nmech) {
+        m.taus = md[M64_TAUS * F + c]; m.taup = md[M64_TAUP * F + c];
+        m.tsipjp = md[M64_TSIPJP * F + c]; m.tsjpkp = md[M64_TSJPKP * F + c]; m.tsipkp = md[M64_TSIPKP * F + c];
+    } else {
+        m.taus = m.taup = m.tsipjp = m.tsjpkp = m.tsipkp = 0.0;
+    }
+    return m;
+}
+
 __global__ void k64_str(Vjp64 a, double *st, double *ps, int nt) {
     const Geo &g = a.g;
     const int k = blockIdx.x * blockDim.x + threadIdx.x + 1, i = blockIdx.y + 1, j = blockIdx.z + 1;
@@ -201,35 +244,65 @@ __global__ void k64_str(Vjp64 a, double *st, double *ps, int nt) {
     const long long F = g.field, c = widx(g, j, i, k), dJ = g.plane;
     VDer v;
     vel_derivs(a, st, ps + 3 * (a.sl.sx + a.sl.sy + a.sl.sz), j, i, k, v);
-    const double *md = a.md;
-    const double pim = md[M64_PI * F + c], um = md[M64_U * F + c], DT = a.dt;
+    const Mod64 m = mod64(a, c);
+    const int L = a.nmech;
+    const double DT = a.dt, h = 0.5 * DT, Lf = L;
     const double *e = v.e;
+    const double gg = m.pim * (1.0 + Lf * m.taup), f = 2.0 * m.um * (1.0 + Lf * m.taus);
+    const double fxy = DT * m.uipjp * (1.0 + Lf * m.tsipjp), fyz = DT * m.ujpkp * (1.0 + Lf * m.tsjpkp),
+                 fxz = DT * m.uipkp * (1.0 + Lf * m.tsipkp);
+    const double exy = e[1] + e[3], eyz = e[5] + e[7], exz = e[2] + e[6];
+    const double div = e[0] + e[4] + e[8], syz_ = e[4] + e[8], sxz_ = e[0] + e[8], sxy_ = e[0] + e[4];
     double *S = st + c;
-    double sxx = S[SXX * F], syy = S[SYY * F], szz = S[SZZ * F], sxy = S[SXY * F], syz = S[SYZ * F], sxz = S[SXZ * F];
-    const double div = e[0] + e[4] + e[8], f2 = 2.0 * um;
-    sxy += DT * md[M64_UIPJP * F + c] * (e[1] + e[3]);
-    syz += DT * md[M64_UJPKP * F + c] * (e[5] + e[7]);
-    sxz += DT * md[M64_UIPKP * F + c] * (e[2] + e[6]);
-    sxx += DT * (pim * div - f2 * (e[4] + e[8]));
-    syy += DT * (pim * div - f2 * (e[0] + e[8]));
-    szz += DT * (pim * div - f2 * (e[0] + e[4]));
+    // sigma slots in the order xx yy zz xy yz xz of the memory variables
+    double sg[6] = {S[SXX * F], S[SYY * F], S[SZZ * F], S[SXY * F], S[SYZ * F], S[SXZ * F]};
+    sg[0] += DT * (gg * div - f * syz_);
+    sg[1] += DT * (gg * div - f * sxz_);
+    sg[2] += DT * (gg * div - f * sxy_);
+    sg[3] += fxy * exy;
+    sg[4] += fyz * eyz;
+    sg[5] += fxz * exz;
+    double rn[MAXMECH][6];
+    for (int l = 0; l < L; ++l) {
+        double *R = st + (NEL + 6 * l) * F + c;
+        const double El = m.pim * a.eta[l] * m.taup, Dl = 2.0 * m.um * a.eta[l] * m.taus;
+        const double drive[6] = {El * div - Dl * syz_, El * div - Dl * sxz_, El * div - Dl * sxy_,
+                                 m.uipjp * a.eta[l] * m.tsipjp * exy, m.ujpkp * a.eta[l] * m.tsjpkp * eyz,
+                                 m.uipkp * a.eta[l] * m.tsipkp * exz};
+        for (int q = 0; q < 6; ++q) {
+            const double ro = R[q * F];
+            rn[l][q] = a.bb[l] * (a.cc[l] * ro - drive[q]);
+            sg[q] += h * (ro + rn[l][q]);
+        }
+    }
     for (int q = 0; q < a.nsrc; ++q)
         if (a.src[3 * q] == j && a.src[3 * q + 1] == i && a.src[3 * q + 2] == k) {
             const double am = a.amp[(long long)q * a.nt_total + nt - 1];
-            sxx += am; syy += am; szz += am;
+            sg[0] += am; sg[1] += am; sg[2] += am;
         }
     if (g.free_surf && j == 1) {
-        syy = 0.0;
-        const double gg = pim, ff = f2;
-        const double h = -(DT * (gg - ff) * (gg - ff) * (v.d[0] + v.d[8]) / gg) - (DT * (gg - ff) * v.d[4]);
-        sxx += h;
-        szz += h;
+        sg[1] = 0.0;
+        const double X = v.d[0] + v.d[8], Y = v.d[4];
+        const double hs = -(DT * (gg - f) * (gg - f) * X / gg) - (DT * (gg - f) * Y);
+        sg[0] += hs;
+        sg[2] += hs;
+        const double dd = 2.0 * m.um * m.taus, ee = m.pim * m.taup;
+        for (int l = 0; l < L; ++l) {
+            const double hh = a.msb[l] * ((dd - ee) * (f / gg - 1.0) * X - (dd - ee) * Y);
+            rn[l][1] = 0.0;
+            rn[l][0] += hh;
+            rn[l][2] += hh;
+            sg[0] += h * hh;
+            sg[2] += h * hh;
+        }
     }
-    S[SXX * F] = sxx; S[SYY * F] = syy; S[SZZ * F] = szz; S[SXY * F] = sxy; S[SYZ * F] = syz; S[SXZ * F] = sxz;
+    S[SXX * F] = sg[0]; S[SYY * F] = sg[1]; S[SZZ * F] = sg[2]; S[SXY * F] = sg[3]; S[SYZ * F] = sg[4]; S[SXZ * F] = sg[5];
+    for (int l = 0; l < L; ++l)
+        for (int q = 0; q < 6; ++q) st[(NEL + 6 * l + q) * F + c] = rn[l][q];
     if (g.free_surf && j <= 3) {
-        if (j == 1) { S[SXY * F - dJ] = -sxy; S[SYZ * F - dJ] = -syz; }
-        if (j == 2) { S[SYY * F - 2 * dJ] = -syy; S[SXY * F - 3 * dJ] = -sxy; S[SYZ * F - 3 * dJ] = -syz; }
-        if (j == 3) { S[SYY * F - 4 * dJ] = -syy; }
+        if (j == 1) { S[SXY * F - dJ] = -sg[3]; S[SYZ * F - dJ] = -sg[4]; }
+        if (j == 2) { S[SYY * F - 2 * dJ] = -sg[1]; S[SXY * F - 3 * dJ] = -sg[3]; S[SYZ * F - 3 * dJ] = -sg[4]; }
+        if (j == 3) { S[SYY * F - 4 * dJ] = -sg[1]; }
     }
 }
 
@@ -272,21 +345,23 @@ struct Grad64 {
 };
 
 // B^T at one interior cell: the adjoints of the nine velocity derivatives (ld),
-// the velocity-derivative PML memories (lps, one step back), the stresses'
-// pass-through, and the moduli gradients. cur = x^n (v^n), prev = x^{n-1} (psi_v^{n-1}).
+// the velocity-derivative PML memories (lps, one step back), the stresses' and
+// memory variables' adjoints one step back, and the gradients of the cell's
+// coefficients. cur = x^n (v^n), prev_ps = the PML memory of x^{n-1}.
 __global__ void k64_str_T(Vjp64 a, double *lam, double *lps, double *ld, const double *cur, const double *prev_ps,
                           Grad64 gr) {
     const Geo &g = a.g;
     const int k = blockIdx.x * blockDim.x + threadIdx.x + 1, i = blockIdx.y + 1, j = blockIdx.z + 1;
     if (k > g.nz) return;
     const long long F = g.field, c = widx(g, j, i, k);
-    const long long m = ((long long)(j - 1) * g.nx + (i - 1)) * g.nz + (k - 1);
+    const long long mm = ((long long)(j - 1) * g.nx + (i - 1)) * g.nz + (k - 1);
     const long long poff = 3 * (a.sl.sx + a.sl.sy + a.sl.sz);
+    const int hx = face_x(g, i), hy = face_y(g, j), hz = face_z(g, k);
+    const float *cg = a.cpg;
     // the forward derivatives of step n: v^n with the old psi_v, whose recursion runs
     // in registers (the stored forward state stays as it is)
     VDer v;
     {
-        const int hx = face_x(g, i), hy = face_y(g, j), hz = face_z(g, k);
         const double *st = cur;
         const long long dI = g.pz, dJ = g.plane;
         const double *vx = st + VX * F, *vy = st + VY * F, *vz = st + VZ * F;
@@ -301,7 +376,6 @@ __global__ void k64_str_T(Vjp64 a, double *lam, double *lps, double *ld, const d
         v.d[7] = dup(vz, c, dJ, b1, b2) / a.rdy;
         v.d[8] = ddn(vz, c, 1, b1, b2) / a.rdz;
         for (int q = 0; q < 9; ++q) v.e[q] = v.d[q];
-        const float *cg = a.cpg;
         const double *P = prev_ps + poff;
         if (hx) {
             const long long o = sxi(g, j, hx, k), s = a.sl.sx;
@@ -328,37 +402,99 @@ __global__ void k64_str_T(Vjp64 a, double *lam, double *lps, double *ld, const d
             v.e[8] = cpml_fwd(v.d[8], t2, kf, cp64(cg, A_Z, hz), cp64(cg, B_Z, hz));
         }
     }
-    const double *md = a.md;
-    const double pim = md[M64_PI * F + c], um = md[M64_U * F + c], DT = a.dt, f2 = 2.0 * um;
-    double *L = lam + c;
-    double lxx = L[SXX * F], lyy = L[SYY * F], lzz = L[SZZ * F], lxy = L[SXY * F], lyz = L[SYZ * F], lxz = L[SXZ * F];
-    double lh = 0.0;
+    const Mod64 m = mod64(a, c);
+    const int L = a.nmech;
+    const double DT = a.dt, h = 0.5 * DT, Lf = L;
+    const double *e = v.e;
+    const double gg = m.pim * (1.0 + Lf * m.taup), f = 2.0 * m.um * (1.0 + Lf * m.taus);
+    const double fxy = DT * m.uipjp * (1.0 + Lf * m.tsipjp), fyz = DT * m.ujpkp * (1.0 + Lf * m.tsjpkp),
+                 fxz = DT * m.uipkp * (1.0 + Lf * m.tsipkp);
+    const double exy = e[1] + e[3], eyz = e[5] + e[7], exz = e[2] + e[6];
+    const double div = e[0] + e[4] + e[8], syz_ = e[4] + e[8], sxz_ = e[0] + e[8], sxy_ = e[0] + e[4];
+    static constexpr int sslot[6] = {SXX, SYY, SZZ, SXY, SYZ, SXZ};
+    double Ls[6], Lr[MAXMECH][6];
+    for (int q = 0; q < 6; ++q) Ls[q] = lam[sslot[q] * F + c];
+    for (int l = 0; l < L; ++l)
+        for (int q = 0; q < 6; ++q) Lr[l][q] = lam[(NEL + 6 * l + q) * F + c];
+    double g_gg = 0.0, g_f = 0.0, g_dd = 0.0, g_ee = 0.0;
+    double Wd[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};  // adjoints of the plain derivatives (surface terms)
     const bool surf = g.free_surf && j == 1;
     if (surf) {
-        lh = lxx + lzz;  // sxx, szz += h
-        lyy = 0.0;       // syy = 0 after the update: nothing before it reaches syy(n)
-        L[SYY * F] = 0.0;
+        const double X = v.d[0] + v.d[8], Y = v.d[4], gf = gg - f;
+        const double lhs = Ls[0] + Ls[2];
+        const double dd = 2.0 * m.um * m.taus, ee = m.pim * m.taup, B = dd - ee;
+        g_gg += lhs * (-DT * X * (2.0 * gf * gg - gf * gf) / (gg * gg) - DT * Y);
+        g_f += lhs * (DT * 2.0 * gf * X / gg + DT * Y);
+        Wd[0] += lhs * (-(DT * gf * gf / gg));
+        Wd[8] += lhs * (-(DT * gf * gf / gg));
+        Wd[4] += lhs * (-(DT * gf));
+        for (int l = 0; l < L; ++l) {
+            const double lhh = h * lhs + Lr[l][0] + Lr[l][2];
+            const double dhdB = a.msb[l] * ((f / gg - 1.0) * X - Y);
+            g_dd += lhh * dhdB;
+            g_ee -= lhh * dhdB;
+            g_f += lhh * a.msb[l] * B * X / gg;
+            g_gg += lhh * (-a.msb[l] * B * f * X / (gg * gg));
+            Wd[0] += lhh * a.msb[l] * B * (f / gg - 1.0);
+            Wd[8] += lhh * a.msb[l] * B * (f / gg - 1.0);
+            Wd[4] += lhh * (-a.msb[l] * B);
+            Lr[l][1] = 0.0;  // r_yy = 0 after the update
+        }
+        Ls[1] = 0.0;  // syy = 0 after the update
     }
-    // moduli gradients of the update sigma += DT C(model) e
-    const double *e = v.e;
-    gr.q[M64_PI][m] += DT * (lxx + lyy + lzz) * (e[0] + e[4] + e[8]);
-    gr.q[M64_U][m] += -2.0 * DT * (lxx * (e[4] + e[8]) + lyy * (e[0] + e[8]) + lzz * (e[0] + e[4]));
-    gr.q[M64_UIPJP][m] += DT * lxy * (e[1] + e[3]);
-    gr.q[M64_UJPKP][m] += DT * lyz * (e[5] + e[7]);
-    gr.q[M64_UIPKP][m] += DT * lxz * (e[2] + e[6]);
-    // adjoints of the effective derivatives
+    // the update: sigma' = sigma + M e + h (sum r + sum r'), r' = bb (cc r - D(e))
     double W[9];
-    W[0] = DT * (pim * lxx + (pim - f2) * (lyy + lzz));
-    W[4] = DT * (pim * lyy + (pim - f2) * (lxx + lzz));
-    W[8] = DT * (pim * lzz + (pim - f2) * (lxx + lyy));
-    W[1] = W[3] = DT * md[M64_UIPJP * F + c] * lxy;
-    W[5] = W[7] = DT * md[M64_UJPKP * F + c] * lyz;
-    W[2] = W[6] = DT * md[M64_UIPKP * F + c] * lxz;
+    W[0] = DT * (gg * Ls[0] + (gg - f) * (Ls[1] + Ls[2]));
+    W[4] = DT * (gg * Ls[1] + (gg - f) * (Ls[0] + Ls[2]));
+    W[8] = DT * (gg * Ls[2] + (gg - f) * (Ls[0] + Ls[1]));
+    W[1] = W[3] = fxy * Ls[3];
+    W[5] = W[7] = fyz * Ls[4];
+    W[2] = W[6] = fxz * Ls[5];
+    g_gg += DT * div * (Ls[0] + Ls[1] + Ls[2]);
+    g_f += -DT * (syz_ * Ls[0] + sxz_ * Ls[1] + sxy_ * Ls[2]);
+    double g_fxy = exy * Ls[3], g_fyz = eyz * Ls[4], g_fxz = exz * Ls[5];
+    double g_pi_r = 0.0, g_u_r = 0.0, g_tp_r = 0.0, g_ts_r = 0.0;
+    double g_uxy_r = 0.0, g_uyz_r = 0.0, g_uxz_r = 0.0, g_txy_r = 0.0, g_tyz_r = 0.0, g_txz_r = 0.0;
+    for (int l = 0; l < L; ++l) {
+        double Lrn[6];
+        for (int q = 0; q < 6; ++q) Lrn[q] = Lr[l][q] + h * Ls[q];  // adjoint of r' (before the surface terms)
+        const double eta = a.eta[l], bb = a.bb[l];
+        const double El = m.pim * eta * m.taup, Dl = 2.0 * m.um * eta * m.taus;
+        const double sn = Lrn[0] + Lrn[1] + Lrn[2];
+        W[0] += -bb * (El * sn - Dl * (Lrn[1] + Lrn[2]));
+        W[4] += -bb * (El * sn - Dl * (Lrn[0] + Lrn[2]));
+        W[8] += -bb * (El * sn - Dl * (Lrn[0] + Lrn[1]));
+        const double dxy = m.uipjp * eta * m.tsipjp, dyz = m.ujpkp * eta * m.tsjpkp, dxz = m.uipkp * eta * m.tsipkp;
+        W[1] += -bb * dxy * Lrn[3]; W[3] += -bb * dxy * Lrn[3];
+        W[5] += -bb * dyz * Lrn[4]; W[7] += -bb * dyz * Lrn[4];
+        W[2] += -bb * dxz * Lrn[5]; W[6] += -bb * dxz * Lrn[5];
+        const double gE = -bb * div * sn, gD = bb * (syz_ * Lrn[0] + sxz_ * Lrn[1] + sxy_ * Lrn[2]);
+        g_pi_r += gE * eta * m.taup; g_tp_r += gE * m.pim * eta;
+        g_u_r += gD * 2.0 * eta * m.taus; g_ts_r += gD * 2.0 * m.um * eta;
+        const double gxy = -bb * exy * Lrn[3], gyz = -bb * eyz * Lrn[4], gxz = -bb * exz * Lrn[5];
+        g_uxy_r += gxy * eta * m.tsipjp; g_txy_r += gxy * m.uipjp * eta;
+        g_uyz_r += gyz * eta * m.tsjpkp; g_tyz_r += gyz * m.ujpkp * eta;
+        g_uxz_r += gxz * eta * m.tsipkp; g_txz_r += gxz * m.uipkp * eta;
+        // the memory variable one step back: r' reads cc r, sigma' reads h r
+        for (int q = 0; q < 6; ++q) lam[(NEL + 6 * l + q) * F + c] = bb * a.cc[l] * Lrn[q] + h * Ls[q];
+    }
+    for (int q = 0; q < 6; ++q) lam[sslot[q] * F + c] = Ls[q];
+    // the coefficients' gradients, onto the cell's model values
+    gr.q[M64_PI][mm] += g_gg * (1.0 + Lf * m.taup) + g_pi_r + g_ee * m.taup;
+    gr.q[M64_U][mm] += g_f * 2.0 * (1.0 + Lf * m.taus) + g_u_r + g_dd * 2.0 * m.taus;
+    gr.q[M64_UIPJP][mm] += g_fxy * DT * (1.0 + Lf * m.tsipjp) + g_uxy_r;
+    gr.q[M64_UJPKP][mm] += g_fyz * DT * (1.0 + Lf * m.tsjpkp) + g_uyz_r;
+    gr.q[M64_UIPKP][mm] += g_fxz * DT * (1.0 + Lf * m.tsipkp) + g_uxz_r;
+    if (L) {
+        gr.q[M64_TAUP][mm] += g_gg * Lf * m.pim + g_tp_r + g_ee * m.pim;
+        gr.q[M64_TAUS][mm] += g_f * 2.0 * m.um * Lf + g_ts_r + g_dd * 2.0 * m.um;
+        gr.q[M64_TSIPJP][mm] += g_fxy * DT * m.uipjp * Lf + g_txy_r;
+        gr.q[M64_TSJPKP][mm] += g_fyz * DT * m.ujpkp * Lf + g_tyz_r;
+        gr.q[M64_TSIPKP][mm] += g_fxz * DT * m.uipkp * Lf + g_txz_r;
+    }
     // through the CPML recursions (the adjoint memory steps back one step)
     double Ld[9];
     for (int q = 0; q < 9; ++q) Ld[q] = W[q];
-    const int hx = face_x(g, i), hy = face_y(g, j), hz = face_z(g, k);
-    const float *cg = a.cpg;
     double *P = lps + poff;
     if (hx) {
         const long long o = sxi(g, j, hx, k), s = a.sl.sx;
@@ -381,21 +517,7 @@ __global__ void k64_str_T(Vjp64 a, double *lam, double *lps, double *ld, const d
         Ld[5] = cpml_adj(W[5], P[o + s], kh, cp64(cg, AH_Z, hz), cp64(cg, BH_Z, hz));
         Ld[8] = cpml_adj(W[8], P[o + 2 * s], kf, cp64(cg, A_Z, hz), cp64(cg, B_Z, hz));
     }
-    if (surf) {
-        // h = -DT (g-f)^2 (dxx + dzz) / g - DT (g-f) dyy on the plain derivatives
-        const double gg = pim, gf = pim - f2;
-        const double hxz = -(DT * gf * gf / gg), hy_ = -(DT * gf);
-        Ld[0] += lh * hxz;
-        Ld[8] += lh * hxz;
-        Ld[4] += lh * hy_;
-        const double sxz_ = v.d[0] + v.d[8];
-        // d h / d g and d h / d f, f = 2 u
-        const double dhdg = -DT * (2.0 * gf * gg - gf * gf) / (gg * gg) * sxz_ - DT * v.d[4];
-        const double dhdf = DT * 2.0 * gf / gg * sxz_ + DT * v.d[4];
-        gr.q[M64_PI][m] += lh * dhdg;
-        gr.q[M64_U][m] += lh * 2.0 * dhdf;
-    }
-    for (int q = 0; q < 9; ++q) ld[q * F + c] = Ld[q];
+    for (int q = 0; q < 9; ++q) ld[q * F + c] = Ld[q] + Wd[q];
 }
 
 // velocity adjoint from the derivative adjoints: lambda_v += E^T ld

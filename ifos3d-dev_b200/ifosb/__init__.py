@@ -135,6 +135,7 @@ def lib():
             "ifosb_set_wait_test": (C.c_int, [vp, C.c_longlong, C.c_int, C.c_int]),
             "ifosb_set_surface_moduli": (C.c_int, [vp, vp, vp]),
             "ifosb_vjp_exact": (C.c_int, [vp, C.c_int, vp, vp]),
+            "ifosb_vjp_exact_moduli": (C.c_int, [vp, C.c_int, vp, vp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -159,7 +160,7 @@ def exported_symbols():
         "ifosb_write_model", "ifosb_write_gradient", "ifosb_filt_seis", "ifosb_hessian_green", "ifosb_hessian",
         "ifosb_zero_hessian", "ifosb_get_hessian", "ifosb_read_hessian", "ifosb_hess_apply", "ifosb_resample",
         "ifosb_set_seismo", "ifosb_gradient_td", "ifosb_get_gradient_q", "ifosb_set_wait_test",
-        "ifosb_set_surface_moduli", "ifosb_vjp_exact",
+        "ifosb_set_surface_moduli", "ifosb_vjp_exact", "ifosb_vjp_exact_moduli",
     ]
 
 
@@ -423,15 +424,19 @@ class Engine:
         self._c(lib().ifosb_gradient_td(self.h, int(interval), _p(k)))
         return k
 
-    def vjp_exact(self, interval=25, want_grad=True):
+    def vjp_exact(self, interval=25, want_grad=True, moduli=False):
         """The exact discrete gradient of the misfit of the last forward batch and its
-        residual: (d misfit / d (vp, vs, rho) as float64 [3, NY, NX, NZ] summed over the
-        batch's shots, or None without want_grad; the FP64 misfit per shot). The time
-        loop runs in FP64 with a checkpoint every `interval` steps; elastic, explosive
-        sources."""
-        g = np.zeros((3, self.p.ny, self.p.nx, self.p.nz), np.float64) if want_grad else None
+        residual: (the gradient summed over the batch's shots, or None without
+        want_grad; the FP64 misfit per shot). The time loop runs in FP64 with a
+        checkpoint every `interval` steps; explosive sources. moduli=False (elastic
+        engines): d misfit / d (vp, vs, rho), float64 [3, NY, NX, NZ]. moduli=True
+        (any L): d misfit / d (rho, pi, u, taus, taup) of the model set_model received,
+        float64 [5, NY, NX, NZ]."""
+        nq = 5 if moduli else 3
+        g = np.zeros((nq, self.p.ny, self.p.nx, self.p.nz), np.float64) if want_grad else None
         mis = np.zeros(max(1, self.max_shots), np.float64)
-        self._c(lib().ifosb_vjp_exact(self.h, int(interval), _p(g), _p(mis)))
+        fn = lib().ifosb_vjp_exact_moduli if moduli else lib().ifosb_vjp_exact
+        self._c(fn(self.h, int(interval), _p(g), _p(mis)))
         return g, mis
 
     # -- approximate Hessian (hess_F) -----------------------------------------

@@ -175,18 +175,27 @@ int ifosb_get_gradient_q(ifosb_engine *e, double *gradq);
 /* The exact discrete vector-Jacobian product of the misfit (no counterpart in the
  * reference, whose gradient_F correlates a back-propagation with the forward operator,
  * src/ifos3d.c:882-975 — an approximation of the derivative). For each shot of the last
- * forward batch: the elastic time loop in FP64 (the engine's expressions without float
- * rounding) with a checkpoint every `interval` steps; the misfit
- * misfit[s] = sum D^2, D = DT * cumsum(syn - obs) over every trace of the shot (the
- * residual of residual.c:35-60; obs are the last ifosb_residual's observed traces); then
- * the transposed time steps in reverse — the CPML memory recursions, the free-surface
- * update and its image rows, the stress and velocity stencils — each segment of forward
- * states recomputed from its checkpoint. grad (optional, [3][NY][NX][NZ] FP64): the
- * derivative of the batch's summed misfit with respect to vp, vs, rho of each interior
- * cell, through av_mat's averages (src/av_mat.c:45-69), the model's ghost layers taken
- * as matcopy's periodic copies on one rank, and pi = rho vp^2, u = rho vs^2. NULL grad:
- * the misfits only. Elastic engines, explosive sources, NDT 1, NDTSHIFT 0. Device
- * memory: ceil(NT/interval) + interval + 2 FP64 states of one shot. */
+ * forward batch: the time loop in FP64 (the engine's expressions without float
+ * rounding: elastic, or L relaxation mechanisms with their memory variables) with a
+ * checkpoint every `interval` steps; the misfit misfit[s] = sum D^2,
+ * D = DT * cumsum(syn - obs) over every trace of the shot (the residual of
+ * residual.c:35-60; obs are the last ifosb_residual's observed traces); then the
+ * transposed time steps in reverse — the CPML memory recursions, the memory-variable
+ * recursions, the free-surface update and its image rows, the stress and velocity
+ * stencils — each segment of forward states recomputed from its checkpoint.
+ * grad (optional, [5][NY][NX][NZ] FP64): the derivative of the batch's summed misfit
+ * with respect to the raw model ifosb_set_model received — rho, pi, u, taus, taup of
+ * each interior cell (taus, taup zero for L = 0) — through av_mat's averages
+ * (src/av_mat.c:45-69, the taus means at :57-59) and the model's ghost layers taken as
+ * matcopy's periodic copies on one rank. NULL grad: the misfits only. Explosive
+ * sources, NDT 1, NDTSHIFT 0. Device memory: ceil(NT/interval) + interval + 2 FP64
+ * states of one shot (fields, 6 L memory variables, PML memory). */
+int ifosb_vjp_exact_moduli(ifosb_engine *e, int interval, double *grad, double *misfit);
+
+/* The same for elastic engines (nmech 0) with grad [3][NY][NX][NZ] with respect to
+ * vp, vs, rho: the moduli gradient through pi = rho vp^2, u = rho vs^2 (readmod.c with
+ * L = 0). EARG for L > 0, whose velocities depend on the reference frequency the
+ * engine does not hold: take the moduli form there. */
 int ifosb_vjp_exact(ifosb_engine *e, int interval, double *grad, double *misfit);
 
 /* Zero the accumulated gradients (zero_grad, src/zero_grad.c). */

@@ -16,6 +16,11 @@ misfit along any model direction d must equal <g, d>:
    and ifosb_residual, eps = 1e-3 relative): within 1e-3 along 8 seeded random
    directions.
 
+The same three checks hold for the viscoelastic loop (three relaxation
+mechanisms, Q = 20 fitted over 100-600 Hz; the gradient with respect to rho,
+pi, u, taus and taup, the random directions mixing all five; taus and taup are
+perturbed independently, so the free surface's taus - taup term is exercised).
+
 The case is a small version of the adjoint-check configuration: a 2000-3500 m/s
 depth gradient with a +-3 % Gaussian random field as the true model, the smooth
 gradient as the start model, free surface, CPML on the other faces, two
@@ -61,10 +66,10 @@ def _set_moduli(e, mods):
     e.set_model(*mods, None, None, None)
 
 
-def _directions(rng, count):
+def _directions(rng, count, nfield=3):
     out = []
     for _ in range(count):
-        w = rng.uniform(-1, 1, 3)
+        w = rng.uniform(-1, 1, nfield)
         f = synth._gauss_field((NY, NX, NZ), 3.0, rng).astype(np.float64)
         out.append(tuple(wi * f for wi in w))
     return out
@@ -141,6 +146,57 @@ def test_exact_vjp_matches_finite_differences():
     e.close()
 
 
+def test_exact_vjp_viscoelastic_matches_finite_differences():
+    p, rng, e, shots, true, start = _case()
+    e.close()
+    tau, fl = synth.q_tau_fit(20.0, 100.0, 600.0, 3)
+    pv = ifosb.make_params(NX, NY, NZ, dh=1.0, dt=DT, nt=NT, fdcoeff=2, free_surf=1, fw=FW, nmech=3)
+    e = ifosb.Engine(pv, max_shots=len(shots), max_nf=0)
+    e.set_cpml(ifosb.cpml_coeff(pv, 3500.0, FC))
+    e.set_receivers(synth._grid_receivers(NX, NZ, 4, 1, 9))
+    e.set_frequencies(None, 1)
+
+    def vmods(vp, vs, rho):
+        m = ifosb.moduli(pv, vp.ravel(), vs.ravel(), rho.ravel(), tau=tau, fl=fl)
+        return tuple(m[k].reshape(NY, NX, NZ) for k in ("rho", "pi", "u", "taus", "taup")), m["eta"]
+
+    mt, eta = vmods(*true)
+    e.set_model(*mt, eta)
+    obs = e.forward(shots)
+    mods, _ = vmods(*start)
+
+    def gpu_misfit(m):
+        e.set_model(*m, eta)
+        e.forward(shots, want_sections=False)
+        return float(e.residual(obs).sum())
+
+    def exact_misfit(m):
+        e.set_model(*m, eta)
+        e.forward(shots, want_sections=False)
+        e.residual(obs)
+        return float(e.vjp_exact(40, want_grad=False, moduli=True)[1][:len(shots)].sum())
+
+    mis32 = np.array([gpu_misfit(mods)])
+    g, mis64 = e.vjp_exact(40, moduli=True)
+    assert abs(mis64[:len(shots)].sum() / mis32[0] - 1) < 1e-5, (mis64, mis32)
+    assert np.isfinite(g).all() and all(np.abs(g[q]).max() > 0 for q in range(5))
+    with pytest.raises(ifosb.IfosbError):
+        e.vjp_exact(40)  # the (vp, vs, rho) form is elastic
+    for d in _directions(rng, 4, 5):
+        plus, minus, half = _pm(mods, d, 1e-5)
+        fd = (exact_misfit(plus) - exact_misfit(minus)) / 2
+        dot = sum(float((gq * hq).sum()) for gq, hq in zip(g, half))
+        print(f"L=3 FP64 misfit: <g,d> {dot:.12e} FD {fd:.12e} rel {abs(dot - fd) / abs(fd):.2e}")
+        assert abs(dot - fd) <= 1e-6 * abs(fd)
+    for d in _directions(rng, 6, 5):
+        plus, minus, half = _pm(mods, d, 1e-3)
+        fd = (gpu_misfit(plus) - gpu_misfit(minus)) / 2
+        dot = sum(float((gq * hq).sum()) for gq, hq in zip(g, half))
+        print(f"L=3 FP32 misfit: <g,d> {dot:.6e} FD {fd:.6e} rel {abs(dot - fd) / abs(fd):.2e}")
+        assert abs(dot - fd) <= 1e-3 * abs(fd)
+    e.close()
+
+
 def test_exact_vjp_preconditions():
     c = synth.small_case(nx=20, ny=18, nz=20, nt=30, fw=4, nmech=1, nshots=1, seed=3)
     from helpers import engine_for
@@ -148,7 +204,9 @@ def test_exact_vjp_preconditions():
     syn = e.forward(shots)
     e.residual(syn * 0.5)
     with pytest.raises(ifosb.IfosbError):
-        e.vjp_exact(5)  # viscoelastic: the transposes are elastic
+        e.vjp_exact(5)  # viscoelastic: velocities need the reference frequency; the moduli form
+    g, mis = e.vjp_exact(5, moduli=True)
+    assert g.shape == (5, 18, 20, 20) and np.abs(g[3:]).max() > 0 and mis[0] > 0
     e.close()
     c = synth.small_case(nx=20, ny=18, nz=20, nt=30, fw=4, nmech=0, nshots=1, seed=3)
     e, m, cp, shots = engine_for(c)
@@ -162,6 +220,8 @@ def test_exact_vjp_preconditions():
         e.vjp_exact(0)
     g, mis = e.vjp_exact(4)
     assert np.abs(g).max() > 0 and mis[0] > 0
+    gm, mis2 = e.vjp_exact(4, moduli=True)  # the moduli form of the same gradient
+    assert np.array_equal(mis, mis2) and not gm[3:].any()
     e.close()
 
 
