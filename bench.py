@@ -317,6 +317,9 @@ def main():
     ap.add_argument("--nshots", type=int, default=None, help="visco384 only: shots per step (profiling runs)")
     ap.add_argument("--shape", default=None,
                     help="launch shape cy_vel,l2_vel,cy_str,l2_str instead of autotuning (profiling runs)")
+    ap.add_argument("--td-interval", type=int, default=0,
+                    help="elastic128 only: the step is the time-domain gradient (forward with checkpoints every "
+                         "K steps, residual, ifosb_gradient_td) instead of the DFT shot-gradient")
     args = ap.parse_args()
     world, rank, local, dist = setup_dist(args)
     if args.impl == "reference":
@@ -348,6 +351,9 @@ def main():
     stream = torch.cuda.current_stream(dev)
 
     wl = args.workload
+    td_k = args.td_interval if wl == "elastic128" else 0
+    if td_k and dist:
+        raise SystemExit("--td-interval runs on one GPU")
     c = synth.case(wl, nt=args.nt)
     p = c["params"]
     # shot sharding: rank r models its own source position (a shifted copy of the case's shot)
@@ -390,9 +396,16 @@ def main():
     else:
         tuned = eng.autotune(shots, steps=min(60, p.nt))
 
+    if td_k:
+        eng.set_td_checkpoints(td_k)
+
     def step():
         if wl == "elastic128" and dist:
             distributed_shot_gradient(eng, all_shots, all_obs, max_batch=1, dist=dist)
+        elif td_k:
+            eng.forward(shots, want_sections=False)
+            eng.residual(obs)
+            eng.gradient_td(td_k)
         elif wl == "elastic128":
             eng.shot_gradient(shots, obs)
         else:
@@ -423,6 +436,11 @@ def main():
     # our kernels per step: 2 per time step (velocity, stress); a shot-gradient adds the
     # adjoint loop, residual + misfit and the gradient kernel
     launches = args.steps * (2 * p.nt if wl == "visco256" else 4 * p.nt + 3)
+    if td_k:
+        # forward 2 NT + NT sums; residual 2; recomputed steps 2 last + last sums, adjoint
+        # 2 NT + NT sums, last correlations, one dc kernel (last = TIME/DT - 1)
+        last = round(float(p.time) / float(p.dt)) - 1
+        launches = args.steps * (3 * p.nt + 2 + 3 * last + 3 * p.nt + last + 1)
     value = world * cells_step * args.steps / (ms / 1000.0) / 1e9
 
     # ---- end to end through the public API: host model + wavelet in, traces out, every step
@@ -439,7 +457,11 @@ def main():
     for _ in range(args.steps):
         eng.set_model(*[None if hm[k] is None else hm[k].numpy() for k in ("rho", "pi", "u", "taus", "taup")],
                       m["eta"], ghosted=True)
-        if wl == "elastic128":
+        if td_k:
+            eng.forward([(sp, sig_pinned.numpy())], want_sections=False)
+            eng.residual(obs)
+            eng.gradient_td(td_k)
+        elif wl == "elastic128":
             eng.shot_gradient([(sp, sig_pinned.numpy())], obs)
             eng.get_gradient()
         else:
@@ -454,6 +476,9 @@ def main():
     e2e = world * cells_step * args.steps / (ms_e2e / 1000.0) / 1e9
     if wl == "elastic128":
         d2h = 3 * eng.ntr * eng.ns * 4 + 3 * p.nx * p.ny * p.nz * 4
+    if td_k:
+        h2d += obs.nbytes
+        d2h = 4 * p.nx * p.ny * p.nz * 8 + 8  # the four FP64 kernels and the misfit
 
     # ---- roofline: per-kernel CUDA events on the launching stream over one profiled step
     eng.set_profiling(True)
@@ -494,12 +519,17 @@ def main():
     }
     if wl == "elastic128":
         out["shot_gradients_per_s"] = round(world * args.steps / (ms / 1000.0), 4)
+    if td_k:
+        out["config"]["gradient"] = (f"time-domain kernels (ifosb_gradient_td, interval {td_k}, checkpoints kept by "
+                                     "the forward) instead of the DFT shot-gradient")
 
     # ---- extras (rank 0, one GPU): batched vs one-shot-per-launch shot-gradients of elastic128
-    if rank == 0 and world == 1 and not args.no_extras:
+    if rank == 0 and world == 1 and not args.no_extras and not td_k:
         eng.close()
         out["shot_gradients"] = shot_gradient_comparison(torch, ifosb, synth, dev, stream, args.nt)
         out["shot_gradients_small_grid"] = small_grid_comparison(torch, ifosb, synth, dev, stream, args.nt)
+        if wl == "elastic128":
+            out["time_domain_gradient"] = time_domain_comparison(torch, ifosb, synth, dev, stream, args.nt)
     # ---- CPU baseline (rank 0, N=1): the oracle on a bounded sample of this workload
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline_line(wl, args)
@@ -904,6 +934,54 @@ def multiscale_workload(args, local):
                       "seconds": round(t_total, 2)},
     }
     print(json.dumps(out), flush=True)
+
+
+def time_domain_comparison(torch, ifosb, synth, dev, stream, nt_override, interval=50, reps=2):
+    """One elastic128 shot-gradient by the DFT path (forward + residual + adjoint +
+    gradient_F at the case's 2 frequencies) against the time-domain path (forward
+    keeping checkpoints every `interval` steps + residual + ifosb_gradient_td),
+    elastic and L=3 (Q=50 over 20-200 Hz): seconds per shot-gradient, CUDA events
+    over `reps` repetitions after one warm-up each."""
+    out = {"interval": interval}
+    for nmech in (0, 3):
+        c = synth.case("elastic128", nt=nt_override)
+        p = c["params"]
+        if nmech:
+            p.nmech = 3
+            c["tau"], c["fl"] = synth.q_tau_fit(50.0, 20.0, 200.0, 3)
+        m, cp, shots = synth.build_inputs(c)
+        e = ifosb.Engine(p, max_shots=1, max_nf=2)
+        e.set_stream(stream.cuda_stream)
+        e.set_cpml(cp)
+        e.set_model(m["rho"], m["pi"], m["u"], m["taus"], m["taup"], m["eta"])
+        e.set_receivers(c["recpos"])
+        e.set_frequencies(c["finv"], c["ntast"])
+        obs = (0.9 * e.forward(shots)).astype(np.float32)
+
+        def dft():
+            e.shot_gradient(shots, obs)
+
+        def td():
+            e.forward(shots, want_sections=False)
+            e.residual(obs)
+            e.gradient_td(interval)
+
+        res = {}
+        for name, fn in (("dft_s", dft), ("time_domain_s", td)):
+            e.set_td_checkpoints(interval if name == "time_domain_s" else 0)
+            fn()
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize(dev)
+            ev0.record(stream)
+            for _ in range(reps):
+                fn()
+            ev1.record(stream)
+            torch.cuda.synchronize(dev)
+            res[name] = round(ev0.elapsed_time(ev1) / 1000.0 / reps, 4)
+        res["ratio"] = round(res["time_domain_s"] / res["dft_s"], 3)
+        out[f"nmech{nmech}"] = res
+        e.close()
+    return out
 
 
 def shot_gradient_comparison(torch, ifosb, synth, dev, stream, nt_override, nshots=4):

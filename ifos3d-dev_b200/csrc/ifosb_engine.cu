@@ -122,6 +122,14 @@ struct ifosb_engine {
     // time-domain mode's checkpoint/segment block and kernels, kept between calls
     float *d_td_blk = nullptr; size_t cap_td_blk = 0;
     double *d_td_k = nullptr; size_t cap_td_k = 0;
+    // checkpoints the forward itself writes for the time-domain mode
+    // (ifosb_set_td_checkpoints): the interval asked for, and the batch whose
+    // checkpoints the block holds
+    int td_arm = 0;
+    bool td_ck_ok = false;
+    int td_ck_K = 0, td_ck_nshots = 0;
+    cudaError_t hook_err = cudaSuccess;
+    GraphSet gtd;  // time-domain loops, one graph per batch shape and interval
     // TMA staging (default) and its wait-timeout flag; the failure-path test knobs
     int use_tma = 1;
     int *d_tma_err = nullptr;
@@ -348,6 +356,7 @@ extern "C" void ifosb_destroy(ifosb_engine *e) {
     if (e->stream) cudaStreamSynchronize(e->stream);
     release_graph(e->gfwd);
     release_graph(e->gadj);
+    release_graph(e->gtd);
     void *bufs[] = {e->d_state, e->d_psi, e->d_model, e->d_rho_w, e->d_dftf, e->d_dftb, e->d_grad, e->d_grad64,
                     e->d_err, e->d_sec, e->d_diff, e->d_obs, e->d_part, e->d_misfit, e->d_l2, e->d_trig_f,
                     e->d_trig_b, e->d_voff, e->d_soff, e->d_vpts, e->d_spts, e->d_amp, e->d_tma_err, e->d_cpg,
@@ -394,6 +403,7 @@ extern "C" int ifosb_set_stream(ifosb_engine *e, void *stream) {
     e->stream = stream ? (cudaStream_t)stream : e->own_stream;
     release_graph(e->gfwd);
     release_graph(e->gadj);
+    release_graph(e->gtd);
     return IFOSB_OK;
 }
 
@@ -560,6 +570,7 @@ extern "C" int ifosb_set_receivers(ifosb_engine *e, int ntr, const int *recpos) 
     e->fwd_ok = e->res_ok = e->adj_ok = false;
     release_graph(e->gfwd);
     release_graph(e->gadj);
+    release_graph(e->gtd);
     CU(cudaStreamSynchronize(e->stream));
     return IFOSB_OK;
 }
@@ -603,6 +614,7 @@ extern "C" int ifosb_set_frequencies(ifosb_engine *e, int nf, const float *finv,
     e->fwd_ok = e->res_ok = e->adj_ok = false;
     release_graph(e->gfwd);
     release_graph(e->gadj);
+    release_graph(e->gtd);
     return IFOSB_OK;
 }
 
@@ -612,6 +624,15 @@ extern "C" int ifosb_set_frequencies(ifosb_engine *e, int nf, const float *finv,
 static_assert(TZ == BX, "TMA tiles and plain blocks share one block geometry along z");
 
 // Everything one forward or adjoint call launches with.
+// The time-domain checkpoints an armed forward writes after its steps: the
+// running sums U += v DT, a checkpoint (state, PML memory, U) after steps K, 2K,
+// ..., and U at NT (K = 0: none).
+struct TdHook {
+    float *uf, *uf_end, *ckp;
+    size_t ck, ss, ps, us, ssz, psz;
+    int K, nseg;
+};
+
 struct Loop {
     Geo lg;   // launch geometry of the stress kernel (the y chunking depends on the batch size)
     Geo lgv;  // launch geometry of the velocity kernel
@@ -624,6 +645,7 @@ struct Loop {
     bool tma = false;
     bool p2 = false;  // power-of-two spacings (stress kernel multiplies by 1/DX etc.)
     size_t vel_smem = 0, str_smem = 0;
+    TdHook td;
 };
 
 // The launch shape for a batch of nshots: the autotuner's for that batch size,
@@ -900,6 +922,59 @@ static void step_flags(const ifosb_engine *e, bool back, int nt, int &lsamp, int
     }
 }
 
+// The time-domain block of a batch: state2 | psi2 | Uf | Ub | Uf(NT) | checkpoints
+// 1..nseg-1 | segment, each sub-buffer 256-byte aligned. The adjoint's step m
+// stands at time TIME - m DT (discfourier's backward phase), so forward step n
+// meets it at zero lag when n + m = P = TIME / DT (nearest whole step); forward
+// steps 1..P-1 pair with an adjoint step, in segments of K steps. False when P is
+// out of range.
+struct TdLayout {
+    int P, K, last, nseg;
+    size_t ssz, psz, ss, ps, us, ck, seg_shot, total;
+};
+static bool td_layout(const ifosb_engine *e, int nshots, int interval, TdLayout &t) {
+    const ifosb_params &p = e->p;
+    t.P = (int)std::lround((double)p.time / (double)p.dt);
+    if (t.P < 2 || t.P > p.nt + 1) return false;
+    auto al = [](size_t v) { return (v + 63) & ~(size_t)63; };
+    const long long F = e->g.field;
+    t.K = std::min(interval, t.P - 1);
+    t.last = t.P - 1;
+    t.nseg = (t.last + t.K - 1) / t.K;  // segment q covers steps q*K+1 .. min((q+1)*K, last)
+    t.ssz = (size_t)e->st_shot * nshots;
+    t.psz = (size_t)e->psi_shot * nshots;
+    t.ss = al(t.ssz);
+    t.ps = al(t.psz);
+    t.us = al((size_t)3 * F * nshots);
+    t.ck = t.ss + t.ps + t.us;        // one checkpoint: state, PML memory, running sums
+    t.seg_shot = (size_t)6 * F;       // one step of a segment: v and running sums
+    t.total = t.ss + t.ps + 3 * t.us + (size_t)(t.nseg - 1) * t.ck + (size_t)t.K * t.seg_shot * nshots;
+    return true;
+}
+
+static void td_integrate(ifosb_engine *e, int nshots, float *u, const float *st, float *seg, size_t seg_shot) {
+    k_td_integrate<<<dim3(2 * 148, nshots), 256, 0, e->stream>>>(u, st, e->st_shot, e->g.field, nshots, e->p.dt, seg,
+                                                                 (long long)seg_shot);
+}
+
+static void hook_copy(ifosb_engine *e, void *dst, const void *src, size_t words) {
+    const cudaError_t r = cudaMemcpyAsync(dst, src, words * sizeof(float), cudaMemcpyDeviceToDevice, e->stream);
+    if (r != cudaSuccess && e->hook_err == cudaSuccess) e->hook_err = r;
+}
+
+// after forward step nt of an armed forward (the engine's own state)
+static void td_hook(ifosb_engine *e, const Loop &L, int nt) {
+    const TdHook &t = L.td;
+    td_integrate(e, L.nshots, t.uf, e->d_state, nullptr, 0);
+    if (nt % t.K == 0 && nt / t.K < t.nseg) {
+        float *c = t.ckp + (size_t)(nt / t.K - 1) * t.ck;
+        hook_copy(e, c, e->d_state, t.ssz);
+        hook_copy(e, c + t.ss, e->d_psi, t.psz);
+        hook_copy(e, c + t.ss + t.ps, t.uf, t.us);
+    }
+    if (nt == e->p.nt) hook_copy(e, t.uf_end, t.uf, t.us);
+}
+
 // Enqueue the NT steps (two kernels per step) on the engine stream.
 static void enqueue_loop(ifosb_engine *e, const Loop &L) {
     const ifosb_params &p = e->p;
@@ -910,6 +985,7 @@ static void enqueue_loop(ifosb_engine *e, const Loop &L) {
         int do_dft, sample;
         step_flags(e, L.back, nt, lsamp, nlsamp, do_dft, sample);
         launch_str(p.nmech, L, grd, e->stream, nt, do_dft, sample);
+        if (L.td.K) td_hook(e, L, nt);
     }
 }
 
@@ -934,6 +1010,7 @@ static int run_loop_profiled(ifosb_engine *e, const Loop &L) {
         step_flags(e, L.back, nt, lsamp, nlsamp, do_dft, sample);
         launch_str(p.nmech, L, grd, e->stream, nt, do_dft, sample);
         CU(cudaEventRecord(ev[2], e->stream));
+        if (L.td.K) td_hook(e, L, nt);
     }
     int rc = check_launch(e, "time loop");
     if (rc) return rc;
@@ -953,16 +1030,10 @@ static int run_loop_profiled(ifosb_engine *e, const Loop &L) {
     return IFOSB_OK;
 }
 
-static int run_loop(ifosb_engine *e, const Loop &L) {
-    GraphSet &gs = L.back ? e->gadj : e->gfwd;
-    e->launches = 2LL * e->p.nt;
-    if (e->profile) return run_loop_profiled(e, L);
-    if (e->launch_mode == 1) {
-        enqueue_loop(e, L);
-        return check_launch(e, "time loop");
-    }
-    std::vector<unsigned char> key(sizeof(Loop));
-    std::memcpy(key.data(), &L, sizeof(Loop));
+// Replays the graph of `key` from the set, or captures `enqueue` into the least
+// recently used slot and replays that.
+template <class Fn>
+static int replay_graph(ifosb_engine *e, GraphSet &gs, const std::vector<unsigned char> &key, Fn enqueue) {
     GraphCache *hit = nullptr, *lru = &gs.g[0];
     for (GraphCache &c : gs.g) {
         if (c.exec && c.key == key) hit = &c;
@@ -975,7 +1046,7 @@ static int run_loop(ifosb_engine *e, const Loop &L) {
         release_graph(gc);
         cudaGraph_t graph = nullptr;
         CU(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
-        enqueue_loop(e, L);
+        enqueue();
         cudaError_t ce = cudaStreamEndCapture(e->stream, &graph);
         if (ce != cudaSuccess) {
             cudaGetLastError();
@@ -993,6 +1064,19 @@ static int run_loop(ifosb_engine *e, const Loop &L) {
     }
     CU(cudaGraphLaunch(gc.exec, e->stream));
     return IFOSB_OK;
+}
+
+static int run_loop(ifosb_engine *e, const Loop &L) {
+    GraphSet &gs = L.back ? e->gadj : e->gfwd;
+    e->launches = 2LL * e->p.nt;
+    if (e->profile) return run_loop_profiled(e, L);
+    if (e->launch_mode == 1) {
+        enqueue_loop(e, L);
+        return check_launch(e, "time loop");
+    }
+    std::vector<unsigned char> key(sizeof(Loop));
+    std::memcpy(key.data(), &L, sizeof(Loop));
+    return replay_graph(e, gs, key, [&]() { enqueue_loop(e, L); });
 }
 
 static int check_unstable(ifosb_engine *e, int nshots) {
@@ -1091,10 +1175,27 @@ extern "C" int ifosb_forward(ifosb_engine *e, int nshots, const ifosb_shot *shot
     sa.trig = e->d_trig_f;
     L.tma = e->use_tma && setup_tma(e, L, e->d_dftf);
     e->fwd_ok = e->res_ok = e->adj_ok = e->hess_fwd = false;
+    e->td_ck_ok = false;
+    TdLayout tl;
+    if (e->td_arm > 0 && e->nt_limit == 0 && td_layout(e, nshots, e->td_arm, tl)) {
+        // checkpoints for ifosb_gradient_td, written by this forward (the whole loop runs)
+        if ((rc = dgrow(e, &e->d_td_blk, &e->cap_td_blk, tl.total))) return rc;
+        float *uf = e->d_td_blk + tl.ss + tl.ps, *uf_end = uf + 2 * tl.us;
+        L.td = TdHook{uf, uf_end, uf_end + tl.us, tl.ck, tl.ss, tl.ps, tl.us, tl.ssz, tl.psz, tl.K, tl.nseg};
+        CU(cudaMemsetAsync(uf, 0, tl.us * sizeof(float), e->stream));
+    }
+    e->hook_err = cudaSuccess;
     if ((rc = run_loop(e, L))) return rc;
+    if (e->hook_err != cudaSuccess)
+        return fail(e, IFOSB_ECUDA, std::string("time-domain checkpoints: ") + cudaGetErrorString(e->hook_err));
     e->nshots = nshots;
     if ((rc = check_unstable(e, nshots))) return rc;  // a failed batch is not a forward to build on
     e->fwd_ok = true;
+    if (L.td.K) {
+        e->td_ck_ok = true;
+        e->td_ck_K = L.td.K;
+        e->td_ck_nshots = nshots;
+    }
     e->hess_fwd = e->nf > 0;
     if (sections && e->ntr > 0) {
         // [shot][component][ntr][ns] in saveseis's order: vx vy vz (1), p (2), div curl (3), all six (4)
@@ -1226,15 +1327,24 @@ extern "C" int ifosb_gradient(ifosb_engine *e) {
 
 // ---------------------------------------------------------------------------
 // Time-domain gradient kernels with checkpointing: the forward batch is run again
-// with its state saved every `interval` steps; the adjoint then runs forward in
-// its own time, and for each adjoint step the forward step it pairs with is
-// recomputed segment by segment from the nearest checkpoint (segments taken in
-// reverse). Memory: one state per checkpoint plus one segment of velocities,
-// instead of the whole time history. Plain launches, no DFT, no traces.
+// with its state saved every `interval` steps (or the checkpoints the forward
+// wrote itself, ifosb_set_td_checkpoints, are taken); the adjoint then runs
+// forward in its own time, and for each adjoint step the forward step it pairs
+// with is recomputed segment by segment from the nearest checkpoint (segments
+// taken in reverse). Memory: one state per checkpoint plus one segment of
+// velocities, instead of the whole time history. No DFT, no traces; the loops of
+// a call are one CUDA graph per batch shape and interval.
 static void td_step(ifosb_engine *e, const Loop &L, int nt) {
     const dim3 grd(L.lg.ntk, L.lg.nti, L.lg.nyc * L.nshots), grdv(L.lgv.ntk, L.lgv.nti, L.lgv.nyc * L.nshots);
     launch_vel(L, grdv, e->stream, nt);
     launch_str(e->p.nmech, L, grd, e->stream, nt, 0, -1);
+}
+
+extern "C" int ifosb_set_td_checkpoints(ifosb_engine *e, int interval) {
+    if (!e || interval < 0) return IFOSB_EARG;
+    e->td_arm = interval;
+    e->td_ck_ok = false;
+    return IFOSB_OK;
 }
 
 extern "C" int ifosb_gradient_td(ifosb_engine *e, int interval, double *kernels) {
@@ -1242,24 +1352,18 @@ extern "C" int ifosb_gradient_td(ifosb_engine *e, int interval, double *kernels)
     const ifosb_params &p = e->p;
     if (!e->fwd_ok || !e->res_ok) return fail(e, IFOSB_ESTATE, "the time-domain gradient needs a forward batch and its residual");
     if (p.ndt != 1 || p.ndtshift != 0) return fail(e, IFOSB_EARG, "the adjoint indexes the residual by step: NDT=1, NDTSHIFT=0");
-    // The adjoint's step m stands at time TIME - m DT (discfourier's backward phase), so
-    // forward step n meets it at zero lag when n + m = P = TIME / DT (nearest whole step).
-    const int NT = p.nt, P = (int)std::lround((double)p.time / (double)p.dt);
-    if (P < 2 || P > NT + 1) return fail(e, IFOSB_EARG, "TIME / DT must lie between 2 and NT + 1 steps");
-    const int nshots = e->nshots, K = std::min(interval, P - 1);
+    const int NT = p.nt, nshots = e->nshots;
+    TdLayout t;
+    if (!td_layout(e, nshots, interval, t)) return fail(e, IFOSB_EARG, "TIME / DT must lie between 2 and NT + 1 steps");
+    const int K = t.K, last = t.last, nseg = t.nseg;
     const long long F = e->g.field, n = (long long)p.nx * p.ny * p.nz;
-    auto al = [](size_t v) { return (v + 63) & ~(size_t)63; };  // 256-byte sub-buffers
-    const size_t ssz = (size_t)e->st_shot * nshots, psz = (size_t)e->psi_shot * nshots;  // the batch's words
-    const size_t ss = al(ssz), ps = al(psz), us = al((size_t)3 * F * nshots);
-    const int last = P - 1;                   // forward steps that pair with an adjoint step: 1..P-1
-    const int nseg = (last + K - 1) / K;      // segment q covers steps q*K+1 .. min((q+1)*K, last)
-    const size_t ck = ss + ps + us;           // one checkpoint: state, PML memory, running sums
-    const size_t seg_shot = (size_t)6 * F;    // one step of a segment: v and running sums
-    // one device block: state2 | psi2 | Uf | Ub | Uf(NT) | checkpoints 1..nseg-1 | segment
-    const size_t total = ss + ps + 3 * us + (size_t)(nseg - 1) * ck + (size_t)K * seg_shot * nshots;
-    // grow-only blocks kept by the engine: a repeated call allocates nothing
+    const size_t ss = t.ss, ps = t.ps, us = t.us, ck = t.ck, seg_shot = t.seg_shot;
+    // the last forward's own checkpoints at this interval spare the re-run (the
+    // block is grow-only: it still holds them when it is large enough)
+    const bool have_ck = e->td_ck_ok && e->td_ck_K == K && e->td_ck_nshots == nshots && e->d_td_blk &&
+                         e->cap_td_blk >= t.total;
     int grc;
-    if ((grc = dgrow(e, &e->d_td_blk, &e->cap_td_blk, total)) || (grc = dgrow(e, &e->d_td_k, &e->cap_td_k, (size_t)4 * n)))
+    if ((grc = dgrow(e, &e->d_td_blk, &e->cap_td_blk, t.total)) || (grc = dgrow(e, &e->d_td_k, &e->cap_td_k, (size_t)4 * n)))
         return grc;
     float *blk = e->d_td_blk;
     double *dk = e->d_td_k;
@@ -1267,7 +1371,6 @@ extern "C" int ifosb_gradient_td(ifosb_engine *e, int interval, double *kernels)
     float *segb = ckp + (size_t)(nseg - 1) * ck;
     int rc = IFOSB_OK;
     auto run = [&]() -> int {
-        CU(cudaMemsetAsync(dk, 0, (size_t)4 * n * sizeof(double), e->stream));
         // the recomputation loop: the last forward's sources on its own state
         Loop Lf;
         std::memset(static_cast<void *>(&Lf), 0, sizeof(Lf));
@@ -1310,8 +1413,8 @@ extern "C" int ifosb_gradient_td(ifosb_engine *e, int interval, double *kernels)
         La.lgv = launch_geo(e, nshots, true);
         std::vector<HostPt> va;
         for (int sh = 0; sh < nshots; ++sh)
-            for (int t = 0; t < e->ntr; ++t)
-                va.push_back({sh, e->rec[3 * t + 1], e->rec[3 * t], e->rec[3 * t + 2], PT_ADJOINT, sh * 3 * e->ntr + t});
+            for (int tr = 0; tr < e->ntr; ++tr)
+                va.push_back({sh, e->rec[3 * tr + 1], e->rec[3 * tr], e->rec[3 * tr + 2], PT_ADJOINT, sh * 3 * e->ntr + tr});
         if ((r = upload_points(e, La.lgv, nshots, va, &e->d_voff_a, &e->cap_voff_a, &e->d_vpts_a, &e->cap_vpts_a))) return r;
         fill_common(e, La);
         La.va.pt_off = va.empty() ? nullptr : e->d_voff_a;
@@ -1320,39 +1423,8 @@ extern "C" int ifosb_gradient_td(ifosb_engine *e, int interval, double *kernels)
         La.va.val_row = e->ns;
         La.va.val_comp = (long long)e->ntr * e->ns;
         La.tma = e->use_tma && setup_tma(e, La, nullptr);
-        const int nb = 2 * 148, tb = 256;
-        const dim3 grd_c((p.nz + BX - 1) / BX, (p.nx + BY - 1) / BY, p.ny);
-        auto integrate = [&](float *u, const float *st, float *seg) {
-            k_td_integrate<<<dim3(nb, nshots), tb, 0, e->stream>>>(u, st, e->st_shot, F, nshots, p.dt, seg,
-                                                                   (long long)seg_shot);
-        };
-        // 1. the forward again, saving a checkpoint after steps K, 2K, ... and the sums at NT
-        CU(cudaMemsetAsync(st2, 0, ss * sizeof(float), e->stream));
-        CU(cudaMemsetAsync(psi2, 0, ps * sizeof(float), e->stream));
-        CU(cudaMemsetAsync(uf, 0, us * sizeof(float), e->stream));
-        {
-            std::vector<int> init(nshots, INT_MAX);
-            CU(cudaMemcpyAsync(e->d_err, init.data(), sizeof(int) * nshots, cudaMemcpyHostToDevice, e->stream));
-            CU(cudaMemsetAsync(e->d_tma_err, 0, sizeof(int), e->stream));
-            CU(cudaStreamSynchronize(e->stream));  // init lives on the host stack
-        }
-        for (int nt = 1; nt <= NT; ++nt) {
-            td_step(e, Lf, nt);
-            integrate(uf, st2, nullptr);
-            if (nt % K == 0 && nt / K < nseg) {
-                float *c = ckp + (size_t)(nt / K - 1) * ck;
-                CU(cudaMemcpyAsync(c, st2, ss * sizeof(float), cudaMemcpyDeviceToDevice, e->stream));
-                CU(cudaMemcpyAsync(c + ss, psi2, ps * sizeof(float), cudaMemcpyDeviceToDevice, e->stream));
-                CU(cudaMemcpyAsync(c + ss + ps, uf, us * sizeof(float), cudaMemcpyDeviceToDevice, e->stream));
-            }
-        }
-        CU(cudaMemcpyAsync(uf_end, uf, us * sizeof(float), cudaMemcpyDeviceToDevice, e->stream));
-        if ((r = check_launch(e, "time-domain forward"))) return r;
-        // 2. the adjoint, with each segment of forward steps recomputed as it is reached
-        CU(cudaMemsetAsync(e->d_state, 0, ssz * sizeof(float), e->stream));
-        CU(cudaMemsetAsync(e->d_psi, 0, psz * sizeof(float), e->stream));
-        CU(cudaMemsetAsync(ub, 0, us * sizeof(float), e->stream));
-        TdArgs ta{};
+        TdArgs ta;
+        std::memset(static_cast<void *>(&ta), 0, sizeof(ta));  // part of the graph key, padding included
         ta.g = e->g;
         ta.st = e->d_state;
         ta.st_shot = e->st_shot;
@@ -1362,42 +1434,96 @@ extern "C" int ifosb_gradient_td(ifosb_engine *e, int interval, double *kernels)
         ta.b1 = e->b1; ta.b2 = e->b2;
         ta.rdx = p.dx; ta.rdy = p.dy; ta.rdz = p.dz;
         ta.k = dk;
-        int ntb = 1;  // next adjoint step
-        for (int q = nseg - 1; q >= 0; --q) {
-            const int a0 = q * K + 1, a1 = std::min((q + 1) * K, last);
-            if (q == 0) {
-                CU(cudaMemsetAsync(st2, 0, ss * sizeof(float), e->stream));
-                CU(cudaMemsetAsync(psi2, 0, ps * sizeof(float), e->stream));
-                CU(cudaMemsetAsync(uf, 0, us * sizeof(float), e->stream));
-            } else {
-                const float *c = ckp + (size_t)(q - 1) * ck;
-                CU(cudaMemcpyAsync(st2, c, ss * sizeof(float), cudaMemcpyDeviceToDevice, e->stream));
-                CU(cudaMemcpyAsync(psi2, c + ss, ps * sizeof(float), cudaMemcpyDeviceToDevice, e->stream));
-                CU(cudaMemcpyAsync(uf, c + ss + ps, us * sizeof(float), cudaMemcpyDeviceToDevice, e->stream));
+        {
+            std::vector<int> init(nshots, INT_MAX);
+            CU(cudaMemcpyAsync(e->d_err, init.data(), sizeof(int) * nshots, cudaMemcpyHostToDevice, e->stream));
+            CU(cudaMemsetAsync(e->d_tma_err, 0, sizeof(int), e->stream));
+            CU(cudaStreamSynchronize(e->stream));  // init lives on the host stack
+        }
+        const int nb = 2 * 148, tb = 256;
+        const dim3 grd_c((p.nz + BX - 1) / BX, (p.nx + BY - 1) / BY, p.ny);
+        auto integrate = [&](float *u, const float *st, float *seg) { td_integrate(e, nshots, u, st, seg, seg_shot); };
+        auto enqueue = [&]() {
+            cudaMemsetAsync(dk, 0, (size_t)4 * n * sizeof(double), e->stream);
+            if (!have_ck) {
+                // 1. the forward again, a checkpoint after steps K, 2K, ... and the sums at NT
+                cudaMemsetAsync(st2, 0, ss * sizeof(float), e->stream);
+                cudaMemsetAsync(psi2, 0, ps * sizeof(float), e->stream);
+                cudaMemsetAsync(uf, 0, us * sizeof(float), e->stream);
+                for (int nt = 1; nt <= NT; ++nt) {
+                    td_step(e, Lf, nt);
+                    integrate(uf, st2, nullptr);
+                    if (nt % K == 0 && nt / K < nseg) {
+                        float *c = ckp + (size_t)(nt / K - 1) * ck;
+                        hook_copy(e, c, st2, ss);
+                        hook_copy(e, c + ss, psi2, ps);
+                        hook_copy(e, c + ss + ps, uf, us);
+                    }
+                }
+                hook_copy(e, uf_end, uf, us);
             }
-            for (int m = a0; m <= a1; ++m) {  // v and U of each step go to the segment in the same pass
-                td_step(e, Lf, m);
-                integrate(uf, st2, segb + (size_t)(m - a0) * seg_shot * nshots);
+            // 2. the adjoint, with each segment of forward steps recomputed as it is reached
+            cudaMemsetAsync(e->d_state, 0, t.ssz * sizeof(float), e->stream);
+            cudaMemsetAsync(e->d_psi, 0, t.psz * sizeof(float), e->stream);
+            cudaMemsetAsync(ub, 0, us * sizeof(float), e->stream);
+            int ntb = 1;  // next adjoint step
+            for (int q = nseg - 1; q >= 0; --q) {
+                const int a0 = q * K + 1, a1 = std::min((q + 1) * K, last);
+                if (q == 0) {
+                    cudaMemsetAsync(st2, 0, ss * sizeof(float), e->stream);
+                    cudaMemsetAsync(psi2, 0, ps * sizeof(float), e->stream);
+                    cudaMemsetAsync(uf, 0, us * sizeof(float), e->stream);
+                } else {
+                    const float *c = ckp + (size_t)(q - 1) * ck;
+                    hook_copy(e, st2, c, ss);
+                    hook_copy(e, psi2, c + ss, ps);
+                    hook_copy(e, uf, c + ss + ps, us);
+                }
+                for (int m = a0; m <= a1; ++m) {  // v and U of each step go to the segment in the same pass
+                    td_step(e, Lf, m);
+                    integrate(uf, st2, segb + (size_t)(m - a0) * seg_shot * nshots);
+                }
+                for (int m = a1; m >= a0; --m, ++ntb) {  // adjoint steps P-a1 .. P-a0, in order
+                    td_step(e, La, ntb);
+                    integrate(ub, e->d_state, nullptr);
+                    ta.seg = segb + (size_t)(m - a0) * seg_shot * nshots;
+                    k_td_corr<<<grd_c, dim3(BX, BY), 0, e->stream>>>(ta);
+                }
             }
-            for (int m = a1; m >= a0; --m, ++ntb) {  // adjoint steps P-a1 .. P-a0, in order
+            for (; ntb <= NT; ++ntb) {  // adjoint steps past P-1 meet forward steps before the first (zero)
                 td_step(e, La, ntb);
                 integrate(ub, e->d_state, nullptr);
-                ta.seg = segb + (size_t)(m - a0) * seg_shot * nshots;
-                k_td_corr<<<grd_c, dim3(BX, BY), 0, e->stream>>>(ta);
             }
-            if ((r = check_launch(e, "time-domain adjoint"))) return r;
+            k_td_dc<<<nb, tb, 0, e->stream>>>(ta, uf_end);
+        };
+        e->hook_err = cudaSuccess;
+        if (e->launch_mode == 1 || e->profile) {
+            enqueue();
+        } else {
+            // the graph key: both loops, the kernels' arguments and the schedule
+            std::vector<unsigned char> key(2 * sizeof(Loop) + sizeof(TdArgs) + 64);
+            unsigned char *kp = key.data();
+            std::memcpy(kp, &Lf, sizeof(Loop)); kp += sizeof(Loop);
+            std::memcpy(kp, &La, sizeof(Loop)); kp += sizeof(Loop);
+            std::memcpy(kp, &ta, sizeof(TdArgs)); kp += sizeof(TdArgs);
+            const long long sched[8] = {K, nseg, last, NT, have_ck ? 1 : 0, (long long)(uintptr_t)blk, nshots, 0};
+            std::memcpy(kp, sched, sizeof(sched));
+            if ((r = replay_graph(e, e->gtd, key, enqueue))) return r;
         }
-        for (; ntb <= NT; ++ntb) {  // adjoint steps past P-1 meet forward steps before the first (zero)
-            td_step(e, La, ntb);
-            integrate(ub, e->d_state, nullptr);
-        }
-        k_td_dc<<<nb, tb, 0, e->stream>>>(ta, uf_end);
-        if ((r = check_launch(e, "time-domain kernels"))) return r;
+        if ((r = check_launch(e, "time-domain loops"))) return r;
+        if (e->hook_err != cudaSuccess)
+            return fail(e, IFOSB_ECUDA, std::string("time-domain copies: ") + cudaGetErrorString(e->hook_err));
         if ((r = check_unstable(e, nshots))) return r;
         CU(cudaMemcpyAsync(kernels, dk, (size_t)4 * n * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
         CU(cudaStreamSynchronize(e->stream));
+        // the checkpoints stay in the block (the segments only read them): a repeat
+        // call for this forward starts from them
+        e->td_ck_ok = true;
+        e->td_ck_K = K;
+        e->td_ck_nshots = nshots;
         return IFOSB_OK;
     };
+    e->td_ck_ok = false;  // a failure below leaves the block undefined
     rc = run();
     cudaStreamSynchronize(e->stream);
     return rc;
@@ -1974,6 +2100,7 @@ extern "C" int ifosb_autotune(ifosb_engine *e, int nshots, const ifosb_shot *sho
     e->tuned[nshots] = pick;
     release_graph(e->gfwd);
     release_graph(e->gadj);
+    release_graph(e->gtd);
     if (shape) {
         shape[0] = pick.cyv;
         shape[1] = pick.l2v;
@@ -1996,5 +2123,6 @@ extern "C" int ifosb_set_launch_shape(ifosb_engine *e, int nshots, const int *sh
     e->tuned[nshots] = {shape[0], shape[1], shape[2], shape[3]};
     release_graph(e->gfwd);
     release_graph(e->gadj);
+    release_graph(e->gtd);
     return IFOSB_OK;
 }

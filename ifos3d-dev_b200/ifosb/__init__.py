@@ -136,6 +136,7 @@ def lib():
             "ifosb_set_surface_moduli": (C.c_int, [vp, vp, vp]),
             "ifosb_vjp_exact": (C.c_int, [vp, C.c_int, vp, vp]),
             "ifosb_vjp_exact_moduli": (C.c_int, [vp, C.c_int, vp, vp]),
+            "ifosb_set_td_checkpoints": (C.c_int, [vp, C.c_int]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -160,7 +161,7 @@ def exported_symbols():
         "ifosb_write_model", "ifosb_write_gradient", "ifosb_filt_seis", "ifosb_hessian_green", "ifosb_hessian",
         "ifosb_zero_hessian", "ifosb_get_hessian", "ifosb_read_hessian", "ifosb_hess_apply", "ifosb_resample",
         "ifosb_set_seismo", "ifosb_gradient_td", "ifosb_get_gradient_q", "ifosb_set_wait_test",
-        "ifosb_set_surface_moduli", "ifosb_vjp_exact", "ifosb_vjp_exact_moduli",
+        "ifosb_set_surface_moduli", "ifosb_vjp_exact", "ifosb_vjp_exact_moduli", "ifosb_set_td_checkpoints",
     ]
 
 
@@ -423,6 +424,12 @@ class Engine:
         k = np.zeros((4, self.p.ny, self.p.nx, self.p.nz), np.float64)
         self._c(lib().ifosb_gradient_td(self.h, int(interval), _p(k)))
         return k
+
+    def set_td_checkpoints(self, interval):
+        """interval > 0: following forwards also keep the time-domain checkpoints of
+        that interval, so that gradient_td(interval) skips its re-run of the
+        forward; 0: off."""
+        self._c(lib().ifosb_set_td_checkpoints(self.h, int(interval)))
 
     def vjp_exact(self, interval=25, want_grad=True, moduli=False):
         """The exact discrete gradient of the misfit of the last forward batch and its

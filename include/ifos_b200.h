@@ -142,7 +142,9 @@ int ifosb_gradient(ifosb_engine *e);
 
 /* Time-domain gradient kernels of the last forward batch and its residual, with
  * checkpointing instead of the DFT: the forward is run again saving its state
- * every `interval` steps, the residual is back-propagated, and each forward step
+ * every `interval` steps (unless that forward saved them itself, see
+ * ifosb_set_td_checkpoints, or an earlier call for it did), the residual is
+ * back-propagated, and each forward step
  * is recomputed from the nearest checkpoint, one segment at a time, when its
  * zero-lag adjoint step (n + m = TIME/DT, the pairing of discfourier's phases,
  * src/disc_fourier.c:36-37) is reached. kernels[4][NY][NX][NZ] (FP64, summed over
@@ -158,6 +160,13 @@ int ifosb_gradient(ifosb_engine *e);
  * of six fields per shot. The DFT fields, traces and residual stay as they were;
  * the wavefield state (ifosb_get_field) is the time-domain adjoint's last step. */
 int ifosb_gradient_td(ifosb_engine *e, int interval, double *kernels);
+
+/* interval > 0: every following ifosb_forward also keeps the time-domain
+ * checkpoints of that interval (the running sums U and a state every `interval`
+ * steps, in the time-domain block) so that ifosb_gradient_td with the same
+ * interval skips its re-run of the forward; 0 turns it off. Costs the block's
+ * device memory and one extra pass over v per forward step. */
+int ifosb_set_td_checkpoints(ifosb_engine *e, int interval);
 
 /* Viscoelastic engines (nmech > 0): the accumulated FP64 gradients with respect
  * to the model's taup and taus (gradq[2][NY][NX][NZ]), summed like grad64 by

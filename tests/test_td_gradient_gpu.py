@@ -196,3 +196,39 @@ def test_time_domain_partial_batch():
         e.close()
     assert np.abs(out[0][0]).max() > 0
     assert np.array_equal(out[0], out[1])
+
+
+@pytest.mark.parametrize("nmech", [0, 3])
+def test_forward_checkpoints_and_graphs_change_no_bit(nmech):
+    """The checkpoints a forward keeps itself (ifosb_set_td_checkpoints), the
+    checkpoints an earlier call left, the captured graph and its replay, and
+    plain launches all give the kernels of a plain call bit for bit; arming the
+    forward changes no trace."""
+    c = synth.small_case(nx=20, ny=22, nz=18, nt=34, fw=4, nmech=nmech, nshots=2, seed=7, free_surf=1)
+    e, m, cp, shots = engine_for(c, max_shots=2, nf=1)
+    syn = e.forward(shots)
+    obs = (0.5 * np.roll(syn, 2, axis=-1)).astype(np.float32)
+
+    def fresh(interval, arm):
+        e.set_td_checkpoints(arm)
+        s = e.forward(shots)
+        e.residual(obs)
+        return s, e.gradient_td(interval)
+
+    e.set_launch_mode(1)
+    s0, k0 = fresh(4, 0)  # plain launches, the forward run again
+    e.set_launch_mode(0)
+    s1, k1 = fresh(4, 0)  # graph capture
+    c1 = e.graph_captures()
+    k1b = e.gradient_td(4)  # the checkpoints of the call before: no re-run
+    s2, k2 = fresh(4, 4)  # the forward's own checkpoints
+    k2b = e.gradient_td(4)
+    s3, k3 = fresh(4, 5)  # armed at another interval: run again
+    _, k4 = fresh(4, 0)  # replayed graph
+    assert np.abs(k0[0]).max() > 0
+    for k in (k1, k1b, k2, k2b, k3, k4):
+        assert np.array_equal(k, k0)
+    for s in (s1, s2, s3):
+        assert np.array_equal(s, s0)
+    assert e.graph_captures() > c1  # the armed forward and the no-re-run loops are graphs of their own
+    e.close()
