@@ -1297,6 +1297,8 @@ extern "C" int ifosb_gradient(ifosb_engine *e) {
     }
     a.b1 = e->b1; a.b2 = e->b2;
     a.rdx = p.dx; a.rdy = p.dy; a.rdz = p.dz;
+    a.ihx = 1.0f / p.dx; a.ihy = 1.0f / p.dy; a.ihz = 1.0f / p.dz;
+    const bool p2 = pow2(p.dx) && pow2(p.dy) && pow2(p.dz);
     a.grad = e->d_grad;
     a.grad64 = e->d_grad64;
     a.gradq = p.nmech > 0 ? e->d_gradq : nullptr;
@@ -1316,8 +1318,13 @@ extern "C" int ifosb_gradient(ifosb_engine *e) {
         a.iphi[l] = im;
     }
     dim3 blk(BX, BY), grd(e->g.ntk, e->g.nti, e->g.nyc);
-    if (a.gradq) k_gradient<true><<<grd, blk, 0, e->stream>>>(a);
-    else k_gradient<false><<<grd, blk, 0, e->stream>>>(a);
+    if (a.gradq) {
+        if (p2) k_gradient<true, true><<<grd, blk, 0, e->stream>>>(a);
+        else k_gradient<true, false><<<grd, blk, 0, e->stream>>>(a);
+    } else {
+        if (p2) k_gradient<false, true><<<grd, blk, 0, e->stream>>>(a);
+        else k_gradient<false, false><<<grd, blk, 0, e->stream>>>(a);
+    }
     int rc = check_launch(e, "gradient");
     if (rc) return rc;
     CU(cudaStreamSynchronize(e->stream));
@@ -1356,7 +1363,7 @@ extern "C" int ifosb_gradient_td(ifosb_engine *e, int interval, double *kernels)
     TdLayout t;
     if (!td_layout(e, nshots, interval, t)) return fail(e, IFOSB_EARG, "TIME / DT must lie between 2 and NT + 1 steps");
     const int K = t.K, last = t.last, nseg = t.nseg;
-    const long long F = e->g.field, n = (long long)p.nx * p.ny * p.nz;
+    const long long n = (long long)p.nx * p.ny * p.nz;
     const size_t ss = t.ss, ps = t.ps, us = t.us, ck = t.ck, seg_shot = t.seg_shot;
     // the last forward's own checkpoints at this interval spare the re-run (the
     // block is grow-only: it still holds them when it is large enough)
@@ -1433,6 +1440,8 @@ extern "C" int ifosb_gradient_td(ifosb_engine *e, int interval, double *kernels)
         ta.nshots = nshots;
         ta.b1 = e->b1; ta.b2 = e->b2;
         ta.rdx = p.dx; ta.rdy = p.dy; ta.rdz = p.dz;
+        ta.ihx = 1.0f / p.dx; ta.ihy = 1.0f / p.dy; ta.ihz = 1.0f / p.dz;
+        const bool p2 = pow2(p.dx) && pow2(p.dy) && pow2(p.dz);
         ta.k = dk;
         {
             std::vector<int> init(nshots, INT_MAX);
@@ -1487,7 +1496,8 @@ extern "C" int ifosb_gradient_td(ifosb_engine *e, int interval, double *kernels)
                     td_step(e, La, ntb);
                     integrate(ub, e->d_state, nullptr);
                     ta.seg = segb + (size_t)(m - a0) * seg_shot * nshots;
-                    k_td_corr<<<grd_c, dim3(BX, BY), 0, e->stream>>>(ta);
+                    if (p2) k_td_corr<true><<<grd_c, dim3(BX, BY), 0, e->stream>>>(ta);
+                    else k_td_corr<false><<<grd_c, dim3(BX, BY), 0, e->stream>>>(ta);
                 }
             }
             for (; ntb <= NT; ++ntb) {  // adjoint steps past P-1 meet forward steps before the first (zero)
@@ -1885,9 +1895,11 @@ extern "C" int ifosb_hessian(ifosb_engine *e) {
     }
     a.b1 = e->b1; a.b2 = e->b2;
     a.rdx = p.dx; a.rdy = p.dy; a.rdz = p.dz;
+    a.ihx = 1.0f / p.dx; a.ihy = 1.0f / p.dy; a.ihz = 1.0f / p.dz;
     a.hess = e->d_hess;
     dim3 blk(BX, BY), grd(e->g.ntk, e->g.nti, e->g.nyc);
-    k_hessian<<<grd, blk, 0, e->stream>>>(a);
+    if (pow2(p.dx) && pow2(p.dy) && pow2(p.dz)) k_hessian<true><<<grd, blk, 0, e->stream>>>(a);
+    else k_hessian<false><<<grd, blk, 0, e->stream>>>(a);
     if ((rc = check_launch(e, "hessian"))) return rc;
     CU(cudaStreamSynchronize(e->stream));
     e->hess_fwd = false;  // one contribution per forward batch

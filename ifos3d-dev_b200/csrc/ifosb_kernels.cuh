@@ -557,6 +557,7 @@ struct GradArgs {
     const float *rho;          // rho in field layout
     float fdummy[MAXNF];       // 1/(4 pi^2 f^2) in float as gradient_F.c:70-72
     float b1, b2, rdx, rdy, rdz;
+    float ihx, ihy, ihz;       // 1/DX, 1/DY, 1/DZ (exact for power-of-two spacings)
     float *grad;
     double *grad64;
     // viscoelastic only: gradients with respect to taup and taus ([2][NY][NX][NZ],
@@ -566,19 +567,29 @@ struct GradArgs {
     double rphi[MAXNF], iphi[MAXNF];
 };
 
-// d: a float[9] or a column of shared memory (SCol)
-template <class D>
+// x / h with the division operator's bits: for a power-of-two spacing the exact
+// reciprocal (x * (1/h) == x / h for h = 2^k), else div_rn (no slow path for the
+// zero dividends of a field the wave has not reached)
+template <bool P2>
+__device__ __forceinline__ float dvh(float x, float h, float ih) {
+    return P2 ? __fmul_rn(x, ih) : div_rn(x, h);
+}
+
+// d: a float[9] or a column of shared memory (SCol); DX.. the spacings, IX.. their
+// reciprocals (used with P2)
+template <bool P2, class D>
 __device__ __forceinline__ void dft_derivs(const float *X, const float *Y, const float *Z, long long c, long long dI,
-                                           long long dJ, float b1, float b2, float DX, float DY, float DZ, D d) {
-    d[0] = (b1 * (X[c] - X[c - dI]) + b2 * (X[c + dI] - X[c - 2 * dI])) / DX;
-    d[1] = (b1 * (X[c + dJ] - X[c]) + b2 * (X[c + 2 * dJ] - X[c - dJ])) / DY;
-    d[2] = (b1 * (X[c + 1] - X[c]) + b2 * (X[c + 2] - X[c - 1])) / DZ;
-    d[3] = (b1 * (Y[c + dI] - Y[c]) + b2 * (Y[c + 2 * dI] - Y[c - dI])) / DX;
-    d[4] = (b1 * (Y[c] - Y[c - dJ]) + b2 * (Y[c + dJ] - Y[c - 2 * dJ])) / DY;
-    d[5] = (b1 * (Y[c + 1] - Y[c]) + b2 * (Y[c + 2] - Y[c - 1])) / DZ;
-    d[6] = (b1 * (Z[c + dI] - Z[c]) + b2 * (Z[c + 2 * dI] - Z[c - dI])) / DX;
-    d[7] = (b1 * (Z[c + dJ] - Z[c]) + b2 * (Z[c + 2 * dJ] - Z[c - dJ])) / DY;
-    d[8] = (b1 * (Z[c] - Z[c - 1]) + b2 * (Z[c + 1] - Z[c - 2])) / DZ;
+                                           long long dJ, float b1, float b2, float DX, float DY, float DZ, float IX,
+                                           float IY, float IZ, D d) {
+    d[0] = dvh<P2>(b1 * (X[c] - X[c - dI]) + b2 * (X[c + dI] - X[c - 2 * dI]), DX, IX);
+    d[1] = dvh<P2>(b1 * (X[c + dJ] - X[c]) + b2 * (X[c + 2 * dJ] - X[c - dJ]), DY, IY);
+    d[2] = dvh<P2>(b1 * (X[c + 1] - X[c]) + b2 * (X[c + 2] - X[c - 1]), DZ, IZ);
+    d[3] = dvh<P2>(b1 * (Y[c + dI] - Y[c]) + b2 * (Y[c + 2 * dI] - Y[c - dI]), DX, IX);
+    d[4] = dvh<P2>(b1 * (Y[c] - Y[c - dJ]) + b2 * (Y[c + dJ] - Y[c - 2 * dJ]), DY, IY);
+    d[5] = dvh<P2>(b1 * (Y[c + 1] - Y[c]) + b2 * (Y[c + 2] - Y[c - 1]), DZ, IZ);
+    d[6] = dvh<P2>(b1 * (Z[c + dI] - Z[c]) + b2 * (Z[c + 2 * dI] - Z[c - dI]), DX, IX);
+    d[7] = dvh<P2>(b1 * (Z[c + dJ] - Z[c]) + b2 * (Z[c + 2 * dJ] - Z[c - dJ]), DY, IY);
+    d[8] = dvh<P2>(b1 * (Z[c] - Z[c - 1]) + b2 * (Z[c + 1] - Z[c - 2]), DZ, IZ);
 }
 
 // The same pointer, hidden from the optimiser (an empty asm that "changes" it).
@@ -605,7 +616,7 @@ struct SCol {
 #ifndef IFOSB_GRAD_MINB
 #define IFOSB_GRAD_MINB 4
 #endif
-template <bool Q>
+template <bool Q, bool P2>
 __global__ void __launch_bounds__(BX *BY, IFOSB_GRAD_MINB) k_gradient(GradArgs a) {
     __shared__ float sdv[4 * 9 * BX * BY];
     const Geo &g = a.g;
@@ -641,13 +652,13 @@ __global__ void __launch_bounds__(BX *BY, IFOSB_GRAD_MINB) k_gradient(GradArgs a
                 // 144 loads then need few registers (no spills to local memory).
                 const float *Fc = Fb + c, *Bc = Bb + c;
                 const float *p0 = opaque(Fc), *p1 = opaque(Fc + F), *p2 = opaque(Fc + 2 * F);
-                dft_derivs(p0, p1, p2, 0, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, fv);
+                dft_derivs<P2>(p0, p1, p2, 0, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, a.ihx, a.ihy, a.ihz, fv);
                 p0 = opaque(Bc); p1 = opaque(Bc + F); p2 = opaque(Bc + 2 * F);
-                dft_derivs(p0, p1, p2, 0, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, bv);
+                dft_derivs<P2>(p0, p1, p2, 0, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, a.ihx, a.ihy, a.ihz, bv);
                 p0 = opaque(Fc + 3 * F); p1 = opaque(Fc + 4 * F); p2 = opaque(Fc + 5 * F);
-                dft_derivs(p0, p1, p2, 0, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, fi);
+                dft_derivs<P2>(p0, p1, p2, 0, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, a.ihx, a.ihy, a.ihz, fi);
                 p0 = opaque(Bc + 3 * F); p1 = opaque(Bc + 4 * F); p2 = opaque(Bc + 5 * F);
-                dft_derivs(p0, p1, p2, 0, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, bi);
+                dft_derivs<P2>(p0, p1, p2, 0, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, a.ihx, a.ihy, a.ihz, bi);
                 const float fdummy = a.fdummy[l];
                 float gradlam = (fv[0] + fv[4] + fv[8]) * (bv[0] + bv[4] + bv[8]) + (fi[0] + fi[4] + fi[8]) * (bi[0] + bi[4] + bi[8]);
                 gradlam = -gradlam * fdummy;
@@ -724,11 +735,16 @@ struct TdArgs {
     long long seg_shot;
     int nshots;
     float b1, b2, rdx, rdy, rdz;
+    float ihx, ihy, ihz;   // 1/DX, 1/DY, 1/DZ (exact for power-of-two spacings)
     double *k;             // [4][NY][NX][NZ]: rho, lambda, mu, dc
 };
 
 // One thread per interior cell: blocks of BX (z) x BY (x) cells, one plane each
-// (grid ceil(NZ/BX) x ceil(NX/BY) x NY).
+// (grid ceil(NZ/BX) x ceil(NX/BY) x NY). (A variant that marched 1-16 planes per
+// block with the x/z neighbours staged in shared memory and the y neighbours in
+// registers ran 1.5-2.2 times slower at 128^3: fewer loads, but a barrier between
+// each plane's loads and its arithmetic.)
+template <bool P2>
 __global__ void __launch_bounds__(BX *BY, 4) k_td_corr(TdArgs a) {
     const Geo &g = a.g;
     const int k = blockIdx.x * BX + threadIdx.x + 1, i = blockIdx.y * BY + threadIdx.y + 1, j = blockIdx.z + 1;
@@ -744,9 +760,9 @@ __global__ void __launch_bounds__(BX *BY, 4) k_td_corr(TdArgs a) {
             kr += (double)vf[c] * vb[c] + (double)vf[F + c] * vb[F + c] + (double)vf[2 * F + c] * vb[2 * F + c];
             float fu[9], bu[9];
             const float *p0 = opaque(uf + c), *p1 = opaque(uf + F + c), *p2 = opaque(uf + 2 * F + c);
-            dft_derivs(p0, p1, p2, 0, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, fu);
+            dft_derivs<P2>(p0, p1, p2, 0, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, a.ihx, a.ihy, a.ihz, fu);
             p0 = opaque(ub + c); p1 = opaque(ub + F + c); p2 = opaque(ub + 2 * F + c);
-            dft_derivs(p0, p1, p2, 0, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, bu);
+            dft_derivs<P2>(p0, p1, p2, 0, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, a.ihx, a.ihy, a.ihz, bu);
             kl += ((double)fu[0] + fu[4] + fu[8]) * ((double)bu[0] + bu[4] + bu[8]);
             km += 2.0 * ((double)fu[0] * bu[0] + (double)fu[4] * bu[4] + (double)fu[8] * bu[8]) +
                   ((double)fu[1] + fu[3]) * ((double)bu[1] + bu[3]) + ((double)fu[2] + fu[6]) * ((double)bu[2] + bu[6]) +
@@ -819,6 +835,7 @@ struct HessArgs {
     const float *rho;          // rho in field layout
     float fdummy[MAXNF];       // 1/(2 pi f) in float as hess_F.c:72-74
     float b1, b2, rdx, rdy, rdz;
+    float ihx, ihy, ihz;       // 1/DX, 1/DY, 1/DZ (exact for power-of-two spacings)
     float *hess;
 };
 
@@ -829,6 +846,7 @@ struct HessArgs {
 #ifndef IFOSB_HESS_MINB
 #define IFOSB_HESS_MINB 4
 #endif
+template <bool P2>
 __global__ void __launch_bounds__(BX *BY, IFOSB_HESS_MINB) k_hessian(HessArgs a) {
     __shared__ float sdv[4 * 9 * BX * BY];
     const Geo &g = a.g;
@@ -855,13 +873,13 @@ __global__ void __launch_bounds__(BX *BY, IFOSB_HESS_MINB) k_hessian(HessArgs a)
                     // one stencil set at a time, as in k_gradient
                     const float *Fc = Fb + c, *Bc = Bb + c;
                     const float *p0 = opaque(Fc), *p1 = opaque(Fc + F), *p2 = opaque(Fc + 2 * F);
-                    dft_derivs(p0, p1, p2, 0, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, fv);
+                    dft_derivs<P2>(p0, p1, p2, 0, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, a.ihx, a.ihy, a.ihz, fv);
                     p0 = opaque(Bc); p1 = opaque(Bc + F); p2 = opaque(Bc + 2 * F);
-                    dft_derivs(p0, p1, p2, 0, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, bv);
+                    dft_derivs<P2>(p0, p1, p2, 0, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, a.ihx, a.ihy, a.ihz, bv);
                     p0 = opaque(Fc + 3 * F); p1 = opaque(Fc + 4 * F); p2 = opaque(Fc + 5 * F);
-                    dft_derivs(p0, p1, p2, 0, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, fi);
+                    dft_derivs<P2>(p0, p1, p2, 0, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, a.ihx, a.ihy, a.ihz, fi);
                     p0 = opaque(Bc + 3 * F); p1 = opaque(Bc + 4 * F); p2 = opaque(Bc + 5 * F);
-                    dft_derivs(p0, p1, p2, 0, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, bi);
+                    dft_derivs<P2>(p0, p1, p2, 0, dI, dJ, a.b1, a.b2, a.rdx, a.rdy, a.rdz, a.ihx, a.ihy, a.ihz, bi);
                     const float fd = a.fdummy[l];
                     const float fdiv = fv[0] + fv[4] + fv[8], fidiv = fi[0] + fi[4] + fi[8];
                     const float bdiv = bv[0] + bv[4] + bv[8], bidiv = bi[0] + bi[4] + bi[8];

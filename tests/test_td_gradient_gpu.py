@@ -219,7 +219,7 @@ def test_forward_checkpoints_and_graphs_change_no_bit(nmech):
     s0, k0 = fresh(4, 0)  # plain launches, the forward run again
     e.set_launch_mode(0)
     s1, k1 = fresh(4, 0)  # graph capture
-    c1 = e.graph_captures()
+    c1 = e.graph_captures
     k1b = e.gradient_td(4)  # the checkpoints of the call before: no re-run
     s2, k2 = fresh(4, 4)  # the forward's own checkpoints
     k2b = e.gradient_td(4)
@@ -230,5 +230,5 @@ def test_forward_checkpoints_and_graphs_change_no_bit(nmech):
         assert np.array_equal(k, k0)
     for s in (s1, s2, s3):
         assert np.array_equal(s, s0)
-    assert e.graph_captures() > c1  # the armed forward and the no-re-run loops are graphs of their own
+    assert e.graph_captures > c1  # the armed forward and the no-re-run loops are graphs of their own
     e.close()
