@@ -18,6 +18,11 @@ The differences are the ones the engine makes everywhere: shots run in batches,
 misfits are summed in FP64, and the optimiser's dot products and the step-length
 parabola are FP64. Models are the ghosted [NY+2][NX+2][NZ+2] rho, pi, u arrays of
 the reference; their ghost layers are refreshed by the engine (matcopy's wrap).
+With L > 0 relaxation mechanisms (p.nmech, visco = (taus, taup, eta)) the
+relaxation times stay fixed and the iteration updates the relaxed moduli through
+modelupdate's vp, vs, rho exactly as the elastic one does, with the gradient of
+the viscoelastic propagation (the reference cannot run this: its viscoelastic
+stress calls are commented out, src/ifos3d.c:773/777, and L is 1 there).
 """
 from __future__ import annotations
 
@@ -77,8 +82,18 @@ def stages_from_workflow(path: str, nstages: int) -> list:
 
 
 class Inversion:
-    def __init__(self, p: Params, cpml, recpos, shots, obs, srcpos_m, rho, pi, u, stages, cfg: Settings):
+    def __init__(self, p: Params, cpml, recpos, shots, obs, srcpos_m, rho, pi, u, stages, cfg: Settings,
+                 visco=None):
+        """visco: (taus, taup, eta) for p.nmech > 0 — [NY][NX][NZ] relaxation times per
+        cell and the mechanisms' eta — kept fixed through the inversion."""
         self.p, self.cfg, self.stages = p, cfg, list(stages)
+        self.visco = None
+        if p.nmech:
+            if visco is None:
+                raise ValueError("an inversion with L > 0 mechanisms needs visco=(taus, taup, eta)")
+            if cfg.hess:
+                raise ValueError("the Hessian wavefields are elastic (ifos3d.c:929): no HESS with L > 0")
+            self.visco = tuple(np.ascontiguousarray(a, np.float32) for a in visco)
         self.shots_raw, self.obs_raw = list(shots), np.ascontiguousarray(obs, np.float32)
         self.shots, self.obs = self.shots_raw, self.obs_raw
         self.recpos = np.ascontiguousarray(recpos, np.int32)
@@ -134,7 +149,10 @@ class Inversion:
             fio.write_gradient(self.cfg.grad_file, float(self.finv[0]), iteration, g, idx=i[0], idy=i[1], idz=i[2])
 
     def _set_model(self, m):
-        self.eng.set_model(*(a[1:-1, 1:-1, 1:-1] for a in m), None, None, None)
+        if self.visco:
+            self.eng.set_model(*(a[1:-1, 1:-1, 1:-1] for a in m), *self.visco)
+        else:
+            self.eng.set_model(*(a[1:-1, 1:-1, 1:-1] for a in m), None, None, None)
 
     def _batches(self, idx):
         b = self.cfg.max_batch

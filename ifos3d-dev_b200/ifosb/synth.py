@@ -45,6 +45,27 @@ def q_tau_fit(q: float, fmin: float, fmax: float, nmech: int):
     return tau, fl.astype(np.float32)
 
 
+def q_moduli(p, vp, vs, rho, q, fmin, fmax):
+    """readmod's relaxed moduli (src/readmod.c:48-65, generalised to L mechanisms)
+    with a relaxation time per cell: the tau method's fit is linear in 1/Q
+    (q_tau_fit), so tau = tau(Q=1) / Q; taus = taup = tau. ws = 2 pi FL[1] as in
+    readmod. Returns dict(rho, pi, u, taus, taup, eta) as float32 arrays."""
+    L = p.nmech
+    tau1, fl = q_tau_fit(1.0, fmin, fmax, L)
+    tau = (np.float32(tau1) / np.asarray(q, np.float32)).astype(np.float32)
+    pts = (1.0 / (2.0 * PI * fl.astype(np.float64))).astype(np.float32)
+    ws = np.float32(2.0 * PI * float(fl[0]))
+    s = np.float32(0.0)
+    for t in pts:
+        s = np.float32(s + np.float32((ws * ws * t * t) / np.float32(1.0 + ws * ws * t * t)))
+    vp, vs, rho = (np.asarray(a, np.float32) for a in (vp, vs, rho))
+    den = (np.float32(1.0) + tau * s).astype(np.float32)
+    pi = (vp * vp * rho / den).astype(np.float32)
+    u = (vs * vs * rho / den).astype(np.float32)
+    eta = (np.float32(p.dt) / pts).astype(np.float32)
+    return dict(rho=rho, pi=pi, u=u, taus=tau.copy(), taup=tau.copy(), eta=eta)
+
+
 def _grid_receivers(nx, nz, n_side, j, margin):
     xs = np.linspace(margin, nx - margin + 1, n_side).round().astype(int)
     zs = np.linspace(margin, nz - margin + 1, n_side).round().astype(int)
