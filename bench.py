@@ -990,7 +990,8 @@ def multiscale_visco_workload(args, local):
     """The viscoelastic multiscale configuration at half its linear size, on one
     GPU: L=3 with Q from 30 to 100 (fixed), 16 shots in one HBM batch, three
     frequency stages (10-30, 30-60, 60-100 Hz), L-BFGS on vp (NUMPAR 1, WEIGHT
-    1 0 0, BFGSNUM 3), the first two stages on a 128x128x80 grid at 2 m, then the
+    1 0 0, BFGSNUM 3; the first update of a stage normalised, as the reference's
+    would otherwise not move the model), the first two stages on a 128x128x80 grid at 2 m, then the
     model resampled to 256x256x160 at 1 m for the third (the configuration's
     grids are 256x256x160 at 2 m and 512x512x320 at 1 m with 64 shots and 10
     iterations per stage). True model: four layers, three Gaussian blobs (+10 %
@@ -1054,7 +1055,7 @@ def multiscale_visco_workload(args, local):
         ghost = [ifosb.ghost_wrap(mod0[k]) for k in ("rho", "pi", "u")]
         srcpos_m = np.array([[sp[0, 0] * gd["h"], sp[0, 1] * gd["h"], sp[0, 2] * gd["h"]] for sp, _ in shots], np.float32)
         cfg = Settings(teststep=0.02, damptype=2, lbfgs=True, numpar=1, bfgsnum=3, nshots_step=4,
-                       max_batch=len(shots), weight=(1.0, 0.0, 0.0))
+                       max_batch=len(shots), weight=(1.0, 0.0, 0.0), lbfgs_first_normalised=True)
         inv = Inversion(p, cp, rec, shots, obs, srcpos_m, *ghost, gd["stages"], cfg,
                         visco=(mod0["taus"], mod0["taup"], mod0["eta"]))
         iters = sum(st.itmax for st in gd["stages"])

@@ -50,6 +50,7 @@ class Settings:
     rho0: float = 2000.0
     damptype: int = 2              # DAMPTYPE
     lbfgs: bool = False            # LBFGS
+    lbfgs_first_normalised: bool = False  # not in the reference: see Inversion.iterate
     numpar: int = 1                # NUMPAR
     bfgsnum: int = 3               # BFGSNUM
     nshots_step: int = 1           # NSHOTS_STEP (shots of the step-length test forwards)
@@ -221,6 +222,20 @@ class Inversion:
                 self.opt.lbfgs(g, self.it_group)
             else:
                 self.opt.lbfgs_savegrad(g)
+                if cfg.lbfgs_first_normalised:
+                    # The reference's first L-BFGS update of a stage moves the model by
+                    # step * the raw gradient (modelupdate normalises only without
+                    # L-BFGS), about 1e-20 of vp0: the model does not change and the
+                    # history stays empty. With this option that one direction is
+                    # normalised as modelupdate.c:105-117 normalises (each parameter
+                    # by its largest magnitude; max rho 0 -> 1); the saved gradient
+                    # and every later update are the reference's.
+                    m = [float(np.abs(g[c]).max()) for c in range(3)]
+                    if m[2] == 0.0:
+                        m[2] = 1.0
+                    if m[0] > 0.0 and m[1] > 0.0:
+                        for c in range(3):
+                            g[c] /= np.float32(m[c])
         else:
             beta = self.opt.conjugate(g, cdf)
         self._write_grad(g, self.iteration + 2000)

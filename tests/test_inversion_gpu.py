@@ -70,6 +70,21 @@ def test_lbfgs_iterations_run():
     assert np.any(y_hist[0] != 0) and np.any(s_hist != 0)
 
 
+def test_lbfgs_with_a_normalised_first_step_reduces_misfit():
+    """With the first update of the stage normalised (Settings.lbfgs_first_normalised,
+    not the reference's behaviour), the L-BFGS history is not degenerate and the
+    misfit falls over four iterations."""
+    p, cp, rec, shots, obs, srcpos_m, ghost, vp0, vpT = _problem(free_surf=0)
+    cfg = Settings(teststep=0.02, damptype=2, lbfgs=True, numpar=1, bfgsnum=3, nshots_step=4, max_batch=4,
+                   weight=(1.0, 0.0, 0.0), lbfgs_first_normalised=True)
+    inv = Inversion(p, cp, rec, shots, obs, srcpos_m, *ghost, [Stage([300.0, 450.0, 600.0], 4)], cfg)
+    hist = inv.run(4)
+    inv.close()
+    assert all(np.isfinite(hist.misfit)) and all(np.isfinite(hist.step))
+    assert hist.misfit[1] < hist.misfit[0], hist.misfit  # the normalised first step moved the model
+    assert hist.misfit[-1] < 0.95 * hist.misfit[0], hist.misfit
+
+
 def test_free_surface_with_reference_damping_leaves_the_model():
     """With FREE_SURF, precon_grad's top factor is 0 for damping types 0-2 (the
     reference's behaviour): the gradient vanishes; inside the frame that
