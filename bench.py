@@ -1027,7 +1027,7 @@ def multiscale_visco_workload(args, local):
     inner = lambda a: a[fw:-fw, fw:-fw, fw:-fw]  # noqa: E731
     err = lambda vp: float(np.linalg.norm(inner(vp) - inner(vp_t)) / np.linalg.norm(inner(vp_t)))  # noqa: E731
     cur = start
-    hist, cells, t_total, t_obs = [], 0, 0.0, 0.0
+    hist, cells, t_total, t_obs, stage0 = [], 0, 0.0, 0.0, 0
     vp_err = {"start": err(start[0])}
     for gi, gd in enumerate(grids):
         s = gd["h"] / h_fine
@@ -1065,8 +1065,9 @@ def multiscale_visco_workload(args, local):
             mis = inv.iterate()
             t_total += time.perf_counter() - t0
             cells += ncell * p.nt * (2 * len(shots) + 2 * cfg.nshots_step)
-            hist.append({"grid": gi, "stage": inv.stage_i, "misfit": mis, "t_s": round(t_total, 3),
+            hist.append({"grid": gi, "stage": stage0 + inv.stage_i, "misfit": mis, "t_s": round(t_total, 3),
                          "step": inv.hist.step[-1]})
+        stage0 += len(gd["stages"])
         rho, pi, u = (a[1:-1, 1:-1, 1:-1].astype(np.float64) for a in inv.model)
         got = ((np.sqrt(pi / rho)).astype(np.float32), (np.sqrt(u / rho)).astype(np.float32), rho.astype(np.float32))
         inv.close()
