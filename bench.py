@@ -306,6 +306,9 @@ def main():
     ap.add_argument("--workload", default="visco384",
                     choices=["visco384", "visco256", "elastic128", "multiscale", "multiscale_visco"])
     ap.add_argument("--iterations-per-stage", type=int, default=3, help="multiscale_visco: L-BFGS iterations per stage")
+    ap.add_argument("--ms-scale", type=float, default=0.5, help="multiscale_visco: linear size against the configuration")
+    ap.add_argument("--ms-shots-side", type=int, default=4, help="multiscale_visco: shots per side of the surface grid")
+    ap.add_argument("--ms-iterations", type=int, default=0, help="multiscale_visco: cap on the iterations run (0: all)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nt", type=int, default=None, help="override NT (testing only)")
     ap.add_argument("--no-cpu", action="store_true")
@@ -987,17 +990,20 @@ def time_domain_comparison(torch, ifosb, synth, dev, stream, nt_override, interv
 
 
 def multiscale_visco_workload(args, local):
-    """The viscoelastic multiscale configuration at half its linear size, on one
-    GPU: L=3 with Q from 30 to 100 (fixed), 16 shots in one HBM batch, three
-    frequency stages (10-30, 30-60, 60-100 Hz), L-BFGS on vp (NUMPAR 1, WEIGHT
-    1 0 0, BFGSNUM 3; the first update of a stage normalised, as the reference's
-    would otherwise not move the model), the first two stages on a 128x128x80 grid at 2 m, then the
-    model resampled to 256x256x160 at 1 m for the third (the configuration's
-    grids are 256x256x160 at 2 m and 512x512x320 at 1 m with 64 shots and 10
-    iterations per stage). True model: four layers, three Gaussian blobs (+10 %
-    vp, -40 % Q); start: the true model smoothed by a 15 m Gaussian. No free
-    surface (precon_grad's damping types 0-2 zero the gradient with one). Timed by
-    the host clock around the synchronous calls."""
+    """The viscoelastic multiscale configuration on one GPU: L=3 with Q from 30 to
+    100 (fixed), three frequency stages (10-30, 30-60, 60-100 Hz), L-BFGS on vp
+    (NUMPAR 1, WEIGHT 1 0 0, BFGSNUM 3; the first update of a stage normalised,
+    as the reference's would otherwise not move the model), the first two stages
+    on a 2 m grid, then the model resampled to a 1 m grid for the third. The
+    configuration's grids are 256x256x160 at 2 m and 512x512x320 at 1 m (NX x NZ
+    horizontal, NY deep) with 64 shots and 10 iterations per stage; by default
+    this runs it at half the linear size with 16 shots and --iterations-per-stage
+    iterations; --ms-scale 1 --ms-shots-side 8 gives the configuration's grids and
+    shots, and --ms-iterations caps the iterations run (the rest of the schedule is
+    skipped). Shots go in HBM-sized batches. True model: four layers, three
+    Gaussian blobs (+10 % vp, -40 % Q); start: the true model smoothed by a 15 m
+    Gaussian. No free surface (precon_grad's damping types 0-2 zero the gradient
+    with one). Timed by the host clock around the synchronous calls."""
     import torch
     from scipy.ndimage import gaussian_filter
     import ifosb
@@ -1005,31 +1011,38 @@ def multiscale_visco_workload(args, local):
     from ifosb import synth
     from ifosb.inversion import Inversion, Settings, Stage
     torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
     rng = np.random.default_rng(11)
-    fw, fc, nsh_side, h_fine, fmin_q, fmax_q = 10, 50.0, 4, 1.0, 10.0, 100.0
-    fine = (160, 256, 256)  # (NY, NX, NZ), y down
+    sc, nsh_side = args.ms_scale, args.ms_shots_side
+    fw, fc, h_fine, fmin_q, fmax_q = 10, 50.0, 1.0, 10.0, 100.0
+    fine = tuple(int(round(n * sc)) for n in (320, 512, 512))  # (NY, NX, NZ), y down
     its = args.iterations_per_stage
-    jj, ii, kk = np.meshgrid(*(np.arange(n) for n in fine), indexing="ij")
-    bounds = np.sort(rng.choice(np.arange(25, fine[0] - 25), 3, replace=False))
+    cap_it = args.ms_iterations or 10 ** 9
+    jj, ii, kk = np.meshgrid(*(np.arange(n, dtype=np.float32) for n in fine), indexing="ij")
+    bounds = np.sort(rng.choice(np.arange(int(50 * sc), fine[0] - int(50 * sc)), 3, replace=False))
     layer = np.searchsorted(bounds, np.arange(fine[0]), side="right")
     vp_t = np.array([2500.0, 2900.0, 3200.0, 3500.0], np.float32)[layer][:, None, None] * np.ones(fine, np.float32)
     q_t = np.array([30.0, 50.0, 75.0, 100.0], np.float32)[layer][:, None, None] * np.ones(fine, np.float32)
     for _ in range(3):
         c = [rng.uniform(0.3 * n, 0.7 * n) for n in fine]
-        g = np.exp(-((jj - c[0]) ** 2 + (ii - c[1]) ** 2 + (kk - c[2]) ** 2) / (2 * 14.0 ** 2))
+        g = np.exp(-((jj - c[0]) ** 2 + (ii - c[1]) ** 2 + (kk - c[2]) ** 2) / (2 * (28.0 * sc) ** 2))
         vp_t *= 1 + 0.1 * g
         q_t *= 1 - 0.4 * g
+    del jj, ii, kk
     vp_t, q_t = vp_t.astype(np.float32), np.clip(q_t, 30.0, 100.0).astype(np.float32)
     true = (vp_t, (vp_t / np.float32(math.sqrt(3))).astype(np.float32), (1700 + 0.2 * vp_t).astype(np.float32))
     start = tuple(gaussian_filter(a.astype(np.float64), 15.0, mode="nearest").astype(np.float32) for a in true)
-    grids = [dict(h=2.0, dt=2e-4, nt=1000, stages=[Stage([10.0, 20.0, 30.0], its), Stage([30.0, 45.0, 60.0], its)]),
-             dict(h=1.0, dt=1e-4, nt=2000, stages=[Stage([60.0, 80.0, 100.0], its)])]
+    nt_c, nt_f = int(round(2000 * sc)), int(round(4000 * sc))
+    grids = [dict(h=2.0, dt=2e-4, nt=nt_c, stages=[Stage([10.0, 20.0, 30.0], its), Stage([30.0, 45.0, 60.0], its)]),
+             dict(h=1.0, dt=1e-4, nt=nt_f, stages=[Stage([60.0, 80.0, 100.0], its)])]
     inner = lambda a: a[fw:-fw, fw:-fw, fw:-fw]  # noqa: E731
     err = lambda vp: float(np.linalg.norm(inner(vp) - inner(vp_t)) / np.linalg.norm(inner(vp_t)))  # noqa: E731
     cur = start
-    hist, cells, t_total, t_obs, stage0 = [], 0, 0.0, 0.0, 0
+    hist, cells, t_total, t_obs, stage0, batches = [], 0, 0.0, 0.0, 0, []
     vp_err = {"start": err(start[0])}
     for gi, gd in enumerate(grids):
+        if len(hist) >= cap_it:
+            break
         s = gd["h"] / h_fine
         shape = tuple(int(n / s) for n in fine)
         ny, nx, nz = shape
@@ -1042,23 +1055,33 @@ def multiscale_visco_workload(args, local):
         shots = [(sp, ifosb.wavelet(p, 4, sp)) for sp in (synth._src(int(x), fw + 3, int(z), fc) for x in xs for z in zs)]
         rec = synth._grid_receivers(nx, nz, 16, fw + 2, fw + 3)
         cp = ifosb.cpml_coeff(p, 4000.0, fc)
-        e = ifosb.Engine(p, max_shots=len(shots), max_nf=0)
+        # batch size: the shots the free memory holds next to a 6 GB margin
+        sizes = []
+        for nb in (1, 2):
+            e = ifosb.Engine(p, max_shots=nb, max_nf=3)
+            sizes.append(e.device_bytes)
+            e.close()
+        per_shot = sizes[1] - sizes[0]
+        free, _ = torch.cuda.mem_get_info(dev)
+        B = max(1, min(len(shots), int((free - 6e9 - (sizes[0] - per_shot)) // per_shot)))
+        batches.append(B)
+        mod = synth.q_moduli(p, *mt, q, fmin_q, fmax_q)
+        e = ifosb.Engine(p, max_shots=B, max_nf=0)
         e.set_cpml(cp)
         e.set_receivers(rec)
-        mod = synth.q_moduli(p, *mt, q, fmin_q, fmax_q)
         e.set_model(mod["rho"], mod["pi"], mod["u"], mod["taus"], mod["taup"], mod["eta"])
         t0 = time.perf_counter()
-        obs = e.forward(shots)
+        obs = np.concatenate([e.forward(shots[i:i + B]) for i in range(0, len(shots), B)])
         t_obs += time.perf_counter() - t0
         e.close()
         mod0 = synth.q_moduli(p, *m0, q, fmin_q, fmax_q)
         ghost = [ifosb.ghost_wrap(mod0[k]) for k in ("rho", "pi", "u")]
         srcpos_m = np.array([[sp[0, 0] * gd["h"], sp[0, 1] * gd["h"], sp[0, 2] * gd["h"]] for sp, _ in shots], np.float32)
         cfg = Settings(teststep=0.02, damptype=2, lbfgs=True, numpar=1, bfgsnum=3, nshots_step=4,
-                       max_batch=len(shots), weight=(1.0, 0.0, 0.0), lbfgs_first_normalised=True)
+                       max_batch=B, weight=(1.0, 0.0, 0.0), lbfgs_first_normalised=True)
         inv = Inversion(p, cp, rec, shots, obs, srcpos_m, *ghost, gd["stages"], cfg,
                         visco=(mod0["taus"], mod0["taup"], mod0["eta"]))
-        iters = sum(st.itmax for st in gd["stages"])
+        iters = min(sum(st.itmax for st in gd["stages"]), cap_it - len(hist))
         ncell = nx * ny * nz
         for _ in range(iters):
             t0 = time.perf_counter()
@@ -1080,18 +1103,21 @@ def multiscale_visco_workload(args, local):
     for st in sorted({x["stage"] for x in hist}):
         m = [x["misfit"] for x in hist if x["stage"] == st]
         per_stage[f"stage{st}"] = {"first": m[0], "last": m[-1], "reduction": round(1 - m[-1] / m[0], 4)}
+    g0 = tuple(int(n / 2) for n in fine)
     out = {
         "metric": METRIC, "value": round(cells / t_total / 1e9, 3), "unit": UNIT, "n_gpus": 1,
         "steps": len(hist), "warmup": 0, "ms_per_step": round(1000 * t_total / len(hist), 1),
         "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"multiscale_visco: L=3 (Q 30-100) inversion at half the configuration's linear size, "
-                               f"128x80x128 (NX x NY x NZ, y deep) @ 2 m (NT=1000, stages 10-30 and 30-60 Hz) then "
-                               f"256x160x256 @ 1 m (NT=2000, stage 60-100 Hz), {its} L-BFGS iterations per stage, "
-                               "16 shots, 256 receivers, 4 layers + 3 blobs, start smoothed by 15 m",
+        "config": {"workload": f"multiscale_visco: L=3 (Q 30-100) inversion, {g0[1]}x{g0[0]}x{g0[2]} (NX x NY x NZ, y "
+                               f"deep) @ 2 m (NT={nt_c}, stages 10-30 and 30-60 Hz) then {fine[1]}x{fine[0]}x{fine[2]} "
+                               f"@ 1 m (NT={nt_f}, stage 60-100 Hz), {its} L-BFGS iterations per stage"
+                               + (f" (capped at {args.ms_iterations} in all)" if args.ms_iterations else "")
+                               + f", {len(shots)} shots in HBM batches of {batches}, 256 receivers, 4 layers + 3 "
+                                 "blobs, start smoothed by 15 m",
+                   "scale": sc,
                    "timing": "host clock around synchronous calls; value counts the shot gradients and the "
                              "step-length test forwards; the observed-data forwards are not counted",
-                   "full_configuration": "256x256x160 @ 2 m -> 512x512x320 @ 1 m, 64 shots, 10 iterations per "
-                                         "stage: 8x the cells, 4x the shots and 5x the iterations of this run"},
+                   "full_configuration": "256x256x160 @ 2 m -> 512x512x320 @ 1 m, 64 shots, 10 iterations per stage"},
         "inversion": {"iterations": hist, "misfit_per_stage": per_stage, "vp_rel_error": vp_err,
                       "seconds": round(t_total, 2), "observed_data_seconds": round(t_obs, 2)},
     }
