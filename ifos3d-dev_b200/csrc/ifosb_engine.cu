@@ -2082,6 +2082,24 @@ extern "C" int ifosb_autotune(ifosb_engine *e, int nshots, const ifosb_shot *sho
     e->tuned.erase(nshots);
     const Geo hv = launch_geo(e, nshots, true), hs = launch_geo(e, nshots, false);  // built-in choices
     std::vector<int> cys = {2, 3, 4, 6, 8, 12, 16, 24, 32, 64, hv.cy, hs.cy};
+    {
+        // chunkings whose CTA count fills one or two waves at 1-4 CTAs per SM: on
+        // a small grid the fixed list leaves either a nearly empty last wave or
+        // chunks so short that each CTA's pipeline start-up dominates
+        int dev = 0, sms = 148;
+        if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaGetLastError();
+        for (const Geo *lg : {&hv, &hs}) {
+            const long long per_set = (long long)lg->ntk * lg->nti * nshots;
+            for (int per_sm = 1; per_sm <= 4; ++per_sm)
+                for (int waves = 1; waves <= 2; ++waves) {
+                    const long long nyc = (long long)waves * per_sm * sms / per_set;
+                    if (nyc < 1) continue;
+                    const int cy = (int)((e->p.ny + nyc - 1) / nyc);
+                    if (cy >= 2) cys.push_back(cy);
+                }
+        }
+    }
     std::sort(cys.begin(), cys.end());
     cys.erase(std::unique(cys.begin(), cys.end()), cys.end());
     double bv = 1e30, bs = 1e30;
