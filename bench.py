@@ -201,8 +201,8 @@ def cpu_sample(wl):
     """The bounded CPU sample of a workload: (nmech, nf, grid, nt, what)."""
     if wl == "visco384":
         # 1.6 M cells (0.5 GB of state and DFT fields per process, beyond any cache share;
-        # a 36 % CPML frame against the full grid's 14 %), 8 steps: about 10 s on one core
-        return 3, 4, (128, 96, 128), 8, "shot-gradient (forward + residual + adjoint + DFT + gradient_F)"
+        # a 36 % CPML frame against the full grid's 14 %), 24 steps: about 9 s on one core
+        return 3, 4, (128, 96, 128), 24, "shot-gradient (forward + residual + adjoint + DFT + gradient_F)"
     if wl == "elastic128":
         return 0, 2, (64, 64, 64), 40, "shot-gradient (forward + residual + adjoint + DFT + gradient_F)"
     return 3, 0, (64, 64, 64), 40, "forward step"
