@@ -272,7 +272,7 @@ def test_exact_vjp_on_the_adjoint_check_configuration():
         dot = sum(float((gq * hq).sum()) for gq, hq in zip(g, half))
         rel = abs(dot - fd) / abs(fd)
         worst = max(worst, rel)
-        print(f"config-3 grid: <g,d> {dot:.6e} FD {fd:.6e} rel {rel:.2e}")
+        print(f"192x192x160 grid: <g,d> {dot:.6e} FD {fd:.6e} rel {rel:.2e}")
         assert rel <= 1e-3
-    print(f"config-3 grid: worst relative difference {worst:.2e}")
+    print(f"192x192x160 grid: worst relative difference {worst:.2e}")
     e.close()
