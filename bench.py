@@ -1067,7 +1067,8 @@ def multiscale_visco_workload(args, local):
         free, _ = torch.cuda.mem_get_info(dev)
         B = max(1, min(len(shots), int((free - 6e9 - (sizes[0] - per_shot)) // per_shot)))
         batches.append(B)
-        mod = synth.q_moduli(p, *mt, q, fmin_q, fmax_q)
+        tau_q, fl_q = synth.tau_of_q(q, fmin_q, fmax_q, 3)
+        mod = synth.q_moduli(p, *mt, tau_q, fl_q)
         e = ifosb.Engine(p, max_shots=B, max_nf=0)
         e.set_cpml(cp)
         e.set_receivers(rec)
@@ -1076,7 +1077,7 @@ def multiscale_visco_workload(args, local):
         obs = np.concatenate([e.forward(shots[i:i + B]) for i in range(0, len(shots), B)])
         t_obs += time.perf_counter() - t0
         e.close()
-        mod0 = synth.q_moduli(p, *m0, q, fmin_q, fmax_q)
+        mod0 = synth.q_moduli(p, *m0, tau_q, fl_q)
         ghost = [ifosb.ghost_wrap(mod0[k]) for k in ("rho", "pi", "u")]
         srcpos_m = np.array([[sp[0, 0] * gd["h"], sp[0, 1] * gd["h"], sp[0, 2] * gd["h"]] for sp, _ in shots], np.float32)
         cfg = Settings(teststep=0.02, damptype=2, lbfgs=True, numpar=1, bfgsnum=3, nshots_step=4,

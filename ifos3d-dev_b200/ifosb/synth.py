@@ -45,24 +45,36 @@ def q_tau_fit(q: float, fmin: float, fmax: float, nmech: int):
     return tau, fl.astype(np.float32)
 
 
-def q_moduli(p, vp, vs, rho, q, fmin, fmax):
+def tau_of_q(q, fmin, fmax, nmech):
+    """The tau method's relaxation time for a Q field: the fit is linear in 1/Q
+    (q_tau_fit), so tau = tau(Q=1) / Q, in float64 then rounded to float32.
+    Returns (tau[...], fl[nmech])."""
+    tau1, fl = q_tau_fit(1.0, fmin, fmax, nmech)
+    return (tau1 / np.asarray(q, np.float64)).astype(np.float32), fl
+
+
+def q_moduli(p, vp, vs, rho, tau, fl):
     """readmod's relaxed moduli (src/readmod.c:48-65, generalised to L mechanisms)
-    with a relaxation time per cell: the tau method's fit is linear in 1/Q
-    (q_tau_fit), so tau = tau(Q=1) / Q; taus = taup = tau. ws = 2 pi FL[1] as in
-    readmod. Returns dict(rho, pi, u, taus, taup, eta) as float32 arrays."""
+    with a relaxation time per cell (taus = taup = tau), in readmod's arithmetic:
+    pts_l = 1 / (2 pi FL_l) and ws = 2 pi FL[1] rounded to float, the sum
+    sum_l ws^2 pts_l^2 tau / (1 + ws^2 pts_l^2) with float products and double
+    quotients, pi = vp^2 rho / (1 + sum) the same way. Returns dict(rho, pi, u,
+    taus, taup, eta) as float32 arrays."""
     L = p.nmech
-    tau1, fl = q_tau_fit(1.0, fmin, fmax, L)
-    tau = (np.float32(tau1) / np.asarray(q, np.float32)).astype(np.float32)
+    fl = np.asarray(fl, np.float32)
     pts = (1.0 / (2.0 * PI * fl.astype(np.float64))).astype(np.float32)
     ws = np.float32(2.0 * PI * float(fl[0]))
-    s = np.float32(0.0)
-    for t in pts:
-        s = np.float32(s + np.float32((ws * ws * t * t) / np.float32(1.0 + ws * ws * t * t)))
+    tau = np.asarray(tau, np.float32)
+    acc = np.zeros(tau.shape, np.float32)
+    for t in pts[:L]:
+        w2t2 = np.float32(np.float32(np.float32(ws * ws) * t) * t)
+        num = (w2t2 * tau).astype(np.float32)
+        acc = (acc.astype(np.float64) + num.astype(np.float64) / (1.0 + np.float64(w2t2))).astype(np.float32)
+    den = 1.0 + acc.astype(np.float64)
     vp, vs, rho = (np.asarray(a, np.float32) for a in (vp, vs, rho))
-    den = (np.float32(1.0) + tau * s).astype(np.float32)
-    pi = (vp * vp * rho / den).astype(np.float32)
-    u = (vs * vs * rho / den).astype(np.float32)
-    eta = (np.float32(p.dt) / pts).astype(np.float32)
+    pi = ((vp * vp * rho).astype(np.float64) / den).astype(np.float32)
+    u = ((vs * vs * rho).astype(np.float64) / den).astype(np.float32)
+    eta = (np.float32(p.dt) / pts[:L]).astype(np.float32)
     return dict(rho=rho, pi=pi, u=u, taus=tau.copy(), taup=tau.copy(), eta=eta)
 
 

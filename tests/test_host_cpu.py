@@ -136,3 +136,26 @@ def test_q_gradient_chain_rule(ifosb_mod):
     h = 1e-4 * q0
     fd = (gq[0] * (tp(q0 + h) - tp(q0 - h)) + gq[1] * (ts(q0 + h) - ts(q0 - h))) / (2 * h)
     assert np.allclose(got, fd, rtol=1e-6, atol=0)
+
+
+def test_q_moduli_per_cell_matches_readmod(ifosb_mod):
+    """synth.q_moduli (readmod's arithmetic with a relaxation time per cell)
+    equals ifosb_moduli (one tau for the model) bit for bit where tau is
+    uniform; synth.tau_of_q scales tau as 1/Q."""
+    p = ifosb_mod.make_params(10, 9, 8, dh=1.0, dt=1e-4, nt=10, fdcoeff=2, free_surf=0, fw=2, nmech=3)
+    rng = np.random.default_rng(4)
+    shape = (9, 10, 8)
+    vp = rng.uniform(2500, 3500, shape).astype(np.float32)
+    vs = (vp / np.float32(np.sqrt(3.0))).astype(np.float32)
+    rho = rng.uniform(1800, 2400, shape).astype(np.float32)
+    for q in (30.0, 50.0, 100.0):
+        tau, fl = synth.q_tau_fit(q, 10.0, 100.0, 3)
+        ref = ifosb_mod.moduli(p, vp.ravel(), vs.ravel(), rho.ravel(), tau=tau, fl=fl)
+        got = synth.q_moduli(p, vp, vs, rho, np.full(shape, tau, np.float32), fl)
+        for k in ("pi", "u", "taus", "taup"):
+            assert np.array_equal(got[k].ravel(), ref[k]), (q, k)
+        assert np.array_equal(got["eta"], ref["eta"])
+    qf = rng.uniform(30, 100, shape).astype(np.float32)
+    tq, fl = synth.tau_of_q(qf, 10.0, 100.0, 3)
+    t50, _ = synth.q_tau_fit(50.0, 10.0, 100.0, 3)
+    np.testing.assert_allclose(tq * qf, np.float32(t50 * 50.0), rtol=1e-6)

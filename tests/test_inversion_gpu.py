@@ -199,14 +199,15 @@ def test_viscoelastic_inversion_reduces_misfit():
     shots = [(sp, ifosb.wavelet(p, 4, sp)) for sp in src]
     rec = synth._grid_receivers(NX, NZ, 6, FW + 2, FW + 3)
     cp = ifosb.cpml_coeff(p, 3000.0, FC)
-    mT = synth.q_moduli(p, vpT, vpT / np.float32(math.sqrt(3)), rho, q, 100.0, 600.0)
+    tau, fl = synth.tau_of_q(q, 100.0, 600.0, 3)
+    mT = synth.q_moduli(p, vpT, vpT / np.float32(math.sqrt(3)), rho, tau, fl)
     e = ifosb.Engine(p, max_shots=len(shots), max_nf=0)
     e.set_cpml(cp)
     e.set_receivers(rec)
     e.set_model(mT["rho"], mT["pi"], mT["u"], mT["taus"], mT["taup"], mT["eta"])
     obs = e.forward(shots)
     e.close()
-    m0 = synth.q_moduli(p, vp0, vp0 / np.float32(math.sqrt(3)), rho, q, 100.0, 600.0)
+    m0 = synth.q_moduli(p, vp0, vp0 / np.float32(math.sqrt(3)), rho, tau, fl)
     ghost = [ifosb.ghost_wrap(m0[k]) for k in ("rho", "pi", "u")]
     srcpos_m = np.array([[s[0][0, 0], s[0][0, 1], s[0][0, 2]] for s in shots], np.float32)
     cfg = Settings(teststep=0.02, damptype=2, lbfgs=False, nshots_step=4, max_batch=4, weight=(1.0, 0.0, 0.0))
