@@ -478,6 +478,7 @@ extern "C" int ifosb_set_model(ifosb_engine *e, const float *rho, const float *p
     a.rho_w = e->d_rho_w;
     dim3 blk(32, 4), grd((p.nz + 31) / 32, (p.nx + 3) / 4, p.ny);
     k_av_mat<<<grd, blk, 0, e->stream>>>(a);
+    k_rho_field<<<dim3((p.nz + 2 + 31) / 32, (p.nx + 2 + 3) / 4, p.ny + 2), blk, 0, e->stream>>>(a);
     cudaError_t le = cudaGetLastError();
     cudaError_t se = cudaStreamSynchronize(e->stream);
     if (le != cudaSuccess || se != cudaSuccess)
@@ -816,13 +817,17 @@ static bool setup_tma(ifosb_engine *e, Loop &L, float *dft) {
     const cuuint64_t mdims[4] = {(cuuint64_t)g.pz, (cuuint64_t)g.px, (cuuint64_t)(p.ny + 5), (cuuint64_t)NMODEL};
     const cuuint64_t mstr[3] = {(cuuint64_t)g.pz * 4, (cuuint64_t)g.plane * 4, (cuuint64_t)g.field * 4};
     const cuuint32_t bhalov[5] = {(cuuint32_t)RZ, RXV, 1, 3, 1}, bpt[5] = {(cuuint32_t)TZ, TXV, 1, 3, 1};
-    const cuuint32_t bmv[4] = {(cuuint32_t)TZ, TXV, 1, 3};
+    const cuuint64_t rdims[3] = {(cuuint64_t)g.pz, (cuuint64_t)g.px, (cuuint64_t)(p.ny + 5)};
+    const cuuint64_t rstr[2] = {(cuuint64_t)g.pz * 4, (cuuint64_t)g.plane * 4};
+    const cuuint32_t brh[3] = {(cuuint32_t)RZ, RXV, 1}, brp[3] = {(cuuint32_t)TZ, TXV, 1};
     const cuuint32_t bhalo[5] = {(cuuint32_t)RZ, RX, 1, 3, 1}, bsr[5] = {(cuuint32_t)TZ, TX, 1, (cuuint32_t)nsr, 1};
     const cuuint32_t bms[4] = {(cuuint32_t)TZ, TX, 1, (cuuint32_t)nm};
     L.vt = VelTma{};
     L.stt = StrTma{};
     if (!encode(&L.vt.m_halo, e->d_state, 5, sdims, sstr, bhalov) ||
-        !encode(&L.vt.m_pt, e->d_state, 5, sdims, sstr, bpt) || !encode(&L.vt.m_mod, e->d_model, 4, mdims, mstr, bmv) ||
+        !encode(&L.vt.m_pt, e->d_state, 5, sdims, sstr, bpt) ||
+        !encode(&L.vt.m_rho_halo, e->d_rho_w, 3, rdims, rstr, brh) ||
+        !encode(&L.vt.m_rho_pt, e->d_rho_w, 3, rdims, rstr, brp) ||
         !encode(&L.stt.m_halo, e->d_state, 5, sdims, sstr, bhalo) ||
         !encode(&L.stt.m_sr, e->d_state, 5, sdims, sstr, bsr) || !encode(&L.stt.m_mod, e->d_model, 4, mdims, mstr, bms))
         return false;

@@ -928,6 +928,19 @@ struct AvArgs {
     float *rho_w;                              // rho in field layout (gradient)
 };
 
+// rho in field layout over the ghosted box (j, i, k = 0..N+1): the ghost layers
+// matcopy left (periodic on one rank) next to the interior, so the velocity
+// kernel can form av_mat's averages rip, rjp, rkp from rho and its +1 neighbours.
+__global__ void k_rho_field(AvArgs a) {
+    const Geo &g = a.g;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.y * blockDim.y + threadIdx.y;
+    const int j = blockIdx.z;
+    if (k > g.nz + 1 || i > g.nx + 1 || j > g.ny + 1) return;
+    const long long GX = g.nx + 2, GZ = g.nz + 2;
+    a.rho_w[widx(g, j, i, k)] = a.rho[((long long)j * GX + i) * GZ + k];
+}
+
 __global__ void k_av_mat(AvArgs a) {
     const Geo &g = a.g;
     const int k = blockIdx.x * blockDim.x + threadIdx.x + 1;

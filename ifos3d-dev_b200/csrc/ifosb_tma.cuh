@@ -126,10 +126,22 @@ __device__ __forceinline__ void tma_load4(void *dst, const CUtensorMap *m, int c
         : "memory");
 }
 
+__device__ __forceinline__ void tma_load3(void *dst, const CUtensorMap *m, int c0, int c1, int c2, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(su32(dst)),
+        "l"(m), "r"(c0), "r"(c1), "r"(c2), "r"(su32(bar))
+        : "memory");
+}
+
 // L2 prefetch of a box (no shared memory, no completion): warms L2 for a later load.
 __device__ __forceinline__ void tma_prefetch5(const CUtensorMap *m, int c0, int c1, int c2, int c3, int c4) {
     asm volatile("cp.async.bulk.prefetch.tensor.5d.L2.global.tile [%0, {%1, %2, %3, %4, %5}];" ::"l"(m), "r"(c0), "r"(c1),
                  "r"(c2), "r"(c3), "r"(c4)
+                 : "memory");
+}
+__device__ __forceinline__ void tma_prefetch3(const CUtensorMap *m, int c0, int c1, int c2) {
+    asm volatile("cp.async.bulk.prefetch.tensor.3d.L2.global.tile [%0, {%1, %2, %3}];" ::"l"(m), "r"(c0), "r"(c1), "r"(c2)
                  : "memory");
 }
 __device__ __forceinline__ void tma_prefetch4(const CUtensorMap *m, int c0, int c1, int c2, int c3) {
@@ -160,9 +172,10 @@ struct WaitCtl {
 };
 
 struct VelTma {
-    CUtensorMap m_halo;  // state, box {RZ, RX, 1, 3, 1}
-    CUtensorMap m_pt;    // state, box {TZ, TX, 1, 3, 1}
-    CUtensorMap m_mod;   // model, box {TZ, TX, 1, 3}
+    CUtensorMap m_halo;      // state, box {RZ, RX, 1, 3, 1}
+    CUtensorMap m_pt;        // state, box {TZ, TX, 1, 3, 1}
+    CUtensorMap m_rho_halo;  // rho in field layout, box {RZ, RX, 1}
+    CUtensorMap m_rho_pt;    // rho in field layout, box {TZ, TX, 1}
     VelArgs a;
     int *tma_err;
     int l2ahead;

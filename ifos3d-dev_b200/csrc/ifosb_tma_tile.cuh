@@ -8,10 +8,12 @@ constexpr int RX = TX + 2 * HX;              // ring rows
 constexpr int RPLANE = RX * RZ;              // floats per field per ring plane
 constexpr int PT = TX * TZ;                  // floats per point-wise field tile
 constexpr int RSLOT = a32(3 * RPLANE);       // ring slot stride (3 stencil fields)
-constexpr int VS_PT = a32(3 * RPLANE);       // velocity stage: offset of the v box
-constexpr int VS_MOD = VS_PT + a32(3 * PT);  // velocity stage: offset of the rip/rjp/rkp box
-constexpr int VS_SP = VS_MOD + a32(3 * PT);  // velocity stage stride
-static_assert(RSLOT % 32 == 0 && VS_PT % 32 == 0 && VS_MOD % 32 == 0 && VS_SP % 32 == 0, "TMA alignment");
+constexpr int VS_RHO = a32(3 * RPLANE);      // velocity stage: rho of plane j with the x/z halo
+constexpr int VS_PT = VS_RHO + a32(RPLANE);  // velocity stage: offset of the v box
+constexpr int VS_RJ = VS_PT + a32(3 * PT);   // velocity stage: rho of plane j + 1 (the tile)
+constexpr int VS_SP = VS_RJ + a32(PT);       // velocity stage stride
+static_assert(RSLOT % 32 == 0 && VS_RHO % 32 == 0 && VS_PT % 32 == 0 && VS_RJ % 32 == 0 && VS_SP % 32 == 0,
+              "TMA alignment");
 constexpr int NTHR = 32 * (TX + 1);          // TX consumer warps + 1 producer warp
 
 __host__ __device__ constexpr size_t vel_tma_smem() {
@@ -139,9 +141,15 @@ __device__ __forceinline__ void vel_rows(const VelTma &T, int nt, const float *r
             szz_z = dz * (b1 * (IP(1, 0, 1) - IP(1, 0, 0)) + b2 * (IP(1, 0, 2) - IP(1, 0, -1)));
             sxz_x = dx * (b1 * (IP(2, 0, 0) - IP(2, -1, 0)) + b2 * (IP(2, 1, 0) - IP(2, -2, 0)));
 #undef IP
-            const float *pv = stage + VS_PT + tx * TZ + tz, *pm = stage + VS_MOD + tx * TZ + tz;
+            const float *pv = stage + VS_PT + tx * TZ + tz;
             vxo = pv[0]; vyo = pv[PT]; vzo = pv[2 * PT];
-            rip = pm[0]; rjp = pm[PT]; rkp = pm[2 * PT];
+            // av_mat's averaged densities (av_mat.c:63-65) from rho and its +1
+            // neighbours in x, y (the next plane's tile) and z, in its arithmetic
+            const float *rh = stage + VS_RHO + cx * RZ + cz;
+            const float r0 = rh[0];
+            rip = (float)(0.5 * (double)(r0 + rh[RZ]));
+            rjp = (float)(0.5 * (double)(r0 + stage[VS_RJ + tx * TZ + tz]));
+            rkp = (float)(0.5 * (double)(r0 + rh[1]));
         }
         consumer_release<VRING, VNSTAGE>(bar, it, false, true);
         if (active) {
@@ -204,7 +212,9 @@ __device__ __forceinline__ void vel_rows(const VelTma &T, int nt, const float *r
 }
 
 // ---------------------------------------------------------------------------
-// Velocity update. Stage layout: [sxx|szz|sxz halo planes][vx vy vz][rip rjp rkp].
+// Velocity update. Stage layout: [sxx|szz|sxz halo planes][rho halo plane][vx vy vz]
+// [rho of the next plane]: rho (one word per cell, shared by the shots) replaces
+// the three averaged densities.
 template <bool BACK>
 __global__ void __launch_bounds__(NTHR, 3) k_velocity_tma(const __grid_constant__ VelTma T, int nt) {
     extern __shared__ __align__(128) unsigned char smem[];
@@ -233,16 +243,17 @@ __global__ void __launch_bounds__(NTHR, 3) k_velocity_tma(const __grid_constant_
             const int j = j0 + it, b = it % VNSTAGE;
             float *d = stg + b * SP;
             uint64_t *fb = &bar[2 * VRING + b];
-            mbar_expect_tx(fb, (3 * RPLANE + 6 * PT) * 4);
+            mbar_expect_tx(fb, (4 * RPLANE + 4 * PT) * 4);
             tma_load5(d, &T.m_halo, zc(k0) - HZ, xc(i0) - HX, yc_(j), SXX, s, fb);
+            tma_load3(d + VS_RHO, &T.m_rho_halo, zc(k0) - HZ, xc(i0) - HX, yc_(j), fb);
             tma_load5(d + VS_PT, &T.m_pt, zc(k0), xc(i0), yc_(j), VX, s, fb);
-            tma_load4(d + VS_MOD, &T.m_mod, zc(k0), xc(i0), yc_(j), MD_RIP, fb);
+            tma_load3(d + VS_RJ, &T.m_rho_pt, zc(k0), xc(i0), yc_(j + 1), fb);
         };
         auto stage_prefetch = [&](int it) {
             const int j = j0 + it;
             tma_prefetch5(&T.m_halo, zc(k0) - HZ, xc(i0) - HX, yc_(j), SXX, s);
+            tma_prefetch3(&T.m_rho_halo, zc(k0) - HZ, xc(i0) - HX, yc_(j));
             tma_prefetch5(&T.m_pt, zc(k0), xc(i0), yc_(j), VX, s);
-            tma_prefetch4(&T.m_mod, zc(k0), xc(i0), yc_(j), MD_RIP);
         };
         auto ring_prefetch = [&](int P) { tma_prefetch5(&T.m_halo, zc(k0) - HZ, xc(i0) - HX, yc_(P), SYY, s); };
         const uint64_t lim = T.w.limit_ns;
