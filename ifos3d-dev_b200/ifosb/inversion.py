@@ -51,6 +51,8 @@ class Settings:
     damptype: int = 2              # DAMPTYPE
     lbfgs: bool = False            # LBFGS
     lbfgs_first_normalised: bool = False  # not in the reference: see Inversion.iterate
+    exact_gradient: bool = False   # not in the reference: the exact discrete VJP instead of gradient_F
+    exact_interval: int = 25       # its checkpoint interval (time steps)
     numpar: int = 1                # NUMPAR
     bfgsnum: int = 3               # BFGSNUM
     nshots_step: int = 1           # NSHOTS_STEP (shots of the step-length test forwards)
@@ -95,6 +97,8 @@ class Inversion:
             if cfg.hess:
                 raise ValueError("the Hessian wavefields are elastic (ifos3d.c:929): no HESS with L > 0")
             self.visco = tuple(np.ascontiguousarray(a, np.float32) for a in visco)
+        if cfg.exact_gradient and cfg.hess:
+            raise ValueError("the approximate Hessian is formed from gradient_F's wavefields: not with exact_gradient")
         self.shots_raw, self.obs_raw = list(shots), np.ascontiguousarray(obs, np.float32)
         self.shots, self.obs = self.shots_raw, self.obs_raw
         self.recpos = np.ascontiguousarray(recpos, np.int32)
@@ -155,6 +159,15 @@ class Inversion:
         else:
             self.eng.set_model(*(a[1:-1, 1:-1, 1:-1] for a in m), None, None, None)
 
+    def _velocity_gradient(self, gm):
+        """The exact VJP's derivative with respect to (rho, pi, u, taus, taup) onto
+        modelupdate's parameters vp = sqrt(pi / rho), vs = sqrt(u / rho), rho (the
+        relaxed velocities when L > 0, the relaxation times fixed)."""
+        rho, pi, u = (a[1:-1, 1:-1, 1:-1].astype(np.float64) for a in self.model)
+        vp, vs = np.sqrt(pi / rho), np.sqrt(u / rho)
+        g_rho, g_pi, g_u = gm[0], gm[1], gm[2]
+        return np.stack([g_pi * 2.0 * rho * vp, g_u * 2.0 * rho * vs, g_rho + g_pi * vp * vp + g_u * vs * vs])
+
     def _batches(self, idx):
         b = self.cfg.max_batch
         return [idx[i:i + b] for i in range(0, len(idx), b)]
@@ -198,8 +211,17 @@ class Inversion:
             self.eng.hessian_green(list(range(ntr_hess)), self._hess_signals(ntr_hess))
             self.eng.zero_hessian()
         mis = np.zeros(len(self.shots))
+        gx = None
+        if cfg.exact_gradient:
+            gx = np.zeros((3, p.ny, p.nx, p.nz), np.float64)
         for chunk in self._batches(list(range(len(self.shots)))):
-            mis[chunk] = self.eng.shot_gradient([self.shots[i] for i in chunk], self.obs[chunk])
+            if cfg.exact_gradient:
+                self.eng.forward([self.shots[i] for i in chunk], want_sections=False)
+                mis[chunk] = self.eng.residual(self.obs[chunk])
+                gm, _ = self.eng.vjp_exact(cfg.exact_interval, moduli=True)
+                gx += self._velocity_gradient(gm)
+            else:
+                mis[chunk] = self.eng.shot_gradient([self.shots[i] for i in chunk], self.obs[chunk])
             if new_hess:
                 self.eng.hessian()  # hess_F of these shots (ifos3d.c:983)
         L2 = np.zeros(4, np.float64)
@@ -209,7 +231,8 @@ class Inversion:
             if cfg.hess_file:  # ifos3d.c:996
                 fio.write_gradient(cfg.hess_file, float(self.finv[0]), self.iteration, self.hess,
                                    idx=cfg.ids[0], idy=cfg.ids[1], idz=cfg.ids[2])
-        g = self.eng.get_gradient()
+        # gradient_F's sign: minus the misfit's derivative (a descent direction)
+        g = (-gx).astype(np.float32) if cfg.exact_gradient else self.eng.get_gradient()
         self._write_grad(g, self.iteration)
         if cfg.hess and self.hess is not None:  # ifos3d.c:1002
             self.opt.hess_apply(g, self.hess, np.asarray(cfg.water_hess, np.float32), lbfgs=cfg.lbfgs,
